@@ -1,0 +1,331 @@
+"""Benchmark of the SIMPLE outer iteration (Ixchel2D hot path) on B200.
+
+Workload: the heated lid-driven cavity in mixed convection, Re=100, Ri=1,
+Pr=0.71, on a 701x301 staggered mesh (mi=701, nj=301: 702x302 = 212,004
+p-cells) with tanh wall clustering (parameter 1.2), binary64, synthetic
+inputs built in code (no dataset involved).  A step is ITERS outer SIMPLE
+iterations (one inner pass of each equation, as conv_u/p/t are set so each
+inner loop exits after its first pass).  Metric: Mcell-iter/s (p-cells x
+outer iterations per second), whole job over all ranks.
+
+The working set (~45 MB) fits the 126 MB L2, so L2 is flushed (a 256 MiB
+write) before every timed step and every timed kernel launch.
+
+--impl reference times the CPU restatement of the reference (oracle/, the
+reference itself is Fortran + OpenACC and cannot be built here) on all host
+cores for the same workload and metric.
+
+Multi-GPU: one instance does not shard (every sweep spans the whole domain),
+so N ranks run N independent replicas (weak scaling, no collective on the
+data path); value = cells x iterations of all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ITERS = 20                 # outer iterations per step
+FLUSH_BYTES = 256 << 20    # > 126 MB L2
+MI, NJ = 701, 301
+# algorithmic bytes per p-cell of each phase (each array streamed once)
+PHASES = ["u-y sweep", "u-x sweep", "v-y sweep", "v-x sweep", "p'-y sweep", "p'-x sweep", "p/u/v correction",
+          "T-y sweep", "T-x sweep", "u residual"]
+BYTES_PER_CELL = [48, 56, 48, 64, 48, 64, 72, 40, 48, 48]
+MEMSET_BYTES_PER_CELL = 8
+KERNELS_PER_ITER = 18      # 10 phase kernels + 4 gates/controls per inner loop set + outer control
+
+
+def workload_config():
+    return {"workload": f"lid_driven_mixed_{MI}x{NJ}_Re100_Ri1_Pr0.71_tanh1.2", "mi": MI, "nj": NJ,
+            "p_cells": (MI + 1) * (NJ + 1), "outer_iters_per_step": ITERS, "inner_passes": 1,
+            "l2": "flushed (256 MiB write) before every timed step and kernel launch"}
+
+
+def make_case():
+    from ixchel2d_b200 import cases
+    return cases.lid_driven_mixed(MI, NJ, Re=100.0, Ri=1.0, Pr=0.71, beta=1.2)
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_rate(case, budget_s: float = 12.0, chunk: int = 5):
+    """Oracle (C++ restatement, OpenMP over grid lines) on all host cores."""
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+    o = O.OracleCase(case, conv_u=1e30, conv_p=1e30, conv_t=1e30)
+    o.iterations(2)  # warm
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < budget_s:
+        o.iterations(chunk)
+        n += chunk
+    dt = time.perf_counter() - t0
+    return case.cells * n / dt / 1e6, n, O.max_threads(), dt
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+    case = make_case()
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+    o = O.OracleCase(case, conv_u=1e30, conv_p=1e30, conv_t=1e30)
+    # each step is a bounded sample of the workload: 2 outer iterations
+    sample_iters = 2
+    for _ in range(args.warmup):
+        o.iterations(sample_iters)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.iterations(sample_iters)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = case.cells * sample_iters * args.steps / tot / 1e6
+    line = {
+        "impl": "reference", "metric": "Mcell-iter/s (SIMPLE outer iteration, p-cells)", "value": value,
+        "unit": "Mcell-iter/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": "Mcell-iter/s", "cores": O.max_threads(), "kind": "port",
+                         "sample": f"{sample_iters} outer iterations of the full 701x301 case per step"},
+        "e2e": {"value": value, "unit": "Mcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference is Fortran+OpenACC (nvfortran-only build); its C++ restatement (oracle/) is timed",
+    }
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+def run_ours(args):
+    import torch
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    from ixchel2d_b200 import Simple2D, lib
+    if lib.ixb_device_count() < 1:
+        raise RuntimeError("no CUDA device visible")
+    case = make_case()
+    stream = torch.cuda.Stream()
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    sim = Simple2D.from_case(case)
+    sim.set_stream(stream.cuda_stream)
+    # warm-up (also builds the CUDA graph)
+    for _ in range(args.warmup):
+        sim.iterations(ITERS)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region ----
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    t_wall = time.perf_counter()
+    reports = []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+        reports.append(sim.iterations(ITERS))
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    if pg:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    torch.cuda.synchronize()
+    cells_iters = case.cells * ITERS * args.steps * world
+    value = cells_iters / (ms / 1e3) / 1e6
+
+    # ---- end to end through the C ABI with host buffers ----
+    keys = ("u", "v", "p", "T", "u_ant", "v_ant", "T_ant")
+    st0 = sim.download()
+    host = {}
+    for kk in keys:
+        t = torch.empty(st0[kk].shape[::-1], dtype=torch.float64, pin_memory=True)
+        a = t.numpy().T  # Fortran-ordered view of pinned memory
+        a[...] = st0[kk]
+        host[kk] = a
+    h2d = sum(a.nbytes for a in host.values())
+    e2e_ms = 0.0
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        sim.upload(host)
+        sim.iterations(ITERS)
+        out = sim.download()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        for kk in keys:
+            host[kk][...] = out[kk]
+    if pg:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = cells_iters / (e2e_ms / 1e3) / 1e6
+
+    # ---- per-kernel times (cold L2) on a scratch handle ----
+    scratch = Simple2D.from_case(case)
+    scratch.set_stream(stream.cuda_stream)
+    scratch.iterations(3)
+    phase_ms = scratch.time_phases(reps=10, flush_bytes=FLUSH_BYTES)
+    scratch.close()
+    cells = case.cells
+    per_iter_ms = [m * (1 if k != 9 else 1) for k, m in enumerate(phase_ms)]
+    dom = int(np.argmax(per_iter_ms))
+    peak, peak_kind = peaks()
+    alg_bytes = BYTES_PER_CELL[dom] * cells
+    achieved = alg_bytes / (phase_ms[dom] / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(PHASES[dom])
+
+    line = None
+    if rank == 0:
+        cpu_val, cpu_iters, cpu_cores, cpu_s = cpu_oracle_rate(case) if world == 1 else (None, 0, 0, 0)
+        iter_bytes = (sum(BYTES_PER_CELL) + MEMSET_BYTES_PER_CELL) * cells
+        line = {
+            "metric": "Mcell-iter/s (SIMPLE outer iteration, p-cells)", "value": value, "unit": "Mcell-iter/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {**workload_config(), "parallelism": f"replicas{world}"},
+            "e2e": {"value": e2e_value, "unit": "Mcell-iter/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": h2d,
+                    "note": "per step: 7 state arrays host->device, ITERS outer iterations, 7 arrays device->host"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": PHASES[dom],
+                         "peak_kind": f"{peak_kind} (copy bandwidth)",
+                         "alg_bytes_per_launch": alg_bytes, "launch_ms": phase_ms[dom]},
+            "phases_ms_cold_l2": dict(zip(PHASES, phase_ms)),
+            "iteration_alg_bytes": iter_bytes,
+            "iteration_gbs": iter_bytes * ITERS * args.steps / (ms / 1e3) / 1e9 / world * world,
+            "cpu_baseline": None if cpu_val is None else {
+                "value": cpu_val, "unit": "Mcell-iter/s", "cores": cpu_cores, "kind": "port",
+                "sample": f"{cpu_iters} outer iterations of the same 701x301 case ({cpu_s:.1f} s)"},
+            "gpu_launches": (KERNELS_PER_ITER * ITERS + 1) * args.steps,
+            "clocks": clocks,
+            "last_report": {k: reports[-1][k] for k in ("maxbo", "residuo", "n_simple", "n_momen")},
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,197 @@
+/*
+ * ixb.h -- C ABI of libixb, the B200 (sm_100a) SIMPLE outer iteration of
+ * Ixchel2D.
+ *
+ * The reference has no C ABI: its hot path is Fortran module state plus
+ * per-cell `!$acc routine` subroutines called from PROGRAM IXCHEL2D
+ * (source/main.f90:395-1217).  Each entry point below names the reference
+ * code it replaces.  All functions return an int status (IXB_OK = 0).
+ * Calls on one handle are not thread-safe; separate handles are independent
+ * (each owns its own device memory and CUDA stream).
+ *
+ * Array convention (host side): every 2-D array is Fortran column-major
+ * with the reference's shapes, index (ii,jj) at (jj-1)*rows + (ii-1):
+ *   u, u_ant, au, Resu, fuente_*_u   (mi,   nj+1)
+ *   v, v_ant, av, fuente_*_v         (mi+1, nj  )
+ *   p, T, T_ant, corr_pres, b_o, fuente_*_t  (mi+1, nj+1)
+ * Mesh vectors: xu(mi), yv(nj), xp(mi+1), yp(nj+1).
+ */
+#ifndef IXB_H
+#define IXB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define IXB_OK 0
+#define IXB_EINVAL 1     /* bad argument (NULL handle, size out of range, ...) */
+#define IXB_ECUDA 2      /* a CUDA runtime call failed */
+#define IXB_ENONFINITE 3 /* a convergence norm became NaN or Inf */
+#define IXB_ETIMEOUT 4   /* a bounded device wait expired */
+#define IXB_EBC 5        /* a boundary table leaves a solved line without a row */
+#define IXB_ESTATE 6     /* call order: mesh/params/bc not set yet */
+#define IXB_EIO 7        /* file could not be read / parsed / written */
+#define IXB_ENOMEM 8     /* device or host allocation failed */
+
+/* precision modes for ixb_create */
+#define IXB_PREC_FP64 0         /* everything in binary64 */
+#define IXB_PREC_FP32_REFINED 1 /* binary32 assembly + sweeps, binary64 mass
+                                   residual, p' right-hand side and p/T updates */
+
+/* line solvers */
+#define IXB_SOLVER_HYBRID 0 /* warp Thomas-PCR hybrid (default, fast) */
+#define IXB_SOLVER_EXACT 1  /* sequential Thomas, bit-identical to
+                               source/mod_solucionador.f90:25-47 */
+
+/* variables for ixb_set_bc / ixb_set_sources */
+#define IXB_VAR_U 0
+#define IXB_VAR_V 1
+#define IXB_VAR_T 2
+
+/* boundary-segment types (tipo_condi strings of source/mod_cond_frontera.f90:34) */
+#define IXB_BC_OTHER 0 /* any string other than 'diri'/'neum' (e.g. the default 'desc') */
+#define IXB_BC_DIRI 1
+#define IXB_BC_NEUM 2
+
+typedef struct ixb_handle ixb_handle;
+
+/* Solver parameters: the numeric records of parametros.dat after the
+ * non-dimensionalisation of source/main.f90:221-244. */
+typedef struct {
+  double gamma_momen;  /* sqrt(Pr/Ra) natural, 1/Re mixed            */
+  double gamma_energ;  /* sqrt(1/(Pr*Ra)) natural, 1/(Re*Pr) mixed   */
+  double Ri;           /* u-momentum buoyancy coefficient (0 in both modes) */
+  double Riy;          /* v-momentum buoyancy coefficient (-1 natural, Ri mixed) */
+  double dt;
+  double rel_vel, rel_pres, rel_ener;
+  double conv_u, conv_p, conv_t, conv_resi, conv_paso;
+  double p_update;     /* pressure under-relaxation, 0.6 in the reference (main.f90:934) */
+  int iter_ecuaci_max;
+  int iter_simple_max;
+  int solver;          /* IXB_SOLVER_* */
+  int reserved[5];
+} ixb_params;
+
+/* One side of tipo_cond_front (source/mod_cond_frontera.f90:25-38) after
+ * lectura_cond_frontera: `index` holds indice_div(1..ndivis+1), 1-based.
+ * (The reference declares indice_div(14); 16 entries let 15 divisions fit.) */
+typedef struct {
+  int side;         /* 0..3 = 'a','b','c','d' */
+  int ndivis;       /* 0..15 */
+  int type[15];     /* IXB_BC_* */
+  double value[15];
+  int index[16];
+} ixb_bc_side;
+
+/* Outcome of a SIMPLE call. */
+typedef struct {
+  double maxbo;     /* ||b_o||_2 of the last pressure pass (main.f90:898-906) */
+  double residuo;   /* ||Resu||_2 of the last outer iteration (main.f90:1192-1199) */
+  double err_u, err_p, err_t; /* last inner-loop errors (||dv||, ||dp'||, ||dT||) */
+  int64_t n_simple; /* outer iterations run in this call */
+  int64_t n_momen, n_pres, n_ener; /* inner passes run in this call */
+  int exit_code;    /* 0 none (fixed count), 1 converged, 2 iteration limit */
+  int status;
+} ixb_report;
+
+/* ---- library ---- */
+int ixb_version(void);
+const char* ixb_strerror(int status);
+/* Number of CUDA devices visible (0 on a host without a GPU). */
+int ixb_device_count(void);
+
+/* ---- handle lifetime: replaces the `!$acc data` region of main.f90:356-389 ---- */
+/* mi, nj: the grid sizes of source/mod_malla.f90:15, here chosen at run time. */
+int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out);
+int ixb_destroy(ixb_handle* h);
+/* Use an external CUDA stream (cudaStream_t) instead of the handle's own. */
+int ixb_set_stream(ixb_handle* h, void* stream);
+
+/* ---- inputs ---- */
+/* Mesh coordinates; the metrics delta*, fe* are derived exactly as in
+ * lectura_mallas_escalonadas (source/mod_malla.f90:167-218). */
+int ixb_set_mesh(ixb_handle* h, const double* xu, const double* yv, const double* xp, const double* yp);
+int ixb_set_params(ixb_handle* h, const ixb_params* p);
+/* Boundary tables for u, v or T (the cond_front_* structures of
+ * source/mod_ec_momento.f90:46-47, mod_ec_energia.f90:34) as applied by
+ * impone_cond_frontera (source/mod_cond_frontera.f90:254-420).  Returns
+ * IXB_EBC when a line that the reference solves would be left without a
+ * boundary row (the reference would then read stale coefficients). */
+int ixb_set_bc(ixb_handle* h, int var, const ixb_bc_side sides[4]);
+/* Source terms fuente_con_*, fuente_lin_* (source/mod_ec_momento.f90:34-35,
+ * mod_ec_energia.f90:30), e.g. immersed-body masks (mod_front_inmersa.f90:54-179).
+ * NULL arrays mean zero. */
+int ixb_set_sources(ixb_handle* h, int var, const double* fuente_con, const double* fuente_lin);
+
+/* ---- state transfer (host arrays, Fortran shapes); NULL pointers are skipped ---- */
+int ixb_upload_state(ixb_handle* h, const double* u, const double* v, const double* p, const double* T,
+                     const double* u_ant, const double* v_ant, const double* T_ant);
+int ixb_download_state(ixb_handle* h, double* u, double* v, double* p, double* T, double* u_ant,
+                       double* v_ant, double* T_ant);
+/* Work arrays after the last iteration: au, av, b_o, Resu, corr_pres. */
+int ixb_download_aux(ixb_handle* h, double* au, double* av, double* b_o, double* resu, double* corr_pres);
+
+/* ---- the hot path ---- */
+/* Exactly n passes of the ALGORITMO_SIMPLE body (main.f90:404-1200) with
+ * the reference's inner loops, without the outer exit test. */
+int ixb_simple_iterations(ixb_handle* h, int n, ixb_report* rep);
+/* The ALGORITMO_SIMPLE loop of one time step, with the reference's exit
+ * logic (main.f90:1202-1215). */
+int ixb_simple_loop(ixb_handle* h, ixb_report* rep);
+/* Time-step roll T_ant,u_ant,v_ant <- T,u,v (main.f90:1251-1270). */
+int ixb_roll(ixb_handle* h);
+/* One time step: ixb_simple_loop then ixb_roll (main.f90:391-1271 body). */
+int ixb_step(ixb_handle* h, ixb_report* rep);
+/* One phase of the iteration, for per-kernel checks: 0 u-y sweep, 1 u-x,
+ * 2 v-y, 3 v-x, 4 p'-y, 5 p'-x, 6 p/u/v correction, 7 T-y, 8 T-x,
+ * 9 u residual.  Phase 4 reads p' from the current corr_pres. */
+int ixb_phase(ixb_handle* h, int which);
+/* Device time of each phase 0..9 of ixb_phase: each phase is launched
+ * `reps` times on the handle's stream, every launch bracketed by two CUDA
+ * events; when flush_bytes > 0 a scratch buffer of that size is written
+ * before every launch so the kernel starts with a cold L2.  ms[k] receives
+ * the mean milliseconds per launch of phase k.  The state is advanced by the
+ * launches (use on a scratch copy).  No reference counterpart: it measures
+ * the kernels that replace the OpenACC regions. */
+int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
+/* Overwrite corr_pres / au / av on the device (host arrays), for ixb_phase checks. */
+int ixb_set_work(ixb_handle* h, const double* corr_pres, const double* au, const double* av);
+
+/* ---- post-processing on the device ---- */
+/* nusselt_promedio_y (source/mod_postproceso.f90:100-215): walls jj=1 and
+ * jj=nj+1, integrated over ii = i0..i1 step 2. */
+int ixb_nusselt_y(ixb_handle* h, int i0, int i1, double* nu0, double* nu1);
+/* The same rule on the vertical walls ii=1 and ii=mi+1, over jj = j0..j1
+ * step 2 (no counterpart in the reference; it only has the horizontal form). */
+int ixb_nusselt_x(ixb_handle* h, int j0, int j1, double* nu0, double* nu1);
+
+/* ---- batched line solver: tridiagonal (source/mod_solucionador.f90:25-47)
+ * over many systems, DEVICE pointers.  Row i of system s is
+ * a[i]x[i-1] + b[i]x[i] + c[i]x[i+1] = d[i]; a[0] and c[n-1] are ignored.
+ * layout 0: system s row i at s*n + i (contiguous, x-lines);
+ * layout 1: at i*nsys + s (interleaved, y-lines).
+ * x may alias d.  a, b, c, d are not modified (unless x aliases d). ---- */
+int ixb_tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,
+                    int nsys, int layout, int solver, void* stream);
+int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float* d, float* x, int n,
+                    int nsys, int layout, int solver, void* stream);
+
+/* ---- host-side inputs (no GPU needed) ---- */
+/* lectura_cond_frontera index rule (source/mod_cond_frontera.f90:114-238):
+ * for side 0/2 ('a'/'c') the divisions are located on `yy` (nn entries), for
+ * 1/3 ('b'/'d') on `xx` (mm entries). */
+int ixb_bc_locate(int side, int ndivis, const double* x1, const int* type, const double* value,
+                  const double* xx, int mm, const double* yy, int nn, ixb_bc_side* out);
+/* Read cond_frontera{u,v,t}.dat: four sides, each "variable side ndivis"
+ * followed by ndivis lines "x0 x1 type value". */
+int ixb_read_bc_file(const char* path, const double* xx, int mm, const double* yy, int nn,
+                     ixb_bc_side out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IXB_H */

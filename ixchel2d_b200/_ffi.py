@@ -1,0 +1,118 @@
+"""ctypes binding of libixb.so (include/ixb.h).
+
+The library is loaded from the package directory; a missing library is an
+error (there is no CPU fallback for the hot path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("IXB_LIB", _PKG / "libixb.so"))
+
+OK, EINVAL, ECUDA, ENONFINITE, ETIMEOUT, EBC, ESTATE, EIO, ENOMEM = range(9)
+PREC_FP64, PREC_FP32_REFINED = 0, 1
+SOLVER_HYBRID, SOLVER_EXACT = 0, 1
+VAR_U, VAR_V, VAR_T = 0, 1, 2
+BC_OTHER, BC_DIRI, BC_NEUM = 0, 1, 2
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("gamma_momen", C.c_double), ("gamma_energ", C.c_double), ("Ri", C.c_double), ("Riy", C.c_double),
+        ("dt", C.c_double), ("rel_vel", C.c_double), ("rel_pres", C.c_double), ("rel_ener", C.c_double),
+        ("conv_u", C.c_double), ("conv_p", C.c_double), ("conv_t", C.c_double), ("conv_resi", C.c_double),
+        ("conv_paso", C.c_double), ("p_update", C.c_double),
+        ("iter_ecuaci_max", C.c_int), ("iter_simple_max", C.c_int), ("solver", C.c_int),
+        ("reserved", C.c_int * 5),
+    ]
+
+
+class BCSide(C.Structure):
+    _fields_ = [("side", C.c_int), ("ndivis", C.c_int), ("type", C.c_int * 15), ("value", C.c_double * 15),
+                ("index", C.c_int * 16)]
+
+
+class Report(C.Structure):
+    _fields_ = [
+        ("maxbo", C.c_double), ("residuo", C.c_double), ("err_u", C.c_double), ("err_p", C.c_double),
+        ("err_t", C.c_double), ("n_simple", C.c_int64), ("n_momen", C.c_int64), ("n_pres", C.c_int64),
+        ("n_ener", C.c_int64), ("exit_code", C.c_int), ("status", C.c_int),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class IxbError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        msg = lib.ixb_strerror(status).decode() if lib is not None else str(status)
+        super().__init__(f"{what}: status {status} ({msg})")
+
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_vp = C.c_void_p
+
+# (name, restype, argtypes) of every symbol declared in include/ixb.h
+SIGNATURES = [
+    ("ixb_version", C.c_int, []),
+    ("ixb_strerror", C.c_char_p, [C.c_int]),
+    ("ixb_device_count", C.c_int, []),
+    ("ixb_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
+    ("ixb_destroy", C.c_int, [_vp]),
+    ("ixb_set_stream", C.c_int, [_vp, _vp]),
+    ("ixb_set_mesh", C.c_int, [_vp, _dp, _dp, _dp, _dp]),
+    ("ixb_set_params", C.c_int, [_vp, C.POINTER(Params)]),
+    ("ixb_set_bc", C.c_int, [_vp, C.c_int, C.POINTER(BCSide)]),
+    ("ixb_set_sources", C.c_int, [_vp, C.c_int, _dp, _dp]),
+    ("ixb_upload_state", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    ("ixb_download_state", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    ("ixb_download_aux", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
+    ("ixb_simple_iterations", C.c_int, [_vp, C.c_int, C.POINTER(Report)]),
+    ("ixb_simple_loop", C.c_int, [_vp, C.POINTER(Report)]),
+    ("ixb_roll", C.c_int, [_vp]),
+    ("ixb_step", C.c_int, [_vp, C.POINTER(Report)]),
+    ("ixb_phase", C.c_int, [_vp, C.c_int]),
+    ("ixb_set_work", C.c_int, [_vp, _dp, _dp, _dp]),
+    ("ixb_time_phases", C.c_int, [_vp, C.c_int, C.c_size_t, _dp]),
+    ("ixb_nusselt_y", C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp]),
+    ("ixb_nusselt_x", C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp]),
+    ("ixb_tridiag_f64", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
+    ("ixb_tridiag_f32", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
+    ("ixb_bc_locate", C.c_int, [C.c_int, C.c_int, _dp, C.POINTER(C.c_int), _dp, _dp, C.c_int, _dp, C.c_int,
+                                C.POINTER(BCSide)]),
+    ("ixb_read_bc_file", C.c_int, [C.c_char_p, _dp, C.c_int, _dp, C.c_int, C.POINTER(BCSide)]),
+]
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(f"libixb.so not found at {LIB_PATH}; build it with `python -m ixchel2d_b200.build`")
+    h = C.CDLL(str(LIB_PATH))
+    for name, res, args in SIGNATURES:
+        f = getattr(h, name)
+        f.restype = res
+        f.argtypes = args
+    return h
+
+
+lib = _load()
+
+
+def check(status: int, what: str) -> None:
+    if status != OK:
+        raise IxbError(status, what)
+
+
+def dptr(a: np.ndarray | None):
+    """double* of a contiguous float64 array (None -> NULL)."""
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.flags.c_contiguous)
+    return a.ctypes.data_as(_dp)

@@ -1,0 +1,908 @@
+// ixb_api.cu -- the C ABI of include/ixb.h: handle lifetime, state transfer,
+// boundary tables and the SIMPLE driver loop on one CUDA stream.
+//
+// The outer iteration (source/main.f90:395-1217) runs as one CUDA graph per
+// handle: the reference's three inner loops and the outer loop are WHILE
+// conditional nodes whose conditions are set on the device by tiny control
+// kernels that apply the reference's exit tests, so a whole SIMPLE loop is
+// one graph launch with no host round trip.  The same sequence can also be
+// driven from the host (one sync per inner pass) for debugging.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "ixb_internal.h"
+
+using namespace ixb;
+
+namespace {
+
+// device-side loop state for the graph-driven SIMPLE loop
+struct Ctl {
+  // inputs
+  double conv_u, conv_p, conv_t, conv_resi, conv_paso;
+  int iter_ecuaci_max, iter_simple_max;
+  int fixed_count;   // >0: run exactly this many outer passes, no outer test
+  // state
+  int iter_ecuaci, iter_simple;
+  int outer_done;    // passes done in this launch
+  int inner_done;    // passes of the current inner loop (hard cap: iter_ecuaci_max + 2)
+  int exit_code, status;
+  long long n_simple, n_momen, n_pres, n_ener;
+  double err_u, err_p, err_t, maxbo, residuo;
+};
+
+#define CK(x)                                    \
+  do {                                           \
+    cudaError_t e_ = (x);                        \
+    if (e_ != cudaSuccess) {                     \
+      h->last_cuda = e_;                         \
+      return IXB_ECUDA;                          \
+    }                                            \
+  } while (0)
+
+}  // namespace
+
+struct ixb_handle {
+  int mi = 0, nj = 0, LD = 0, rows = 0, prec = 0;
+  size_t fsz = 0;  // elements per field buffer
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaError_t last_cuda = cudaSuccess;
+  // fields (binary64)
+  double *u[2] = {}, *v[2] = {}, *T[2] = {}, *pc[2] = {};
+  double *p = nullptr, *u_ant = nullptr, *v_ant = nullptr, *T_ant = nullptr;
+  double *au = nullptr, *av = nullptr, *b_o = nullptr, *resu = nullptr;
+  double *fcon[3] = {}, *flin[3] = {};
+  int cu = 0, cv = 0, cT = 0, cpc = 0;
+  // mesh
+  double* metrics = nullptr;
+  int mstride = 0;
+  double *xp_d = nullptr, *yp_d = nullptr;
+  std::vector<double> xu, yv, xp, yp;
+  // boundary tables [var][side][line]
+  BCEntry* bc = nullptr;
+  int bcstride = 0;
+  // reductions
+  double* partials = nullptr;
+  unsigned int* counters = nullptr;
+  double* norms = nullptr;
+  int pstride = 0;
+  double* h_norms = nullptr;  // pinned
+  double* nu_d = nullptr;
+  // control for graphs
+  Ctl* ctl_d = nullptr;
+  Ctl* ctl_h = nullptr;  // pinned
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  bool graph_dirty = true;
+  // params and flags
+  ixb_params prm{};
+  bool has_mesh = false, has_params = false, has_bc[3] = {false, false, false};
+  int iter_ecuaci = 0, iter_simple = 0;
+  int use_graph = 1;
+  int tl_override[EQ_COUNT] = {};
+  int nt_override[EQ_COUNT] = {};
+};
+
+namespace {
+
+Geo<double> make_geo(const ixb_handle* h) {
+  Geo<double> G{};
+  G.mi = h->mi; G.nj = h->nj; G.LD = h->LD; G.mstride = h->mstride; G.m = h->metrics;
+  G.gm = h->prm.gamma_momen; G.ge = h->prm.gamma_energ; G.Ri = h->prm.Ri; G.Riy = h->prm.Riy;
+  G.dt = h->prm.dt; G.rel_vel = h->prm.rel_vel; G.rel_pres = h->prm.rel_pres; G.rel_ener = h->prm.rel_ener;
+  G.p_update = h->prm.p_update;
+  return G;
+}
+
+NormSlot slot(ixb_handle* h, int k) {
+  return NormSlot{h->partials + (size_t)k * h->pstride, h->counters + k, h->norms + k};
+}
+
+int ready(const ixb_handle* h) {
+  if (!h) return IXB_EINVAL;
+  if (!h->has_mesh || !h->has_params || !h->has_bc[0] || !h->has_bc[1] || !h->has_bc[2]) return IXB_ESTATE;
+  return IXB_OK;
+}
+
+// Launch one sweep reading field buffers `cur` and writing `cur^1`.
+int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
+  Geo<double> G = make_geo(h);
+  SweepShape s = sweep_shape(eq, h->mi, h->nj, 8, h->tl_override[eq], h->nt_override[eq]);
+  SweepIO<double> io{};
+  io.u = h->u[h->cu]; io.v = h->v[h->cv]; io.T = h->T[h->cT]; io.p = h->p; io.pc = h->pc[h->cpc];
+  io.u_ant = h->u_ant; io.v_ant = h->v_ant; io.T_ant = h->T_ant;
+  io.au = h->au; io.av = h->av;
+  io.m = s.m; io.mp = s.mp;
+  int var = -1;
+  int* cur = nullptr;
+  double** buf = nullptr;
+  switch (eq) {
+    case EQ_UY: case EQ_UX: var = 0; cur = &h->cu; buf = h->u; break;
+    case EQ_VY: case EQ_VX: var = 1; cur = &h->cv; buf = h->v; break;
+    case EQ_PY: case EQ_PX: var = -1; cur = &h->cpc; buf = h->pc; break;
+    default: var = 2; cur = &h->cT; buf = h->T; break;
+  }
+  io.in = buf[*cur];
+  io.out = buf[*cur ^ 1];
+  io.prev = prev;
+  if (var >= 0) {
+    io.fcon = h->fcon[var]; io.flin = h->flin[var];
+    const bool x = (eq & 1) != 0;
+    const BCEntry* base = h->bc + (size_t)var * 4 * h->bcstride;
+    io.bc_first = base + (size_t)(x ? 0 : 1) * h->bcstride;
+    io.bc_last = base + (size_t)(x ? 2 : 3) * h->bcstride;
+  }
+  if (eq == EQ_UX) io.aux = h->au;
+  if (eq == EQ_VX) io.aux = h->av;
+  if (eq == EQ_PX) io.aux = h->b_o;
+  if (with_norm) {
+    if (eq == EQ_VX) io.nrm0 = slot(h, N_DV);
+    if (eq == EQ_PX) { io.nrm0 = slot(h, N_DP); io.nrm1 = slot(h, N_BO); }
+    if (eq == EQ_TX) io.nrm0 = slot(h, N_DT);
+  }
+  CK(launch_sweep_f64(eq, h->prm.solver, s, G, io, h->stream));
+  *cur ^= 1;
+  return IXB_OK;
+}
+
+int correct(ixb_handle* h) {
+  Geo<double> G = make_geo(h);
+  CK(launch_correct_f64(G, h->u[h->cu], h->v[h->cv], h->p, h->pc[h->cpc], h->au, h->av, h->stream));
+  return IXB_OK;
+}
+
+int residual(ixb_handle* h) {
+  Geo<double> G = make_geo(h);
+  CK(launch_residual_f64(G, h->u[h->cu], h->v[h->cv], h->T[h->cT], h->p, h->u_ant, h->fcon[0], h->flin[0],
+                         h->resu, slot(h, N_RES), h->stream));
+  return IXB_OK;
+}
+
+int read_norms(ixb_handle* h) {
+  CK(cudaMemcpyAsync(h->h_norms, h->norms, N_COUNT * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+#define TRY(x)                 \
+  do {                         \
+    int s_ = (x);              \
+    if (s_ != IXB_OK) return s_; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// host-driven body (one sync per inner pass), main.f90:404-1215
+// ---------------------------------------------------------------------------
+int body_host(ixb_handle* h, bool outer_test, ixb_report* rep, int* exit_code) {
+  const ixb_params& P = h->prm;
+  // ecuacion_momento
+  for (;;) {
+    TRY(sweep(h, EQ_UY, nullptr, false));
+    TRY(sweep(h, EQ_UX, nullptr, false));
+    const double* v_start = h->v[h->cv];
+    TRY(sweep(h, EQ_VY, nullptr, false));
+    TRY(sweep(h, EQ_VX, v_start, true));
+    TRY(read_norms(h));
+    const double err = h->h_norms[N_DV];
+    rep->err_u = err;
+    rep->n_momen++;
+    if (!std::isfinite(err)) return IXB_ENONFINITE;
+    if (err < P.conv_u) { h->iter_ecuaci = 0; break; }
+    else if (h->iter_ecuaci > P.iter_ecuaci_max) { h->iter_ecuaci = 0; break; }
+    else h->iter_ecuaci++;
+  }
+  // correccion_presion
+  CK(cudaMemsetAsync(h->pc[h->cpc], 0, h->fsz * sizeof(double), h->stream));
+  for (;;) {
+    const double* pc_start = h->pc[h->cpc];
+    TRY(sweep(h, EQ_PY, nullptr, false));
+    TRY(sweep(h, EQ_PX, pc_start, true));
+    TRY(read_norms(h));
+    const double err = h->h_norms[N_DP];
+    rep->err_p = err;
+    rep->maxbo = h->h_norms[N_BO];
+    rep->n_pres++;
+    if (!std::isfinite(err) || !std::isfinite(rep->maxbo)) return IXB_ENONFINITE;
+    if (err < P.conv_p) { h->iter_ecuaci = 0; break; }
+    else if (h->iter_ecuaci > P.iter_ecuaci_max) { h->iter_ecuaci = 0; break; }
+    else h->iter_ecuaci++;
+  }
+  TRY(correct(h));
+  // solucion_energia
+  for (;;) {
+    const double* t_start = h->T[h->cT];
+    TRY(sweep(h, EQ_TY, nullptr, false));
+    TRY(sweep(h, EQ_TX, t_start, true));
+    TRY(read_norms(h));
+    const double err = h->h_norms[N_DT];
+    rep->err_t = err;
+    rep->n_ener++;
+    if (!std::isfinite(err)) return IXB_ENONFINITE;
+    if (err < P.conv_t) { h->iter_ecuaci = 0; break; }
+    else if (h->iter_ecuaci > P.iter_ecuaci_max) { h->iter_ecuaci = 0; break; }
+    else h->iter_ecuaci++;
+  }
+  TRY(residual(h));
+  TRY(read_norms(h));
+  rep->residuo = h->h_norms[N_RES];
+  rep->n_simple++;
+  if (!std::isfinite(rep->residuo)) return IXB_ENONFINITE;
+  *exit_code = 0;
+  if (!outer_test) return IXB_OK;
+  if (rep->maxbo < P.conv_paso && rep->residuo < P.conv_resi) { h->iter_simple = 0; *exit_code = 1; }
+  else if (h->iter_simple > P.iter_simple_max) { h->iter_simple = 0; *exit_code = 2; }
+  else h->iter_simple++;
+  return IXB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// graph-driven loop: control kernels set the WHILE conditions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
+
+__global__ void ctl_begin_kernel(Ctl* c, cudaGraphConditionalHandle outer) {
+  cudaGraphSetConditional(outer, 1u);
+  c->outer_done = 0;
+  c->exit_code = 0;
+  c->status = 0;
+  c->n_simple = c->n_momen = c->n_pres = c->n_ener = 0;
+}
+
+__global__ void ctl_inner_kernel(Ctl* c, const double* norms, int which, cudaGraphConditionalHandle inner) {
+  // which: 0 momentum (N_DV vs conv_u), 1 pressure (N_DP vs conv_p), 2 energy (N_DT vs conv_t)
+  double err, conv;
+  if (which == 0) { err = norms[N_DV]; conv = c->conv_u; c->err_u = err; c->n_momen++; }
+  else if (which == 1) { err = norms[N_DP]; conv = c->conv_p; c->err_p = err; c->maxbo = norms[N_BO]; c->n_pres++; }
+  else { err = norms[N_DT]; conv = c->conv_t; c->err_t = err; c->n_ener++; }
+  bool again;
+  c->inner_done++;
+  if (!finite_d(err) || (which == 1 && !finite_d(norms[N_BO]))) {
+    c->status = IXB_ENONFINITE;  // the outer control kernel ends the loop
+    again = false;
+  } else if (err < conv) { c->iter_ecuaci = 0; again = false; }
+  else if (c->iter_ecuaci > c->iter_ecuaci_max) { c->iter_ecuaci = 0; again = false; }
+  else { c->iter_ecuaci++; again = true; }
+  // the reference's counter logic bounds a loop by iter_ecuaci_max + 2
+  // passes; enforce it independently so no WHILE node can run away
+  if (again && (long long)c->inner_done >= (long long)c->iter_ecuaci_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
+  cudaGraphSetConditional(inner, again ? 1u : 0u);
+}
+
+// Gate: after a non-finite stop, later inner loops of the same pass must not
+// start.  Sets the inner loop's initial condition.
+__global__ void ctl_gate_kernel(Ctl* c, cudaGraphConditionalHandle inner) {
+  c->inner_done = 0;
+  cudaGraphSetConditional(inner, c->status == 0 ? 1u : 0u);
+}
+
+__global__ void ctl_outer_kernel(Ctl* c, const double* norms, cudaGraphConditionalHandle outer) {
+  if (c->status != 0) { cudaGraphSetConditional(outer, 0); return; }
+  c->residuo = norms[N_RES];
+  c->n_simple++;
+  c->outer_done++;
+  if (!finite_d(c->residuo)) { c->status = IXB_ENONFINITE; cudaGraphSetConditional(outer, 0); return; }
+  if (c->fixed_count > 0) {
+    cudaGraphSetConditional(outer, c->outer_done < c->fixed_count ? 1u : 0u);
+    return;
+  }
+  bool again;
+  if (c->maxbo < c->conv_paso && c->residuo < c->conv_resi) { c->iter_simple = 0; c->exit_code = 1; again = false; }
+  else if (c->iter_simple > c->iter_simple_max) { c->iter_simple = 0; c->exit_code = 2; again = false; }
+  else { c->iter_simple++; again = true; }
+  if (again && (long long)c->outer_done >= (long long)c->iter_simple_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
+  cudaGraphSetConditional(outer, again ? 1u : 0u);
+}
+
+// Add a WHILE node to `g` after `dep` and return its body graph.
+int add_while(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, cudaGraphConditionalHandle cond,
+              cudaGraph_t* body, cudaGraphNode_t* node) {
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  CK(cudaGraphAddNode(node, g, dep, dep ? 1 : 0, &np));
+  *body = np.conditional.phGraph_out[0];
+  return IXB_OK;
+}
+
+// Capture the launches issued by `fn` on the handle's stream into `g`,
+// appended after `dep` (or as roots); returns the last captured node.
+template <class F>
+int capture_into(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, F fn, cudaGraphNode_t* last) {
+  CK(cudaStreamBeginCaptureToGraph(h->stream, g, dep, nullptr, dep ? 1 : 0, cudaStreamCaptureModeThreadLocal));
+  int st = fn();
+  cudaGraph_t out = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &out);
+  if (st != IXB_OK) return st;
+  CK(e);
+  // find the sink node (the only node without dependents)
+  size_t nn = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+  *last = nullptr;
+  for (auto n : nodes) {
+    size_t nd = 0;
+    CK(cudaGraphNodeGetDependentNodes(n, nullptr, &nd));
+    if (nd == 0) *last = n;
+  }
+  return IXB_OK;
+}
+
+int build_graph(ixb_handle* h) {
+  if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  // the graph bakes buffer parity 0 into its kernel arguments
+  const int cu = h->cu, cv = h->cv, cT = h->cT, cpc = h->cpc;
+  h->cu = h->cv = h->cT = h->cpc = 0;
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  h->graph = g;
+  // a conditional handle belongs to the graph that holds its node: the
+  // outer handle to g, the three inner ones to the outer loop's body
+  cudaGraphConditionalHandle c_outer, c_mom, c_pres, c_ener;
+  CK(cudaGraphConditionalHandleCreate(&c_outer, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNode_t n_begin, n_outer;
+  TRY(capture_into(h, g, nullptr, [&]() {
+    ctl_begin_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_outer);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &n_begin));
+  cudaGraph_t outer_body;
+  TRY(add_while(h, g, &n_begin, c_outer, &outer_body, &n_outer));
+  CK(cudaGraphConditionalHandleCreate(&c_mom, outer_body, 1, 0));
+  CK(cudaGraphConditionalHandleCreate(&c_pres, outer_body, 1, 0));
+  CK(cudaGraphConditionalHandleCreate(&c_ener, outer_body, 1, 0));
+  // outer body: gate(mom) -> WHILE(mom) -> memset p' + gate(pres) -> WHILE(pres)
+  //             -> correct + gate(ener) -> WHILE(ener) -> residual + ctl_outer
+  cudaGraphNode_t last, wn;
+  cudaGraph_t b;
+  TRY(capture_into(h, outer_body, nullptr, [&]() {
+    ctl_gate_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_mom);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  TRY(add_while(h, outer_body, &last, c_mom, &b, &wn));
+  TRY(capture_into(h, b, nullptr, [&]() {
+    TRY(sweep(h, EQ_UY, nullptr, false));
+    TRY(sweep(h, EQ_UX, nullptr, false));
+    const double* v_start = h->v[h->cv];
+    TRY(sweep(h, EQ_VY, nullptr, false));
+    TRY(sweep(h, EQ_VX, v_start, true));
+    ctl_inner_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, 0, c_mom);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  TRY(capture_into(h, outer_body, &wn, [&]() {
+    if (cudaMemsetAsync(h->pc[h->cpc], 0, h->fsz * sizeof(double), h->stream) != cudaSuccess) return IXB_ECUDA;
+    ctl_gate_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_pres);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  TRY(add_while(h, outer_body, &last, c_pres, &b, &wn));
+  TRY(capture_into(h, b, nullptr, [&]() {
+    const double* pc_start = h->pc[h->cpc];
+    TRY(sweep(h, EQ_PY, nullptr, false));
+    TRY(sweep(h, EQ_PX, pc_start, true));
+    ctl_inner_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, 1, c_pres);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  TRY(capture_into(h, outer_body, &wn, [&]() {
+    TRY(correct(h));
+    ctl_gate_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_ener);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  TRY(add_while(h, outer_body, &last, c_ener, &b, &wn));
+  TRY(capture_into(h, b, nullptr, [&]() {
+    const double* t_start = h->T[h->cT];
+    TRY(sweep(h, EQ_TY, nullptr, false));
+    TRY(sweep(h, EQ_TX, t_start, true));
+    ctl_inner_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, 2, c_ener);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  TRY(capture_into(h, outer_body, &wn, [&]() {
+    TRY(residual(h));
+    ctl_outer_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, c_outer);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  CK(cudaGraphInstantiate(&h->graph_exec, g, 0));
+  h->cu = cu; h->cv = cv; h->cT = cT; h->cpc = cpc;
+  h->graph_dirty = false;
+  return IXB_OK;
+}
+
+// Bring every ping-pong field to buffer 0 (the parity the graph expects).
+int normalize_parity(ixb_handle* h) {
+  const size_t bytes = h->fsz * sizeof(double);
+  if (h->cu) { CK(cudaMemcpyAsync(h->u[0], h->u[1], bytes, cudaMemcpyDeviceToDevice, h->stream)); h->cu = 0; }
+  if (h->cv) { CK(cudaMemcpyAsync(h->v[0], h->v[1], bytes, cudaMemcpyDeviceToDevice, h->stream)); h->cv = 0; }
+  if (h->cT) { CK(cudaMemcpyAsync(h->T[0], h->T[1], bytes, cudaMemcpyDeviceToDevice, h->stream)); h->cT = 0; }
+  if (h->cpc) { CK(cudaMemcpyAsync(h->pc[0], h->pc[1], bytes, cudaMemcpyDeviceToDevice, h->stream)); h->cpc = 0; }
+  return IXB_OK;
+}
+
+int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
+  if (h->graph_dirty || !h->graph_exec) TRY(build_graph(h));
+  TRY(normalize_parity(h));
+  Ctl* c = h->ctl_h;
+  std::memset(c, 0, sizeof(Ctl));
+  c->conv_u = h->prm.conv_u; c->conv_p = h->prm.conv_p; c->conv_t = h->prm.conv_t;
+  c->conv_resi = h->prm.conv_resi; c->conv_paso = h->prm.conv_paso;
+  c->iter_ecuaci_max = h->prm.iter_ecuaci_max; c->iter_simple_max = h->prm.iter_simple_max;
+  c->fixed_count = fixed_count;
+  c->iter_ecuaci = h->iter_ecuaci;
+  c->iter_simple = h->iter_simple;
+  CK(cudaMemcpyAsync(h->ctl_d, c, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaGraphLaunch(h->graph_exec, h->stream));
+  CK(cudaMemcpyAsync(c, h->ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  rep->maxbo = c->maxbo; rep->residuo = c->residuo;
+  rep->err_u = c->err_u; rep->err_p = c->err_p; rep->err_t = c->err_t;
+  rep->n_simple = c->n_simple; rep->n_momen = c->n_momen; rep->n_pres = c->n_pres; rep->n_ener = c->n_ener;
+  rep->exit_code = c->exit_code;
+  h->iter_ecuaci = c->iter_ecuaci;
+  h->iter_simple = c->iter_simple;
+  return c->status;
+}
+
+void free_all(ixb_handle* h) {
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  double** bufs[] = {&h->u[0], &h->u[1], &h->v[0], &h->v[1], &h->T[0], &h->T[1], &h->pc[0], &h->pc[1],
+                     &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu,
+                     &h->fcon[0], &h->fcon[1], &h->fcon[2], &h->flin[0], &h->flin[1], &h->flin[2],
+                     &h->metrics, &h->xp_d, &h->yp_d, &h->partials, &h->norms, &h->nu_d};
+  for (auto b : bufs) if (*b) cudaFree(*b);
+  if (h->bc) cudaFree(h->bc);
+  if (h->counters) cudaFree(h->counters);
+  if (h->ctl_d) cudaFree(h->ctl_d);
+  if (h->h_norms) cudaFreeHost(h->h_norms);
+  if (h->ctl_h) cudaFreeHost(h->ctl_h);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+// host Fortran array (rows x cols, column-major) <-> device padded field
+int put2d(ixb_handle* h, double* dst, const double* src, int rows, int cols) {
+  if (!src) return IXB_OK;
+  CK(cudaMemcpy2DAsync(dst, (size_t)h->LD * sizeof(double), src, (size_t)rows * sizeof(double),
+                       (size_t)rows * sizeof(double), cols, cudaMemcpyHostToDevice, h->stream));
+  return IXB_OK;
+}
+int get2d(ixb_handle* h, double* dst, const double* src, int rows, int cols) {
+  if (!dst) return IXB_OK;
+  CK(cudaMemcpy2DAsync(dst, (size_t)rows * sizeof(double), src, (size_t)h->LD * sizeof(double),
+                       (size_t)rows * sizeof(double), cols, cudaMemcpyDeviceToHost, h->stream));
+  return IXB_OK;
+}
+
+// effective per-line boundary rows of one side: later segments overwrite
+// earlier ones, as the sequential loop of impone_cond_frontera does
+void side_table(const ixb_bc_side& s, BCEntry* tab, int nlines) {
+  for (int L = 0; L < nlines; ++L) tab[L] = BCEntry{0.0, 0, 0};
+  for (int k = 0; k < s.ndivis && k < 15; ++k) {
+    const int t = s.type[k];
+    if (t != IXB_BC_DIRI && t != IXB_BC_NEUM) continue;
+    for (int L = s.index[k]; L <= s.index[k + 1]; ++L)
+      if (L >= 1 && L < nlines) tab[L] = BCEntry{s.value[k], t, 0};
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int ixb_version(void) { return 100; }
+
+const char* ixb_strerror(int s) {
+  switch (s) {
+    case IXB_OK: return "ok";
+    case IXB_EINVAL: return "invalid argument";
+    case IXB_ECUDA: return "CUDA runtime error";
+    case IXB_ENONFINITE: return "non-finite convergence norm";
+    case IXB_ETIMEOUT: return "bounded device wait expired";
+    case IXB_EBC: return "boundary table leaves a solved line without a boundary row";
+    case IXB_ESTATE: return "mesh, parameters or boundary tables not set";
+    case IXB_EIO: return "file read/parse/write error";
+    case IXB_ENOMEM: return "allocation failed";
+    default: return "unknown status";
+  }
+}
+
+int ixb_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
+  if (!out) return IXB_EINVAL;
+  *out = nullptr;
+  if (mi < 4 || nj < 4 || mi > 16384 || nj > 16384) return IXB_EINVAL;
+  if (prec_mode != IXB_PREC_FP64) return IXB_EINVAL;  // binary32 mode: see ixb_create_refined
+  ixb_handle* h = new (std::nothrow) ixb_handle();
+  if (!h) return IXB_ENOMEM;
+  h->mi = mi; h->nj = nj; h->prec = prec_mode;
+  h->LD = ((mi + 1) + 31) / 32 * 32;
+  h->rows = nj + 2;
+  h->fsz = (size_t)h->LD * h->rows;
+  auto fail = [&](int code) { free_all(h); delete h; return code; };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(IXB_ECUDA);
+  h->own_stream = true;
+  const size_t fb = h->fsz * sizeof(double);
+  double** fields[] = {&h->u[0], &h->u[1], &h->v[0], &h->v[1], &h->T[0], &h->T[1], &h->pc[0], &h->pc[1],
+                       &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu};
+  for (auto f : fields) {
+    if (cudaMalloc(f, fb) != cudaSuccess) return fail(IXB_ENOMEM);
+    if (cudaMemset(*f, 0, fb) != cudaSuccess) return fail(IXB_ECUDA);
+  }
+  // au = av = 1e40 (main.f90:309-310)
+  {
+    std::vector<double> big(h->fsz, 1.e40);
+    if (cudaMemcpy(h->au, big.data(), fb, cudaMemcpyHostToDevice) != cudaSuccess) return fail(IXB_ECUDA);
+    if (cudaMemcpy(h->av, big.data(), fb, cudaMemcpyHostToDevice) != cudaSuccess) return fail(IXB_ECUDA);
+  }
+  h->mstride = std::max(mi, nj) + 3;
+  if (cudaMalloc(&h->metrics, (size_t)M_COUNT * h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMalloc(&h->xp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMalloc(&h->yp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  h->bcstride = std::max(mi, nj) + 3;
+  if (cudaMalloc(&h->bc, (size_t)12 * h->bcstride * sizeof(BCEntry)) != cudaSuccess) return fail(IXB_ENOMEM);
+  cudaMemset(h->bc, 0, (size_t)12 * h->bcstride * sizeof(BCEntry));
+  h->pstride = std::max(max_sweep_lines(mi, nj), residual_grid(mi, nj)) + 32;
+  if (cudaMalloc(&h->partials, (size_t)N_COUNT * h->pstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMalloc(&h->counters, N_COUNT * sizeof(unsigned int)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMemset(h->counters, 0, N_COUNT * sizeof(unsigned int)) != cudaSuccess) return fail(IXB_ECUDA);
+  if (cudaMalloc(&h->norms, N_COUNT * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  cudaMemset(h->norms, 0, N_COUNT * sizeof(double));
+  if (cudaMalloc(&h->nu_d, 4 * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMalloc(&h->ctl_d, sizeof(Ctl)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMallocHost(&h->h_norms, N_COUNT * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMallocHost(&h->ctl_h, sizeof(Ctl)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (sweep_set_smem_limits() != cudaSuccess) return fail(IXB_ECUDA);
+  const char* env = std::getenv("IXB_NO_GRAPH");
+  if (env && env[0] == '1') h->use_graph = 0;
+  h->prm.p_update = 0.6;
+  h->prm.solver = IXB_SOLVER_HYBRID;
+  *out = h;
+  return IXB_OK;
+}
+
+int ixb_destroy(ixb_handle* h) {
+  if (!h) return IXB_EINVAL;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return IXB_OK;
+}
+
+int ixb_set_stream(ixb_handle* h, void* stream) {
+  if (!h) return IXB_EINVAL;
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  h->stream = (cudaStream_t)stream;
+  h->own_stream = false;
+  h->graph_dirty = true;
+  return IXB_OK;
+}
+
+int ixb_set_mesh(ixb_handle* h, const double* xu, const double* yv, const double* xp, const double* yp) {
+  if (!h || !xu || !yv || !xp || !yp) return IXB_EINVAL;
+  const int mi = h->mi, nj = h->nj, ms = h->mstride;
+  h->xu.assign(xu, xu + mi); h->yv.assign(yv, yv + nj);
+  h->xp.assign(xp, xp + mi + 1); h->yp.assign(yp, yp + nj + 1);
+  // 1-based views
+  auto XU = [&](int i) { return xu[i - 1]; };
+  auto YV = [&](int j) { return yv[j - 1]; };
+  auto XP = [&](int i) { return xp[i - 1]; };
+  auto YP = [&](int j) { return yp[j - 1]; };
+  std::vector<double> m((size_t)M_COUNT * ms, 0.0);
+  auto M = [&](int which, int k) -> double& { return m[(size_t)which * ms + k]; };
+  // lectura_mallas_escalonadas, source/mod_malla.f90:167-218
+  for (int ii = 2; ii <= mi; ++ii) M(M_DXP, ii) = XU(ii) - XU(ii - 1);
+  for (int jj = 2; jj <= nj; ++jj) M(M_DYP, jj) = YV(jj) - YV(jj - 1);
+  for (int ii = 1; ii <= mi; ++ii) M(M_DXU, ii) = XP(ii + 1) - XP(ii);
+  for (int jj = 2; jj <= nj; ++jj) M(M_DYU, jj) = YV(jj) - YV(jj - 1);
+  for (int ii = 2; ii <= mi; ++ii) M(M_DXV, ii) = XU(ii) - XU(ii - 1);
+  for (int jj = 1; jj <= nj; ++jj) M(M_DYV, jj) = YP(jj + 1) - YP(jj);
+  for (int ii = 1; ii <= mi; ++ii) M(M_FEXP, ii) = (XP(ii + 1) - XU(ii)) / (XP(ii + 1) - XP(ii));
+  for (int jj = 1; jj <= nj; ++jj) M(M_FEYP, jj) = (YP(jj + 1) - YV(jj)) / (YP(jj + 1) - YP(jj));
+  for (int ii = 1; ii <= mi - 1; ++ii) M(M_FEXU, ii) = (XU(ii + 1) - XP(ii + 1)) / (XU(ii + 1) - XU(ii));
+  for (int jj = 1; jj <= nj - 1; ++jj) M(M_FEYV, jj) = (YV(jj + 1) - YP(jj + 1)) / (YV(jj + 1) - YV(jj));
+  CK(cudaMemcpyAsync(h->metrics, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  std::vector<double> xp1(ms, 0.0), yp1(ms, 0.0);
+  for (int i = 1; i <= mi + 1; ++i) xp1[i] = XP(i);
+  for (int j = 1; j <= nj + 1; ++j) yp1[j] = YP(j);
+  CK(cudaMemcpyAsync(h->xp_d, xp1.data(), ms * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->yp_d, yp1.data(), ms * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->has_mesh = true;
+  return IXB_OK;
+}
+
+int ixb_set_params(ixb_handle* h, const ixb_params* p) {
+  if (!h || !p) return IXB_EINVAL;
+  if (p->solver != IXB_SOLVER_HYBRID && p->solver != IXB_SOLVER_EXACT) return IXB_EINVAL;
+  if (!(p->dt != 0.0) || !(p->rel_vel != 0.0) || !(p->rel_pres != 0.0) || !(p->rel_ener != 0.0)) return IXB_EINVAL;
+  h->prm = *p;
+  h->has_params = true;
+  h->graph_dirty = true;
+  return IXB_OK;
+}
+
+int ixb_set_bc(ixb_handle* h, int var, const ixb_bc_side sides[4]) {
+  if (!h || !sides || var < 0 || var > 2) return IXB_EINVAL;
+  const int mi = h->mi, nj = h->nj, S = h->bcstride;
+  std::vector<BCEntry> tab((size_t)4 * S);
+  for (int k = 0; k < 4; ++k) {
+    const ixb_bc_side& s = sides[k];
+    if (s.side < 0 || s.side > 3 || s.ndivis < 0 || s.ndivis > 15) return IXB_EINVAL;
+  }
+  for (int side = 0; side < 4; ++side) {
+    // a side entry may appear anywhere in the array; the last one for a side wins
+    const ixb_bc_side* s = nullptr;
+    for (int k = 0; k < 4; ++k) if (sides[k].side == side) s = &sides[k];
+    BCEntry* t = tab.data() + (size_t)side * S;
+    if (s) side_table(*s, t, S);
+    else for (int L = 0; L < S; ++L) t[L] = BCEntry{0.0, 0, 0};
+    // solved lines of this side: x-lines (a, c) and y-lines (b, d) of the variable
+    int lo = 2, hi;
+    const bool xside = (side == 0 || side == 2);
+    if (var == 0) hi = xside ? nj : mi - 1;       // u: x-lines jj=2..nj, y-lines ii=2..mi-1
+    else if (var == 1) hi = xside ? nj - 1 : mi;  // v: jj=2..nj-1, ii=2..mi
+    else hi = xside ? nj : mi;                    // T: jj=2..nj, ii=2..mi
+    for (int L = lo; L <= hi; ++L)
+      if (t[L].type != IXB_BC_DIRI && t[L].type != IXB_BC_NEUM) return IXB_EBC;
+  }
+  CK(cudaMemcpyAsync(h->bc + (size_t)var * 4 * S, tab.data(), tab.size() * sizeof(BCEntry),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->has_bc[var] = true;
+  return IXB_OK;
+}
+
+int ixb_set_sources(ixb_handle* h, int var, const double* fcon, const double* flin) {
+  if (!h || var < 0 || var > 2) return IXB_EINVAL;
+  const int rows = var == 0 ? h->mi : h->mi + 1;
+  const int cols = var == 1 ? h->nj : h->nj + 1;
+  const size_t fb = h->fsz * sizeof(double);
+  double** pc[2] = {&h->fcon[var], &h->flin[var]};
+  const double* src[2] = {fcon, flin};
+  for (int k = 0; k < 2; ++k) {
+    if (!src[k]) {
+      if (*pc[k]) { cudaFree(*pc[k]); *pc[k] = nullptr; }
+      continue;
+    }
+    if (!*pc[k]) {
+      if (cudaMalloc(pc[k], fb) != cudaSuccess) return IXB_ENOMEM;
+      CK(cudaMemset(*pc[k], 0, fb));
+    }
+    TRY(put2d(h, *pc[k], src[k], rows, cols));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  h->graph_dirty = true;
+  return IXB_OK;
+}
+
+int ixb_upload_state(ixb_handle* h, const double* u, const double* v, const double* p, const double* T,
+                     const double* u_ant, const double* v_ant, const double* T_ant) {
+  if (!h) return IXB_EINVAL;
+  const int mi = h->mi, nj = h->nj;
+  TRY(put2d(h, h->u[h->cu], u, mi, nj + 1));
+  TRY(put2d(h, h->v[h->cv], v, mi + 1, nj));
+  TRY(put2d(h, h->p, p, mi + 1, nj + 1));
+  TRY(put2d(h, h->T[h->cT], T, mi + 1, nj + 1));
+  TRY(put2d(h, h->u_ant, u_ant, mi, nj + 1));
+  TRY(put2d(h, h->v_ant, v_ant, mi + 1, nj));
+  TRY(put2d(h, h->T_ant, T_ant, mi + 1, nj + 1));
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+int ixb_download_state(ixb_handle* h, double* u, double* v, double* p, double* T, double* u_ant, double* v_ant,
+                       double* T_ant) {
+  if (!h) return IXB_EINVAL;
+  const int mi = h->mi, nj = h->nj;
+  TRY(get2d(h, u, h->u[h->cu], mi, nj + 1));
+  TRY(get2d(h, v, h->v[h->cv], mi + 1, nj));
+  TRY(get2d(h, p, h->p, mi + 1, nj + 1));
+  TRY(get2d(h, T, h->T[h->cT], mi + 1, nj + 1));
+  TRY(get2d(h, u_ant, h->u_ant, mi, nj + 1));
+  TRY(get2d(h, v_ant, h->v_ant, mi + 1, nj));
+  TRY(get2d(h, T_ant, h->T_ant, mi + 1, nj + 1));
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+int ixb_download_aux(ixb_handle* h, double* au, double* av, double* b_o, double* resu, double* corr_pres) {
+  if (!h) return IXB_EINVAL;
+  const int mi = h->mi, nj = h->nj;
+  TRY(get2d(h, au, h->au, mi, nj + 1));
+  TRY(get2d(h, av, h->av, mi + 1, nj));
+  TRY(get2d(h, b_o, h->b_o, mi + 1, nj + 1));
+  TRY(get2d(h, resu, h->resu, mi, nj + 1));
+  TRY(get2d(h, corr_pres, h->pc[h->cpc], mi + 1, nj + 1));
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+int ixb_set_work(ixb_handle* h, const double* corr_pres, const double* au, const double* av) {
+  if (!h) return IXB_EINVAL;
+  const int mi = h->mi, nj = h->nj;
+  TRY(put2d(h, h->pc[h->cpc], corr_pres, mi + 1, nj + 1));
+  TRY(put2d(h, h->au, au, mi, nj + 1));
+  TRY(put2d(h, h->av, av, mi + 1, nj));
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+static void rep_clear(ixb_report* r) { std::memset(r, 0, sizeof(*r)); }
+
+int ixb_simple_iterations(ixb_handle* h, int n, ixb_report* rep) {
+  TRY(ready(h));
+  if (n < 0) return IXB_EINVAL;
+  ixb_report local;
+  ixb_report* r = rep ? rep : &local;
+  rep_clear(r);
+  if (n == 0) return IXB_OK;
+  int st;
+  if (h->use_graph) {
+    st = run_graph(h, n, r);
+  } else {
+    st = IXB_OK;
+    int code = 0;
+    for (int k = 0; k < n && st == IXB_OK; ++k) st = body_host(h, false, r, &code);
+    if (st == IXB_OK) CK(cudaStreamSynchronize(h->stream));
+  }
+  r->status = st;
+  return st;
+}
+
+int ixb_simple_loop(ixb_handle* h, ixb_report* rep) {
+  TRY(ready(h));
+  ixb_report local;
+  ixb_report* r = rep ? rep : &local;
+  rep_clear(r);
+  int st;
+  if (h->use_graph) {
+    st = run_graph(h, 0, r);
+  } else {
+    st = IXB_OK;
+    int code = 0;
+    while (st == IXB_OK) {
+      st = body_host(h, true, r, &code);
+      if (code != 0) break;
+    }
+    r->exit_code = code;
+  }
+  r->status = st;
+  return st;
+}
+
+int ixb_roll(ixb_handle* h) {
+  if (!h) return IXB_EINVAL;
+  const size_t fb = h->fsz * sizeof(double);
+  CK(cudaMemcpyAsync(h->T_ant, h->T[h->cT], fb, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->u_ant, h->u[h->cu], fb, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->v_ant, h->v[h->cv], fb, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+int ixb_step(ixb_handle* h, ixb_report* rep) {
+  TRY(ixb_simple_loop(h, rep));
+  return ixb_roll(h);
+}
+
+int ixb_phase(ixb_handle* h, int which) {
+  TRY(ready(h));
+  int st = IXB_OK;
+  switch (which) {
+    case 0: st = sweep(h, EQ_UY, nullptr, false); break;
+    case 1: st = sweep(h, EQ_UX, nullptr, false); break;
+    case 2: st = sweep(h, EQ_VY, nullptr, false); break;
+    case 3: st = sweep(h, EQ_VX, nullptr, false); break;
+    case 4: st = sweep(h, EQ_PY, nullptr, false); break;
+    case 5: st = sweep(h, EQ_PX, nullptr, false); break;
+    case 6: st = correct(h); break;
+    case 7: st = sweep(h, EQ_TY, nullptr, false); break;
+    case 8: st = sweep(h, EQ_TX, nullptr, false); break;
+    case 9: st = residual(h); break;
+    default: return IXB_EINVAL;
+  }
+  if (st != IXB_OK) return st;
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms) {
+  TRY(ready(h));
+  if (reps < 1 || !ms) return IXB_EINVAL;
+  void* flush = nullptr;
+  if (flush_bytes > 0 && cudaMalloc(&flush, flush_bytes) != cudaSuccess) return IXB_ENOMEM;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int st = IXB_OK;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) st = IXB_ECUDA;
+  for (int k = 0; k < 10 && st == IXB_OK; ++k) {
+    auto launch = [&]() -> int {
+      switch (k) {
+        case 0: return sweep(h, EQ_UY, nullptr, false);
+        case 1: return sweep(h, EQ_UX, nullptr, false);
+        case 2: return sweep(h, EQ_VY, nullptr, false);
+        case 3: return sweep(h, EQ_VX, h->v[h->cv ^ 1], true);
+        case 4: return sweep(h, EQ_PY, nullptr, false);
+        case 5: return sweep(h, EQ_PX, h->pc[h->cpc ^ 1], true);
+        case 6: return correct(h);
+        case 7: return sweep(h, EQ_TY, nullptr, false);
+        case 8: return sweep(h, EQ_TX, h->T[h->cT ^ 1], true);
+        default: return residual(h);
+      }
+    };
+    st = launch();  // warm-up (module load, first-touch)
+    double total = 0.0;
+    for (int r = 0; r < reps && st == IXB_OK; ++r) {
+      if (flush && cudaMemsetAsync(flush, r & 0xff, flush_bytes, h->stream) != cudaSuccess) { st = IXB_ECUDA; break; }
+      if (cudaEventRecord(e0, h->stream) != cudaSuccess) { st = IXB_ECUDA; break; }
+      st = launch();
+      if (st != IXB_OK) break;
+      if (cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+        st = IXB_ECUDA;
+        break;
+      }
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      total += t;
+    }
+    ms[k] = total / reps;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (flush) cudaFree(flush);
+  return st;
+}
+
+static int nusselt(ixb_handle* h, int vertical, int k0, int k1, double* nu0, double* nu1) {
+  if (!h || !h->has_mesh) return IXB_ESTATE;
+  const int n_along = vertical ? h->nj + 1 : h->mi + 1;
+  if (k0 < 1 || k1 < k0) return IXB_EINVAL;
+  for (int k = k0; k <= k1; k += 2)
+    if (k + 2 > n_along) return IXB_EINVAL;
+  Geo<double> G = make_geo(h);
+  CK(launch_nusselt_f64(G, h->T[h->cT], h->xp_d, h->yp_d, vertical, k0, k1, h->nu_d, h->stream));
+  double out[2];
+  CK(cudaMemcpyAsync(out, h->nu_d, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (nu0) *nu0 = out[0];
+  if (nu1) *nu1 = out[1];
+  return IXB_OK;
+}
+
+int ixb_nusselt_y(ixb_handle* h, int i0, int i1, double* nu0, double* nu1) { return nusselt(h, 0, i0, i1, nu0, nu1); }
+int ixb_nusselt_x(ixb_handle* h, int j0, int j1, double* nu0, double* nu1) { return nusselt(h, 1, j0, j1, nu0, nu1); }
+
+int ixb_tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n, int nsys,
+                    int layout, int solver, void* stream) {
+  if (!a || !b || !c || !d || !x || n < 1 || nsys < 1 || (layout != 0 && layout != 1)) return IXB_EINVAL;
+  if (solver != IXB_SOLVER_HYBRID && solver != IXB_SOLVER_EXACT) return IXB_EINVAL;
+  cudaError_t e = tridiag_f64(a, b, c, d, x, n, nsys, layout, solver, (cudaStream_t)stream);
+  if (e == cudaErrorInvalidValue) return IXB_EINVAL;
+  return e == cudaSuccess ? IXB_OK : IXB_ECUDA;
+}
+
+int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float* d, float* x, int n, int nsys,
+                    int layout, int solver, void* stream) {
+  if (!a || !b || !c || !d || !x || n < 1 || nsys < 1 || (layout != 0 && layout != 1)) return IXB_EINVAL;
+  if (solver != IXB_SOLVER_HYBRID && solver != IXB_SOLVER_EXACT) return IXB_EINVAL;
+  cudaError_t e = tridiag_f32(a, b, c, d, x, n, nsys, layout, solver, (cudaStream_t)stream);
+  if (e == cudaErrorInvalidValue) return IXB_EINVAL;
+  return e == cudaSuccess ? IXB_OK : IXB_ECUDA;
+}
+
+}  // extern "C"

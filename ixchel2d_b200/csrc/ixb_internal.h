@@ -1,0 +1,49 @@
+// ixb_internal.h -- host-side declarations shared by the library's
+// translation units (not part of the public ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ixb.h"
+#include "ixb_device.cuh"
+
+namespace ixb {
+
+enum NormId { N_DV = 0, N_DP, N_BO, N_DT, N_RES, N_COUNT };
+
+// launch shape of one sweep
+struct SweepShape {
+  int n;          // rows per line
+  int line_lo;    // first solved line (1-based)
+  int line_hi;    // last solved line
+  int nfull;      // lines of the field (unsolved ones are copied)
+  int tl;         // lines per CTA
+  int nt;         // threads per CTA
+  int m, mp;      // chunk rows per lane, padded pitch
+  size_t smem;    // dynamic shared memory bytes
+  int grid;       // CTAs
+};
+
+SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl_override, int nt_override);
+int max_sweep_lines(int mi, int nj);
+
+// kernel launchers (ixb_kernels.cu); return cudaError_t
+cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
+                             const SweepIO<double>& io, cudaStream_t st);
+cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
+                               const double* au, const double* av, cudaStream_t st);
+cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const double* v, const double* T,
+                                const double* p, const double* u_ant, const double* fcon, const double* flin,
+                                double* resu, NormSlot ns, cudaStream_t st);
+int residual_grid(int mi, int nj);
+cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,
+                               int vertical, int k0, int k1, double* out2, cudaStream_t st);
+cudaError_t sweep_set_smem_limits();
+
+// batched standalone tridiagonal solvers (ixb_tridiag.cu)
+cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,
+                        int nsys, int layout, int solver, cudaStream_t st);
+cudaError_t tridiag_f32(const float* a, const float* b, const float* c, const float* d, float* x, int n,
+                        int nsys, int layout, int solver, cudaStream_t st);
+
+}  // namespace ixb

@@ -1,0 +1,174 @@
+// ixb_tridiag.cu -- batched tridiagonal solves over device arrays, the
+// batched form of tridiagonal (source/mod_solucionador.f90:25-47).
+//
+// layout 0 (each system contiguous, like the reference's x-lines): a CTA
+// stages TL systems into shared memory with coalesced loads, one warp per
+// system solves (exact sequential Thomas or the warp Thomas-PCR hybrid),
+// and the solution is written back coalesced.
+//
+// layout 1 (systems interleaved, row i of system s at i*nsys+s, like the
+// y-lines of a column-major field): one thread per system walks the rows;
+// consecutive threads touch consecutive addresses.  The forward sweep keeps
+// its modified diagonal (exact) or normalised super-diagonal (hybrid) in a
+// scratch array of n*nsys elements taken from the stream-ordered allocator,
+// and the modified right-hand side in x.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ixb_internal.h"
+
+namespace ixb {
+
+template <class R, int SOLVER, int TL>
+__global__ void __launch_bounds__(256) tri_contig_kernel(const R* __restrict__ a, const R* __restrict__ b,
+                                                         const R* __restrict__ c, const R* __restrict__ d,
+                                                         R* x, int n, int nsys, int m, int mp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sm = reinterpret_cast<R*>(smem_raw);
+  const int npad = 32 * m, chunk = 32 * mp;
+  const long long s0 = (long long)blockIdx.x * TL;
+  for (int idx = threadIdx.x; idx < TL * npad; idx += blockDim.x) {
+    const int l = idx / npad, r = idx - l * npad;
+    const long long s = s0 + l;
+    if (s >= nsys) continue;
+    R ra = R(0), rb = R(1), rc = R(0), rd = R(0);
+    if (r < n) {
+      const size_t g = (size_t)s * n + r;
+      ra = r == 0 ? R(0) : a[g];
+      rb = b[g];
+      rc = r == n - 1 ? R(0) : c[g];
+      rd = d[g];
+    }
+    const int lane = r / m;
+    const int o = lane * mp + (r - lane * m);
+    R* base = sm + l * 4 * chunk;
+    base[o] = ra; base[chunk + o] = rb; base[2 * chunk + o] = rc; base[3 * chunk + o] = rd;
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5;
+  if (w < TL && s0 + w < nsys) {
+    R* base = sm + w * 4 * chunk;
+    if (SOLVER == IXB_SOLVER_EXACT) {
+      if ((threadIdx.x & 31) == 0) thomas_exact(base, base + chunk, base + 2 * chunk, base + 3 * chunk, n, m, mp);
+    } else {
+      thomas_pcr_warp(base, base + chunk, base + 2 * chunk, base + 3 * chunk, m, mp);
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < TL * n; idx += blockDim.x) {
+    const int l = idx / n, r = idx - l * n;
+    const long long s = s0 + l;
+    if (s >= nsys) continue;
+    const int lane = r / m;
+    x[(size_t)s * n + r] = sm[l * 4 * chunk + 3 * chunk + lane * mp + (r - lane * m)];
+  }
+}
+
+// One thread per interleaved system.  EXACT keeps the reference's operation
+// order (modified diagonal in `work`); HYBRID uses the normalised Thomas form
+// (c' in `work`).
+template <class R, int SOLVER>
+__global__ void __launch_bounds__(128) tri_inter_kernel(const R* __restrict__ a, const R* __restrict__ b,
+                                                        const R* __restrict__ c, const R* __restrict__ d, R* x,
+                                                        R* __restrict__ work, int n, int nsys) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  const size_t S = (size_t)nsys;
+  if (SOLVER == IXB_SOLVER_EXACT) {
+    R bp = b[s], dp = d[s];
+    work[s] = bp;
+    x[s] = dp;
+    for (int i = 1; i < n; ++i) {
+      const size_t g = (size_t)i * S + s;
+      const R q = a[g] / bp;
+      dp = d[g] - q * dp;
+      bp = b[g] - q * c[g - S];
+      x[g] = dp;
+      work[g] = bp;
+    }
+    R xn = dp / bp;
+    x[(size_t)(n - 1) * S + s] = xn;
+    for (int i = n - 2; i >= 0; --i) {
+      const size_t g = (size_t)i * S + s;
+      xn = (x[g] - c[g] * xn) / work[g];
+      x[g] = xn;
+    }
+  } else {
+    R r = R(1) / b[s];
+    R cp = (n > 1 ? c[s] : R(0)) * r;
+    R dp = d[s] * r;
+    work[s] = cp;
+    x[s] = dp;
+    for (int i = 1; i < n; ++i) {
+      const size_t g = (size_t)i * S + s;
+      const R ai = a[g];
+      r = R(1) / (b[g] - ai * cp);
+      dp = (d[g] - ai * dp) * r;
+      cp = (i < n - 1 ? c[g] : R(0)) * r;
+      x[g] = dp;
+      work[g] = cp;
+    }
+    R xn = dp;
+    for (int i = n - 2; i >= 0; --i) {
+      const size_t g = (size_t)i * S + s;
+      xn = x[g] - work[g] * xn;
+      x[g] = xn;
+    }
+  }
+}
+
+template <class R, int SOLVER, int TL>
+static cudaError_t contig_tl(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, int m, int mp,
+                             size_t smem, cudaStream_t st) {
+  auto k = tri_contig_kernel<R, SOLVER, TL>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int grid = (nsys + TL - 1) / TL;
+  const int nt = std::max(128, 32 * TL);
+  k<<<grid, nt, smem, st>>>(a, b, c, d, x, n, nsys, m, mp);
+  return cudaGetLastError();
+}
+
+template <class R, int SOLVER>
+static cudaError_t tridiag_impl(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, int layout,
+                                cudaStream_t st) {
+  if (layout == 0) {
+    const int m = std::max(3, (n + 31) / 32);
+    const int mp = m | 1;
+    const size_t per = (size_t)4 * 32 * mp * sizeof(R);
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (per > (size_t)optin) return cudaErrorInvalidValue;  // line too long for one CTA
+    int tl = 1;
+    while (tl < 8 && per * tl * 2 <= 96 * 1024 && tl * 2 <= nsys) tl *= 2;
+    switch (tl) {
+      case 1: return contig_tl<R, SOLVER, 1>(a, b, c, d, x, n, nsys, m, mp, per, st);
+      case 2: return contig_tl<R, SOLVER, 2>(a, b, c, d, x, n, nsys, m, mp, per * 2, st);
+      case 4: return contig_tl<R, SOLVER, 4>(a, b, c, d, x, n, nsys, m, mp, per * 4, st);
+      default: return contig_tl<R, SOLVER, 8>(a, b, c, d, x, n, nsys, m, mp, per * 8, st);
+    }
+  }
+  R* work = nullptr;
+  cudaError_t e = cudaMallocAsync((void**)&work, (size_t)n * nsys * sizeof(R), st);
+  if (e != cudaSuccess) return e;
+  tri_inter_kernel<R, SOLVER><<<(nsys + 127) / 128, 128, 0, st>>>(a, b, c, d, x, work, n, nsys);
+  e = cudaGetLastError();
+  cudaError_t e2 = cudaFreeAsync(work, st);
+  return e != cudaSuccess ? e : e2;
+}
+
+cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,
+                        int nsys, int layout, int solver, cudaStream_t st) {
+  if (solver == IXB_SOLVER_EXACT) return tridiag_impl<double, IXB_SOLVER_EXACT>(a, b, c, d, x, n, nsys, layout, st);
+  return tridiag_impl<double, IXB_SOLVER_HYBRID>(a, b, c, d, x, n, nsys, layout, st);
+}
+
+cudaError_t tridiag_f32(const float* a, const float* b, const float* c, const float* d, float* x, int n, int nsys,
+                        int layout, int solver, cudaStream_t st) {
+  if (solver == IXB_SOLVER_EXACT) return tridiag_impl<float, IXB_SOLVER_EXACT>(a, b, c, d, x, n, nsys, layout, st);
+  return tridiag_impl<float, IXB_SOLVER_HYBRID>(a, b, c, d, x, n, nsys, layout, st);
+}
+
+}  // namespace ixb

@@ -1,0 +1,146 @@
+"""Python view of one libixb handle: the SIMPLE hot path of Ixchel2D on one
+GPU, driven through the C ABI (include/ixb.h)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _ffi as F
+from .cases import Case, shapes
+
+
+def _f64(a) -> np.ndarray:
+    return np.asfortranarray(a, dtype=np.float64)
+
+
+class Simple2D:
+    """Owns an ixb handle (device memory + stream) for an (mi, nj) grid."""
+
+    def __init__(self, mi: int, nj: int, prec: int = F.PREC_FP64):
+        self.mi, self.nj = mi, nj
+        h = C.c_void_p()
+        F.check(F.lib.ixb_create(mi, nj, prec, C.byref(h)), "ixb_create")
+        self.h = h
+        self._shapes = shapes(mi, nj)
+
+    # ---- setup ----
+    def set_mesh(self, xu, yv, xp, yp):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (xu, yv, xp, yp)]
+        F.check(F.lib.ixb_set_mesh(self.h, *map(F.dptr, arrs)), "ixb_set_mesh")
+
+    def set_params(self, **kw):
+        p = F.Params()
+        for k, v in kw.items():
+            setattr(p, k, v)
+        F.check(F.lib.ixb_set_params(self.h, C.byref(p)), "ixb_set_params")
+
+    def set_bc(self, var: int, sides):
+        arr = (F.BCSide * 4)(*sides)
+        F.check(F.lib.ixb_set_bc(self.h, var, arr), "ixb_set_bc")
+
+    def set_sources(self, var: int, fcon=None, flin=None):
+        fc = None if fcon is None else _f64(fcon)
+        fl = None if flin is None else _f64(flin)
+        F.check(F.lib.ixb_set_sources(self.h, var, F.dptr(fc), F.dptr(fl)), "ixb_set_sources")
+
+    def upload(self, state: dict):
+        keys = ("u", "v", "p", "T", "u_ant", "v_ant", "T_ant")
+        arrs = [None if state.get(k) is None else _f64(state[k]) for k in keys]
+        for k, a in zip(keys, arrs):
+            if a is not None and a.shape != self._shapes[k]:
+                raise ValueError(f"{k}: shape {a.shape} != {self._shapes[k]}")
+        F.check(F.lib.ixb_upload_state(self.h, *map(F.dptr, arrs)), "ixb_upload_state")
+
+    def download(self) -> dict:
+        out = {k: np.zeros(s, order="F") for k, s in self._shapes.items()}
+        keys = ("u", "v", "p", "T", "u_ant", "v_ant", "T_ant")
+        F.check(F.lib.ixb_download_state(self.h, *[F.dptr(out[k]) for k in keys]), "ixb_download_state")
+        return out
+
+    def download_aux(self) -> dict:
+        mi, nj = self.mi, self.nj
+        out = {"au": np.zeros((mi, nj + 1), order="F"), "av": np.zeros((mi + 1, nj), order="F"),
+               "b_o": np.zeros((mi + 1, nj + 1), order="F"), "Resu": np.zeros((mi, nj + 1), order="F"),
+               "corr_pres": np.zeros((mi + 1, nj + 1), order="F")}
+        F.check(F.lib.ixb_download_aux(self.h, *[F.dptr(out[k]) for k in ("au", "av", "b_o", "Resu", "corr_pres")]),
+                "ixb_download_aux")
+        return out
+
+    def set_work(self, corr_pres=None, au=None, av=None):
+        a = [None if x is None else _f64(x) for x in (corr_pres, au, av)]
+        F.check(F.lib.ixb_set_work(self.h, *map(F.dptr, a)), "ixb_set_work")
+
+    @classmethod
+    def from_case(cls, case: Case, prec: int = F.PREC_FP64, **param_over) -> "Simple2D":
+        s = cls(case.mi, case.nj, prec)
+        s.set_mesh(case.xu, case.yv, case.xp, case.yp)
+        prm = dict(case.params)
+        prm.update(param_over)
+        s.set_params(**prm)
+        for var, sides in case.bc.items():
+            s.set_bc(var, sides)
+        for var, (fc, fl) in case.sources.items():
+            s.set_sources(var, fc, fl)
+        s.upload(case.state)
+        return s
+
+    # ---- hot path ----
+    def iterations(self, n: int) -> dict:
+        r = F.Report()
+        F.check(F.lib.ixb_simple_iterations(self.h, n, C.byref(r)), "ixb_simple_iterations")
+        return r.as_dict()
+
+    def loop(self) -> dict:
+        r = F.Report()
+        F.check(F.lib.ixb_simple_loop(self.h, C.byref(r)), "ixb_simple_loop")
+        return r.as_dict()
+
+    def step(self) -> dict:
+        r = F.Report()
+        F.check(F.lib.ixb_step(self.h, C.byref(r)), "ixb_step")
+        return r.as_dict()
+
+    def roll(self):
+        F.check(F.lib.ixb_roll(self.h), "ixb_roll")
+
+    def phase(self, which: int):
+        F.check(F.lib.ixb_phase(self.h, which), "ixb_phase")
+
+    def time_phases(self, reps: int = 20, flush_bytes: int = 0) -> list[float]:
+        """Mean device milliseconds per launch of each phase 0..9 (advances the state);
+        flush_bytes > 0 writes that many bytes before every launch (cold L2)."""
+        ms = np.zeros(10)
+        F.check(F.lib.ixb_time_phases(self.h, reps, flush_bytes, F.dptr(ms)), "ixb_time_phases")
+        return ms.tolist()
+
+    def nusselt_x(self, j0: int, j1: int):
+        a, b = C.c_double(), C.c_double()
+        F.check(F.lib.ixb_nusselt_x(self.h, j0, j1, C.byref(a), C.byref(b)), "ixb_nusselt_x")
+        return a.value, b.value
+
+    def nusselt_y(self, i0: int, i1: int):
+        a, b = C.c_double(), C.c_double()
+        F.check(F.lib.ixb_nusselt_y(self.h, i0, i1, C.byref(a), C.byref(b)), "ixb_nusselt_y")
+        return a.value, b.value
+
+    def set_stream(self, stream_handle: int):
+        """Launch on an external cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
+        F.check(F.lib.ixb_set_stream(self.h, C.c_void_p(stream_handle)), "ixb_set_stream")
+
+    def close(self):
+        if getattr(self, "h", None):
+            F.lib.ixb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
