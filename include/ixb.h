@@ -105,7 +105,8 @@ const char* ixb_strerror(int status);
 int ixb_device_count(void);
 
 /* ---- handle lifetime: replaces the `!$acc data` region of main.f90:356-389 ---- */
-/* mi, nj: the grid sizes of source/mod_malla.f90:15, here chosen at run time. */
+/* mi, nj: the grid sizes of source/mod_malla.f90:15, here chosen at run time
+ * (4 <= mi, nj <= 6000). */
 int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out);
 int ixb_destroy(ixb_handle* h);
 /* Use an external CUDA stream (cudaStream_t) instead of the handle's own. */
@@ -158,6 +159,21 @@ int ixb_phase(ixb_handle* h, int which);
  * launches (use on a scratch copy).  No reference counterpart: it measures
  * the kernels that replace the OpenACC regions. */
 int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
+/* Launch shape of one sweep (0..7 = u-y, u-x, v-y, v-x, p'-y, p'-x, T-y,
+ * T-x): lines per CTA and threads per line, one of (1,128) (1,256) (2,64)
+ * (2,128) (4,32) (4,64) (8,32); each thread eliminates a chunk of
+ * max(3, ceil(n/threads_per_line)) rows.  lines_per_cta = 0 restores the
+ * default (the fewest waves of resident CTAs, then the shortest chunks).
+ * No reference counterpart: the reference runs one sequential tridiagonal
+ * per OpenACC gang. */
+int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads_per_line);
+/* Autotuner for the launch shapes: for every sweep, times each candidate
+ * shape `reps` times on the current state (a scratch buffer of flush_bytes
+ * is written before every timed launch when flush_bytes > 0) and keeps the
+ * fastest.  The state is restored afterwards.  chosen[2k], chosen[2k+1]
+ * receive sweep k's lines per CTA and threads per line; ms[k] its mean
+ * milliseconds per launch (either may be NULL). */
+int ixb_autotune(ixb_handle* h, int reps, size_t flush_bytes, int* chosen, double* ms);
 /* Overwrite corr_pres / au / av on the device (host arrays), for ixb_phase checks. */
 int ixb_set_work(ixb_handle* h, const double* corr_pres, const double* au, const double* av);
 

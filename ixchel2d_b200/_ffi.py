@@ -81,6 +81,8 @@ SIGNATURES = [
     ("ixb_phase", C.c_int, [_vp, C.c_int]),
     ("ixb_set_work", C.c_int, [_vp, _dp, _dp, _dp]),
     ("ixb_time_phases", C.c_int, [_vp, C.c_int, C.c_size_t, _dp]),
+    ("ixb_set_sweep_shape", C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+    ("ixb_autotune", C.c_int, [_vp, C.c_int, C.c_size_t, C.POINTER(C.c_int), _dp]),
     ("ixb_nusselt_y", C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp]),
     ("ixb_nusselt_x", C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp]),
     ("ixb_tridiag_f64", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),

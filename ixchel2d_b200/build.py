@@ -76,6 +76,9 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> Path:
             for obj, log in ex.map(lambda j: _compile(j[0], j[1], extra), jobs):
                 if verbose or ptxas_v:
                     print(f"[ixb build] {obj.name}\n{log}", file=sys.stderr)
+    for stale in BUILD.glob("*.o"):
+        if stale not in objs:
+            stale.unlink()
     newest_obj = max(o.stat().st_mtime for o in objs)
     if jobs or not LIB.exists() or LIB.stat().st_mtime < newest_obj:
         tmp = LIB.with_suffix(".so.tmp")

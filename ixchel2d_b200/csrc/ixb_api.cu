@@ -64,6 +64,8 @@ struct ixb_handle {
   // mesh
   double* metrics = nullptr;
   int mstride = 0;
+  double* tables = nullptr;  // T_COUNT mesh-constant 2-D tables
+  bool tables_dirty = true;
   double *xp_d = nullptr, *yp_d = nullptr;
   std::vector<double> xu, yv, xp, yp;
   // boundary tables [var][side][line]
@@ -87,8 +89,9 @@ struct ixb_handle {
   bool has_mesh = false, has_params = false, has_bc[3] = {false, false, false};
   int iter_ecuaci = 0, iter_simple = 0;
   int use_graph = 1;
-  int tl_override[EQ_COUNT] = {};
-  int nt_override[EQ_COUNT] = {};
+  int shape_tl[EQ_COUNT] = {};  // launch shape per sweep (0 = not chosen yet)
+  int shape_g[EQ_COUNT] = {};
+  int nsm = 148;
 };
 
 namespace {
@@ -96,6 +99,7 @@ namespace {
 Geo<double> make_geo(const ixb_handle* h) {
   Geo<double> G{};
   G.mi = h->mi; G.nj = h->nj; G.LD = h->LD; G.mstride = h->mstride; G.m = h->metrics;
+  G.tstride = h->fsz; G.tab = h->tables;
   G.gm = h->prm.gamma_momen; G.ge = h->prm.gamma_energ; G.Ri = h->prm.Ri; G.Riy = h->prm.Riy;
   G.dt = h->prm.dt; G.rel_vel = h->prm.rel_vel; G.rel_pres = h->prm.rel_pres; G.rel_ener = h->prm.rel_ener;
   G.p_update = h->prm.p_update;
@@ -106,21 +110,55 @@ NormSlot slot(ixb_handle* h, int k) {
   return NormSlot{h->partials + (size_t)k * h->pstride, h->counters + k, h->norms + k};
 }
 
-int ready(const ixb_handle* h) {
+int ensure_tables(ixb_handle* h);
+
+int ready(ixb_handle* h) {
   if (!h) return IXB_EINVAL;
   if (!h->has_mesh || !h->has_params || !h->has_bc[0] || !h->has_bc[1] || !h->has_bc[2]) return IXB_ESTATE;
+  return ensure_tables(h);
+}
+
+// (Re)build the mesh-constant tables after a mesh or diffusivity change.
+int ensure_tables(ixb_handle* h) {
+  if (!h->tables_dirty) return IXB_OK;
+  Geo<double> G = make_geo(h);
+  CK(launch_tables_f64(G, h->metrics, h->tables, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->tables_dirty = false;
   return IXB_OK;
+}
+
+const int kShapes[7][2] = {{1, 128}, {1, 256}, {2, 64}, {2, 128}, {4, 32}, {4, 64}, {8, 32}};
+
+// Default launch shape of a sweep: the fewest waves of CTAs (every CTA
+// resident at once when possible), then the shortest chunks, then the
+// larger CTA.
+void pick_shape(ixb_handle* h, int eq) {
+  int best = -1;
+  long long best_key = 0;
+  for (int k = 0; k < 7; ++k) {
+    SweepShape s = sweep_shape(eq, h->mi, h->nj, 8, kShapes[k][0], kShapes[k][1]);
+    const int occ = sweep_occupancy(eq, h->prm.solver, s);
+    if (occ <= 0) continue;
+    const long long waves = (s.grid + (long long)occ * h->nsm - 1) / ((long long)occ * h->nsm);
+    const long long key = waves * 1000000LL + (long long)s.m * 1000 + (256 - s.nt);
+    if (best < 0 || key < best_key) { best = k; best_key = key; }
+  }
+  if (best < 0) best = 1;
+  h->shape_tl[eq] = kShapes[best][0];
+  h->shape_g[eq] = kShapes[best][1];
 }
 
 // Launch one sweep reading field buffers `cur` and writing `cur^1`.
 int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
   Geo<double> G = make_geo(h);
-  SweepShape s = sweep_shape(eq, h->mi, h->nj, 8, h->tl_override[eq], h->nt_override[eq]);
+  if (h->shape_tl[eq] == 0) pick_shape(h, eq);
+  SweepShape s = sweep_shape(eq, h->mi, h->nj, 8, h->shape_tl[eq], h->shape_g[eq]);
   SweepIO<double> io{};
   io.u = h->u[h->cu]; io.v = h->v[h->cv]; io.T = h->T[h->cT]; io.p = h->p; io.pc = h->pc[h->cpc];
   io.u_ant = h->u_ant; io.v_ant = h->v_ant; io.T_ant = h->T_ant;
   io.au = h->au; io.av = h->av;
-  io.m = s.m; io.mp = s.mp;
+  io.m = s.m; io.mp = s.mp; io.rs = s.rs;
   int var = -1;
   int* cur = nullptr;
   double** buf = nullptr;
@@ -456,7 +494,7 @@ void free_all(ixb_handle* h) {
   double** bufs[] = {&h->u[0], &h->u[1], &h->v[0], &h->v[1], &h->T[0], &h->T[1], &h->pc[0], &h->pc[1],
                      &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu,
                      &h->fcon[0], &h->fcon[1], &h->fcon[2], &h->flin[0], &h->flin[1], &h->flin[2],
-                     &h->metrics, &h->xp_d, &h->yp_d, &h->partials, &h->norms, &h->nu_d};
+                     &h->metrics, &h->tables, &h->xp_d, &h->yp_d, &h->partials, &h->norms, &h->nu_d};
   for (auto b : bufs) if (*b) cudaFree(*b);
   if (h->bc) cudaFree(h->bc);
   if (h->counters) cudaFree(h->counters);
@@ -525,7 +563,8 @@ int ixb_device_count(void) {
 int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   if (!out) return IXB_EINVAL;
   *out = nullptr;
-  if (mi < 4 || nj < 4 || mi > 16384 || nj > 16384) return IXB_EINVAL;
+  // a line of up to 6000 rows (chunks of <= 24 rows per thread) fits one CTA's shared memory
+  if (mi < 4 || nj < 4 || mi > 6000 || nj > 6000) return IXB_EINVAL;
   if (prec_mode != IXB_PREC_FP64) return IXB_EINVAL;  // binary32 mode: see ixb_create_refined
   ixb_handle* h = new (std::nothrow) ixb_handle();
   if (!h) return IXB_ENOMEM;
@@ -551,6 +590,9 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   }
   h->mstride = std::max(mi, nj) + 3;
   if (cudaMalloc(&h->metrics, (size_t)M_COUNT * h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMemset(h->metrics, 0, (size_t)M_COUNT * h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ECUDA);
+  if (cudaMalloc(&h->tables, (size_t)T_COUNT * fb) != cudaSuccess) return fail(IXB_ENOMEM);
+  if (cudaMemset(h->tables, 0, (size_t)T_COUNT * fb) != cudaSuccess) return fail(IXB_ECUDA);
   if (cudaMalloc(&h->xp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMalloc(&h->yp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   h->bcstride = std::max(mi, nj) + 3;
@@ -567,6 +609,12 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   if (cudaMallocHost(&h->h_norms, N_COUNT * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMallocHost(&h->ctl_h, sizeof(Ctl)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (sweep_set_smem_limits() != cudaSuccess) return fail(IXB_ECUDA);
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return fail(IXB_ECUDA);
+  }
   const char* env = std::getenv("IXB_NO_GRAPH");
   if (env && env[0] == '1') h->use_graph = 0;
   h->prm.p_update = 0.6;
@@ -624,6 +672,7 @@ int ixb_set_mesh(ixb_handle* h, const double* xu, const double* yv, const double
   CK(cudaMemcpyAsync(h->yp_d, yp1.data(), ms * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->has_mesh = true;
+  h->tables_dirty = true;
   return IXB_OK;
 }
 
@@ -631,6 +680,9 @@ int ixb_set_params(ixb_handle* h, const ixb_params* p) {
   if (!h || !p) return IXB_EINVAL;
   if (p->solver != IXB_SOLVER_HYBRID && p->solver != IXB_SOLVER_EXACT) return IXB_EINVAL;
   if (!(p->dt != 0.0) || !(p->rel_vel != 0.0) || !(p->rel_pres != 0.0) || !(p->rel_ener != 0.0)) return IXB_EINVAL;
+  if (p->gamma_momen != h->prm.gamma_momen || p->gamma_energ != h->prm.gamma_energ) h->tables_dirty = true;
+  if (p->solver != h->prm.solver)
+    for (int k = 0; k < EQ_COUNT; ++k) h->shape_tl[k] = h->shape_g[k] = 0;
   h->prm = *p;
   h->has_params = true;
   h->graph_dirty = true;
@@ -865,6 +917,86 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms) {
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   if (flush) cudaFree(flush);
+  return st;
+}
+
+int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads_per_line) {
+  if (!h || sweep < 0 || sweep >= EQ_COUNT) return IXB_EINVAL;
+  if (lines_per_cta == 0) {  // back to the default choice
+    h->shape_tl[sweep] = h->shape_g[sweep] = 0;
+    h->graph_dirty = true;
+    return IXB_OK;
+  }
+  int k = 0;
+  for (; k < 7; ++k)
+    if (kShapes[k][0] == lines_per_cta && kShapes[k][1] == threads_per_line) break;
+  if (k == 7) return IXB_EINVAL;
+  SweepShape s = sweep_shape(sweep, h->mi, h->nj, 8, lines_per_cta, threads_per_line);
+  if (sweep_occupancy(sweep, h->prm.solver, s) <= 0) return IXB_EINVAL;
+  h->shape_tl[sweep] = lines_per_cta;
+  h->shape_g[sweep] = threads_per_line;
+  h->graph_dirty = true;
+  return IXB_OK;
+}
+
+int ixb_autotune(ixb_handle* h, int reps, size_t flush_bytes, int* chosen, double* ms) {
+  TRY(ready(h));
+  if (reps < 1) return IXB_EINVAL;
+  // save the state the timing launches overwrite
+  const size_t fb = h->fsz * sizeof(double);
+  double* save = nullptr;
+  const int nsave = 11;
+  double* bufs[nsave] = {h->u[0], h->u[1], h->v[0], h->v[1], h->T[0], h->T[1], h->pc[0], h->pc[1],
+                         h->au, h->av, h->b_o};
+  if (cudaMalloc(&save, nsave * fb) != cudaSuccess) return IXB_ENOMEM;
+  void* flush = nullptr;
+  if (flush_bytes > 0 && cudaMalloc(&flush, flush_bytes) != cudaSuccess) { cudaFree(save); return IXB_ENOMEM; }
+  const int cu = h->cu, cv = h->cv, cT = h->cT, cpc = h->cpc;
+  int st = IXB_OK;
+  for (int k = 0; k < nsave && st == IXB_OK; ++k)
+    if (cudaMemcpyAsync(save + k * h->fsz, bufs[k], fb, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
+      st = IXB_ECUDA;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (st == IXB_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) st = IXB_ECUDA;
+  for (int eq = 0; eq < EQ_COUNT && st == IXB_OK; ++eq) {
+    double best = 1e30;
+    int best_k = -1;
+    for (int k = 0; k < 7 && st == IXB_OK; ++k) {
+      if (ixb_set_sweep_shape(h, eq, kShapes[k][0], kShapes[k][1]) != IXB_OK) continue;
+      st = sweep(h, eq, nullptr, false);  // warm-up
+      double total = 0.0;
+      for (int r = 0; r < reps && st == IXB_OK; ++r) {
+        if (flush && cudaMemsetAsync(flush, r & 0xff, flush_bytes, h->stream) != cudaSuccess) { st = IXB_ECUDA; break; }
+        if (cudaEventRecord(e0, h->stream) != cudaSuccess) { st = IXB_ECUDA; break; }
+        st = sweep(h, eq, nullptr, false);
+        if (st != IXB_OK) break;
+        if (cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+          st = IXB_ECUDA;
+          break;
+        }
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        total += t;
+      }
+      const double mean = total / reps;
+      if (st == IXB_OK && mean < best) { best = mean; best_k = k; }
+    }
+    if (st != IXB_OK) break;
+    if (best_k < 0) { st = IXB_ECUDA; break; }
+    h->shape_tl[eq] = kShapes[best_k][0];
+    h->shape_g[eq] = kShapes[best_k][1];
+    if (chosen) { chosen[2 * eq] = kShapes[best_k][0]; chosen[2 * eq + 1] = kShapes[best_k][1]; }
+    if (ms) ms[eq] = best;
+  }
+  for (int k = 0; k < nsave; ++k)
+    cudaMemcpyAsync(bufs[k], save + k * h->fsz, fb, cudaMemcpyDeviceToDevice, h->stream);
+  h->cu = cu; h->cv = cv; h->cT = cT; h->cpc = cpc;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess && st == IXB_OK) st = IXB_ECUDA;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (flush) cudaFree(flush);
+  cudaFree(save);
+  h->graph_dirty = true;
   return st;
 }
 

@@ -17,8 +17,26 @@
 
 namespace ixb {
 
-// metric arrays inside one device buffer, each `mstride` long, 1-based
-enum Metric { M_DXP = 0, M_DYP, M_DXU, M_DYU, M_DXV, M_DYV, M_FEXP, M_FEYP, M_FEXU, M_FEYV, M_COUNT };
+// metric arrays inside one device buffer, each `mstride` long, 1-based.
+// M_HXU/M_HYV are the energy equation's face diffusivities
+// hmean(ge,ge,fexu(k)) / hmean(ge,ge,feyv(k)), filled by the table kernel.
+enum Metric { M_DXP = 0, M_DYP, M_DXU, M_DYU, M_DXV, M_DYV, M_FEXP, M_FEYP, M_FEXU, M_FEYV, M_HXU, M_HYV, M_COUNT };
+
+// Mesh-constant 2-D tables (field layout).  With the uniform diffusion
+// coefficients of the reference (main.f90:226-239) every harmonic face
+// diffusivity and every diffusive conductance gamma*delta/d of the assembly
+// is a function of the mesh alone; the table kernel evaluates each one once,
+// with the reference's operands in the reference's order, so reading a table
+// entry gives the same bits as recomputing it in the cell loop.
+//   T_GU (ii,jj)  u: gamman at (ii,jj); gammas(ii,jj) = T_GU(ii,jj-1)
+//   T_CU1(ii,jj)  u: gammai*deltay/di;  AD conductance = T_CU1(ii+1,jj)
+//   T_CU2(ii,jj)  u: gamman*deltax/dn;  BS conductance = T_CU2(ii,jj-1)
+//   T_GV (ii,jj)  v: gammad at (ii,jj); gammai(ii,jj) = T_GV(ii-1,jj)
+//   T_CV1(ii,jj)  v: gammai*deltayv/di; AD conductance = T_CV1(ii+1,jj)
+//   T_CV2(ii,jj)  v: gammas*deltaxv/ds; BN conductance = T_CV2(ii,jj+1)
+//   T_CT1(ii,jj)  T: gammai*deltayp/di; AD conductance = T_CT1(ii+1,jj)
+//   T_CT2(ii,jj)  T: gamman*deltaxp/dn; BS conductance = T_CT2(ii,jj-1)
+enum Table { T_GU = 0, T_CU1, T_CU2, T_GV, T_CV1, T_CV2, T_CT1, T_CT2, T_COUNT };
 
 // sweeps: the eight line-solve phases of main.f90
 enum Eq { EQ_UY = 0, EQ_UX, EQ_VY, EQ_VX, EQ_PY, EQ_PX, EQ_TY, EQ_TX, EQ_COUNT };
@@ -35,13 +53,22 @@ struct NormSlot {        // deterministic two-level sum of squares
   double* result;        // sqrt(sum) written by the last CTA
 };
 
+// Read-only loads of the assembly: every array an assembly reads is left
+// untouched by the kernel that reads it, so the non-coherent path applies
+// and the compiler may batch the loads ahead of the shared-memory stores.
+template <class R>
+__device__ __forceinline__ R ldg(const R* p, int i) { return __ldg(p + i); }
+
 template <class R>
 struct Geo {
   int mi, nj, LD, mstride;
-  const R* m;  // M_COUNT arrays
+  int tstride;     // elements per 2-D table (fields stay below 2^31 elements)
+  const R* m;      // M_COUNT 1-D arrays
+  const R* tab;    // T_COUNT 2-D tables
   R gm, ge, Ri, Riy, dt, rel_vel, rel_pres, rel_ener, p_update;
-  __device__ __forceinline__ R met(int which, int k) const { return m[which * mstride + k]; }
-  __device__ __forceinline__ size_t at(int ii, int jj) const { return (size_t)(jj - 1) * LD + (ii - 1); }
+  __device__ __forceinline__ R met(int which, int k) const { return __ldg(m + which * mstride + k); }
+  __device__ __forceinline__ int at(int ii, int jj) const { return (jj - 1) * LD + (ii - 1); }
+  __device__ __forceinline__ R t(int which, int ii, int jj) const { return __ldg(tab + which * tstride + at(ii, jj)); }
 };
 
 template <class R>
@@ -58,7 +85,8 @@ struct SweepIO {
   const BCEntry* bc_last;
   NormSlot nrm0;                      // ||out - prev|| over interior rows of solved lines
   NormSlot nrm1;                      // ||b_o|| (p'-x)
-  int m, mp;                          // rows per lane chunk, padded chunk pitch
+  int m, mp;                          // rows per thread chunk, padded chunk pitch
+  int rs;                             // reduced-system solver (RS_PCR / RS_WARP)
 };
 
 template <class R>
@@ -85,41 +113,30 @@ __device__ __forceinline__ R hmean(R g1, R g2, R f) {
 // ---------------------------------------------------------------------------
 // u momentum (ensambla_velu_x/_y, source/mod_ec_momento.f90:365-724)
 // ---------------------------------------------------------------------------
-template <class R>
-struct UParts { R AI, AD, BS, BN, dxdy, tail; };
-
-// Everything of the u row except the in-line/cross-line arrangement.
-// `tail` = - dxdy*Ri*T_int + dxdy*fcon + dxdy*u_ant/dt + (p_P - p_E)*dy
-// is NOT formed here because the reference adds it after the cross terms;
-// the caller adds the terms in the reference order.
+// The four neighbour coefficients of the u row (:512-526), face velocities
+// interpolated as in :447-455, diffusivities and conductances from the
+// tables (gammai = gammad = gamma_momen).
 template <class R>
 __device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<R>& io, const R* u, int ii, int jj,
                                         R& AI, R& AD, R& BS, R& BN, R& deltax, R& deltay, R& temp_int) {
   const R* v = io.v;
   const R fexu_i = G.met(M_FEXU, ii), fexu_m = G.met(M_FEXU, ii - 1);
   const R fexp_i = G.met(M_FEXP, ii);
-  const R feyp_j = G.met(M_FEYP, jj), feyp_m = G.met(M_FEYP, jj - 1);
-  R ud = fexu_i * u[G.at(ii + 1, jj)] + (R(1) - fexu_i) * u[G.at(ii, jj)];
-  R ui = fexu_m * u[G.at(ii, jj)] + (R(1) - fexu_m) * u[G.at(ii - 1, jj)];
-  R vn = fexp_i * v[G.at(ii + 1, jj)] + (R(1) - fexp_i) * v[G.at(ii, jj)];
-  R vs = fexp_i * v[G.at(ii + 1, jj - 1)] + (R(1) - fexp_i) * v[G.at(ii, jj - 1)];
-  const R g = G.gm;  // gamma_momen is uniform (main.f90:226, :238)
-  R gammad = hmean(g, g, feyp_j);
-  R gammai = hmean(g, g, feyp_j);
-  R gamman = gammai * gammad / (gammad * (R(1) - fexp_i) + gammai * fexp_i);
-  gammad = hmean(g, g, feyp_m);
-  gammai = hmean(g, g, feyp_m);
-  R gammas = gammai * gammad / (gammad * (R(1) - fexp_i) + gammai * fexp_i);
-  gammai = g;
-  gammad = g;
+  R ud = fexu_i * ldg(u, G.at(ii + 1, jj)) + (R(1) - fexu_i) * ldg(u, G.at(ii, jj));
+  R ui = fexu_m * ldg(u, G.at(ii, jj)) + (R(1) - fexu_m) * ldg(u, G.at(ii - 1, jj));
+  R vn = fexp_i * ldg(v, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj));
+  R vs = fexp_i * ldg(v, G.at(ii + 1, jj - 1)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj - 1));
+  const R g = G.gm;
+  const R gamman = G.t(T_GU, ii, jj);
+  const R gammas = G.t(T_GU, ii, jj - 1);
   R di = G.met(M_DXP, ii), dd = G.met(M_DXP, ii + 1), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   deltax = G.met(M_DXU, ii);
   deltay = G.met(M_DYU, jj);
-  temp_int = fexp_i * io.T[G.at(ii + 1, jj)] + (R(1) - fexp_i) * io.T[G.at(ii, jj)];
-  AI = -(gammai * deltay / di * plaw(ui * di / gammai) + dmax0(ui * deltay));
-  AD = -(gammad * deltay / dd * plaw(ud * dd / gammad) + dmax0(-ud * deltay));
-  BS = -(gammas * deltax / ds * plaw(vs * ds / gammas) + dmax0(vs * deltax));
-  BN = -(gamman * deltax / dn * plaw(vn * dn / gamman) + dmax0(-vn * deltax));
+  temp_int = fexp_i * ldg(io.T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(io.T, G.at(ii, jj));
+  AI = -(G.t(T_CU1, ii, jj) * plaw(ui * di / g) + dmax0(ui * deltay));
+  AD = -(G.t(T_CU1, ii + 1, jj) * plaw(ud * dd / g) + dmax0(-ud * deltay));
+  BS = -(G.t(T_CU2, ii, jj - 1) * plaw(vs * ds / gammas) + dmax0(vs * deltax));
+  BN = -(G.t(T_CU2, ii, jj) * plaw(vn * dn / gamman) + dmax0(-vn * deltax));
 }
 
 // X form (ensambla_velu_x): a=AI c=AD b=AC d=Rx, aux = au = AC*rel
@@ -128,16 +145,16 @@ __device__ __forceinline__ Row<R> assemble_ux(const Geo<R>& G, const SweepIO<R>&
   const R* u = io.in;
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
-  const size_t c0 = G.at(ii, jj);
-  const R flin = io.flin ? io.flin[c0] : R(0);
-  const R fcon = io.fcon ? io.fcon[c0] : R(0);
+  const int c0 = G.at(ii, jj);
+  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
   r.b = (-AI - AD - BS - BN - dx * dy * flin + dx * dy / G.dt) / G.rel_vel;
-  r.d = -BS * u[G.at(ii, jj - 1)] - BN * u[G.at(ii, jj + 1)] - dx * dy * G.Ri * tint + dx * dy * fcon +
-        dx * dy * io.u_ant[c0] / G.dt + (io.p[c0] - io.p[G.at(ii + 1, jj)]) * dy +
-        r.b * (R(1) - G.rel_vel) * u[c0];
+  r.d = -BS * ldg(u, G.at(ii, jj - 1)) - BN * ldg(u, G.at(ii, jj + 1)) - dx * dy * G.Ri * tint + dx * dy * fcon +
+        dx * dy * ldg(io.u_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
+        r.b * (R(1) - G.rel_vel) * ldg(u, c0);
   au = r.b * G.rel_vel;
   return r;
 }
@@ -148,16 +165,16 @@ __device__ __forceinline__ Row<R> assemble_uy(const Geo<R>& G, const SweepIO<R>&
   const R* u = io.in;
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
-  const size_t c0 = G.at(ii, jj);
-  const R flin = io.flin ? io.flin[c0] : R(0);
-  const R fcon = io.fcon ? io.fcon[c0] : R(0);
+  const int c0 = G.at(ii, jj);
+  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
   r.b = (-AI - AD - BS - BN - dx * dy * flin + dx * dy / G.dt) / G.rel_vel;
-  r.d = -AI * u[G.at(ii - 1, jj)] - AD * u[G.at(ii + 1, jj)] - dx * dy * G.Ri * tint + dx * dy * fcon +
-        dx * dy * io.u_ant[c0] / G.dt + (io.p[c0] - io.p[G.at(ii + 1, jj)]) * dy +
-        r.b * (R(1) - G.rel_vel) * u[c0];
+  r.d = -AI * ldg(u, G.at(ii - 1, jj)) - AD * ldg(u, G.at(ii + 1, jj)) - dx * dy * G.Ri * tint + dx * dy * fcon +
+        dx * dy * ldg(io.u_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
+        r.b * (R(1) - G.rel_vel) * ldg(u, c0);
   return r;
 }
 
@@ -170,27 +187,20 @@ __device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<R>& io, c
   const R* u = io.u;
   const R feyp_j = G.met(M_FEYP, jj);
   const R feyv_j = G.met(M_FEYV, jj), feyv_m = G.met(M_FEYV, jj - 1);
-  const R fexp_i = G.met(M_FEXP, ii), fexp_m = G.met(M_FEXP, ii - 1);
-  R ud = feyp_j * u[G.at(ii, jj + 1)] + (R(1) - feyp_j) * u[G.at(ii, jj)];
-  R ui = feyp_j * u[G.at(ii - 1, jj + 1)] + (R(1) - feyp_j) * u[G.at(ii - 1, jj)];
-  R vn = feyv_j * v[G.at(ii, jj + 1)] + (R(1) - feyv_j) * v[G.at(ii, jj)];
-  R vs = feyv_m * v[G.at(ii, jj)] + (R(1) - feyv_m) * v[G.at(ii, jj - 1)];
-  const R g = G.gm;
-  R gammas = hmean(g, g, fexp_i);
-  R gamman = hmean(g, g, fexp_i);
-  R gammad = (gamman * gammas) / (gamman * (R(1) - feyp_j) + gammas * feyp_j);
-  gammas = hmean(g, g, fexp_m);
-  gamman = hmean(g, g, fexp_m);
-  R gammai = (gammas * gamman) / (gamman * (R(1) - feyp_j) + gammas * feyp_j);
-  gamman = g;
-  gammas = g;
+  R ud = feyp_j * ldg(u, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ldg(u, G.at(ii, jj));
+  R ui = feyp_j * ldg(u, G.at(ii - 1, jj + 1)) + (R(1) - feyp_j) * ldg(u, G.at(ii - 1, jj));
+  R vn = feyv_j * ldg(v, G.at(ii, jj + 1)) + (R(1) - feyv_j) * ldg(v, G.at(ii, jj));
+  R vs = feyv_m * ldg(v, G.at(ii, jj)) + (R(1) - feyv_m) * ldg(v, G.at(ii, jj - 1));
+  const R g = G.gm;  // gamman = gammas = gamma_momen (:854-858)
+  const R gammad = G.t(T_GV, ii, jj);
+  const R gammai = G.t(T_GV, ii - 1, jj);
   R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYP, jj), dn = G.met(M_DYP, jj + 1);
   const R dyv = G.met(M_DYV, jj), dxv = G.met(M_DXV, ii);
-  temp_int = feyp_j * io.T[G.at(ii, jj + 1)] + (R(1) - feyp_j) * io.T[G.at(ii, jj)];
-  AI = -(gammai * dyv / di * plaw(ui * di / gammai) + dmax0(ui * dyv));
-  AD = -(gammad * dyv / dd * plaw(ud * dd / gammad) + dmax0(-ud * dyv));
-  BS = -(gammas * dxv / ds * plaw(vs * ds / gammas) + dmax0(vs * dxv));
-  BN = -(gamman * dxv / dn * plaw(vn * dn / gamman) + dmax0(-vn * dxv));
+  temp_int = feyp_j * ldg(io.T, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ldg(io.T, G.at(ii, jj));
+  AI = -(G.t(T_CV1, ii, jj) * plaw(ui * di / gammai) + dmax0(ui * dyv));
+  AD = -(G.t(T_CV1, ii + 1, jj) * plaw(ud * dd / gammad) + dmax0(-ud * dyv));
+  BS = -(G.t(T_CV2, ii, jj) * plaw(vs * ds / g) + dmax0(vs * dxv));
+  BN = -(G.t(T_CV2, ii, jj + 1) * plaw(vn * dn / g) + dmax0(-vn * dxv));
 }
 
 template <class R>
@@ -198,18 +208,18 @@ __device__ __forceinline__ Row<R> assemble_vx(const Geo<R>& G, const SweepIO<R>&
   const R* v = io.in;
   R AI, AD, BS, BN, tint;
   v_parts(G, io, v, ii, jj, AI, AD, BS, BN, tint);
-  const size_t c0 = G.at(ii, jj);
+  const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = io.flin ? io.flin[c0] : R(0);
-  const R fcon = io.fcon ? io.fcon[c0] : R(0);
+  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
   r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_vel;
-  r.d = -BS * v[G.at(ii, jj - 1)] - BN * v[G.at(ii, jj + 1)] - dxdy * G.Riy * tint + dxdy * fcon +
-        dxdy * io.v_ant[c0] / G.dt + (io.p[c0] - io.p[G.at(ii, jj + 1)]) * dxv +
-        r.b * (R(1) - G.rel_vel) * v[c0];
+  r.d = -BS * ldg(v, G.at(ii, jj - 1)) - BN * ldg(v, G.at(ii, jj + 1)) - dxdy * G.Riy * tint + dxdy * fcon +
+        dxdy * ldg(io.v_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
+        r.b * (R(1) - G.rel_vel) * ldg(v, c0);
   av = r.b * G.rel_vel;
   return r;
 }
@@ -219,18 +229,18 @@ __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<R>&
   const R* v = io.in;
   R AI, AD, BS, BN, tint;
   v_parts(G, io, v, ii, jj, AI, AD, BS, BN, tint);
-  const size_t c0 = G.at(ii, jj);
+  const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = io.flin ? io.flin[c0] : R(0);
-  const R fcon = io.fcon ? io.fcon[c0] : R(0);
+  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
   r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_vel;
-  r.d = -AI * v[G.at(ii - 1, jj)] - AD * v[G.at(ii + 1, jj)] - dxdy * G.Riy * tint + dxdy * fcon +
-        dxdy * io.v_ant[c0] / G.dt + (io.p[c0] - io.p[G.at(ii, jj + 1)]) * dxv +
-        r.b * (R(1) - G.rel_vel) * v[c0];
+  r.d = -AI * ldg(v, G.at(ii - 1, jj)) - AD * ldg(v, G.at(ii + 1, jj)) - dxdy * G.Riy * tint + dxdy * fcon +
+        dxdy * ldg(io.v_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
+        r.b * (R(1) - G.rel_vel) * ldg(v, c0);
   return r;
 }
 
@@ -241,19 +251,18 @@ __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<R>&
 template <class R>
 __device__ __forceinline__ void t_parts(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& AI, R& AD,
                                         R& BS, R& BN) {
-  const R ud = io.u[G.at(ii, jj)], ui = io.u[G.at(ii - 1, jj)];
-  const R vn = io.v[G.at(ii, jj)], vs = io.v[G.at(ii, jj - 1)];
+  const R ud = ldg(io.u, G.at(ii, jj)), ui = ldg(io.u, G.at(ii - 1, jj));
+  const R vn = ldg(io.v, G.at(ii, jj)), vs = ldg(io.v, G.at(ii, jj - 1));
   const R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
-  const R g = G.ge;
-  const R gammad = hmean(g, g, G.met(M_FEXU, ii));
-  const R gammai = hmean(g, g, G.met(M_FEXU, ii - 1));
-  const R gamman = hmean(g, g, G.met(M_FEYV, jj));
-  const R gammas = hmean(g, g, G.met(M_FEYV, jj - 1));
+  const R gammad = G.met(M_HXU, ii);
+  const R gammai = G.met(M_HXU, ii - 1);
+  const R gamman = G.met(M_HYV, jj);
+  const R gammas = G.met(M_HYV, jj - 1);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
-  AI = -(gammai * dyp / di * plaw(ui * di / gammai) + dmax0(ui * dyp));
-  AD = -(gammad * dyp / dd * plaw(ud * dd / gammad) + dmax0(-ud * dyp));
-  BS = -(gammas * dxp / ds * plaw(vs * ds / gammas) + dmax0(vs * dxp));
-  BN = -(gamman * dxp / dn * plaw(vn * dn / gamman) + dmax0(-vn * dxp));
+  AI = -(G.t(T_CT1, ii, jj) * plaw(ui * di / gammai) + dmax0(ui * dyp));
+  AD = -(G.t(T_CT1, ii + 1, jj) * plaw(ud * dd / gammad) + dmax0(-ud * dyp));
+  BS = -(G.t(T_CT2, ii, jj - 1) * plaw(vs * ds / gammas) + dmax0(vs * dxp));
+  BN = -(G.t(T_CT2, ii, jj) * plaw(vn * dn / gamman) + dmax0(-vn * dxp));
 }
 
 template <class R>
@@ -261,16 +270,16 @@ __device__ __forceinline__ Row<R> assemble_tx(const Geo<R>& G, const SweepIO<R>&
   const R* T = io.in;
   R AI, AD, BS, BN;
   t_parts(G, io, ii, jj, AI, AD, BS, BN);
-  const size_t c0 = G.at(ii, jj);
+  const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = io.flin ? io.flin[c0] : R(0);
-  const R fcon = io.fcon ? io.fcon[c0] : R(0);
+  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
   r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_ener;
-  r.d = -BS * T[G.at(ii, jj - 1)] - BN * T[G.at(ii, jj + 1)] + dxdy * fcon + dxdy * io.T_ant[c0] / G.dt +
-        r.b * (R(1) - G.rel_ener) * T[c0];
+  r.d = -BS * ldg(T, G.at(ii, jj - 1)) - BN * ldg(T, G.at(ii, jj + 1)) + dxdy * fcon + dxdy * ldg(io.T_ant, c0) / G.dt +
+        r.b * (R(1) - G.rel_ener) * ldg(T, c0);
   return r;
 }
 
@@ -279,16 +288,16 @@ __device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<R>&
   const R* T = io.in;
   R AI, AD, BS, BN;
   t_parts(G, io, ii, jj, AI, AD, BS, BN);
-  const size_t c0 = G.at(ii, jj);
+  const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = io.flin ? io.flin[c0] : R(0);
-  const R fcon = io.fcon ? io.fcon[c0] : R(0);
+  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
   r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_ener;
-  r.d = -AI * T[G.at(ii - 1, jj)] - AD * T[G.at(ii + 1, jj)] + dxdy * fcon + dxdy * io.T_ant[c0] / G.dt +
-        r.b * (R(1) - G.rel_ener) * T[c0];
+  r.d = -AI * ldg(T, G.at(ii - 1, jj)) - AD * ldg(T, G.at(ii + 1, jj)) + dxdy * fcon + dxdy * ldg(io.T_ant, c0) / G.dt +
+        r.b * (R(1) - G.rel_ener) * ldg(T, c0);
   return r;
 }
 
@@ -297,14 +306,14 @@ __device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<R>&
 // ---------------------------------------------------------------------------
 template <class R>
 __device__ __forceinline__ R pc_at(const SweepIO<R>& io, const Geo<R>& G, int ii, int jj) {
-  return io.in ? io.in[G.at(ii, jj)] : R(0);
+  return io.in ? ldg(io.in, G.at(ii, jj)) : R(0);
 }
 
 template <class R>
 __device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& bo) {
-  const size_t c0 = G.at(ii, jj);
-  const R ud = io.u[c0], ui = io.u[G.at(ii - 1, jj)], vn = io.v[c0], vs = io.v[G.at(ii, jj - 1)];
-  const R ai = io.au[G.at(ii - 1, jj)], ad = io.au[c0], as = io.av[G.at(ii, jj - 1)], an = io.av[c0];
+  const int c0 = G.at(ii, jj);
+  const R ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
+  const R ai = ldg(io.au, G.at(ii - 1, jj)), ad = ldg(io.au, c0), as = ldg(io.av, G.at(ii, jj - 1)), an = ldg(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   Row<R> r;
   r.a = -dyp * dyp / ai;
@@ -320,9 +329,9 @@ __device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<R>&
 
 template <class R>
 __device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
-  const size_t c0 = G.at(ii, jj);
-  const R ud = io.u[c0], ui = io.u[G.at(ii - 1, jj)], vn = io.v[c0], vs = io.v[G.at(ii, jj - 1)];
-  const R ai = io.au[G.at(ii - 1, jj)], ad = io.au[c0], as = io.av[G.at(ii, jj - 1)], an = io.av[c0];
+  const int c0 = G.at(ii, jj);
+  const R ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
+  const R ai = ldg(io.au, G.at(ii - 1, jj)), ad = ldg(io.au, c0), as = ldg(io.av, G.at(ii, jj - 1)), an = ldg(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   const R AI = -dyp * dyp / ai;
   const R AD = -dyp * dyp / ad;
@@ -339,47 +348,40 @@ __device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<R>&
 // ---------------------------------------------------------------------------
 // u residual (residuo_u, source/mod_ec_momento.f90:1107-1266).  With a
 // uniform gamma the reference's different south numerator (:1208) has the
-// same value as in ensambla_velu_x.
+// same value as in ensambla_velu_x, so it shares the u tables.
 // ---------------------------------------------------------------------------
 template <class R>
 __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v, const R* T, const R* p,
                                         const R* u_ant, const R* fcon, const R* flin, int ii, int jj) {
   const R fexu_i = G.met(M_FEXU, ii), fexu_m = G.met(M_FEXU, ii - 1);
   const R fexp_i = G.met(M_FEXP, ii);
-  const R feyp_j = G.met(M_FEYP, jj), feyp_m = G.met(M_FEYP, jj - 1);
-  R ud = fexu_i * u[G.at(ii + 1, jj)] + (R(1) - fexu_i) * u[G.at(ii, jj)];
-  R ui = fexu_m * u[G.at(ii, jj)] + (R(1) - fexu_m) * u[G.at(ii - 1, jj)];
-  R vn = fexp_i * v[G.at(ii + 1, jj)] + (R(1) - fexp_i) * v[G.at(ii, jj)];
-  R vs = fexp_i * v[G.at(ii + 1, jj - 1)] + (R(1) - fexp_i) * v[G.at(ii, jj - 1)];
+  R ud = fexu_i * ldg(u, G.at(ii + 1, jj)) + (R(1) - fexu_i) * ldg(u, G.at(ii, jj));
+  R ui = fexu_m * ldg(u, G.at(ii, jj)) + (R(1) - fexu_m) * ldg(u, G.at(ii - 1, jj));
+  R vn = fexp_i * ldg(v, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj));
+  R vs = fexp_i * ldg(v, G.at(ii + 1, jj - 1)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj - 1));
   const R g = G.gm;
-  R gammad = hmean(g, g, feyp_j);
-  R gammai = hmean(g, g, feyp_j);
-  R gamman = gammai * gammad / (gammad * (R(1) - fexp_i) + gammai * fexp_i);
-  gammad = hmean(g, g, feyp_m);
-  gammai = hmean(g, g, feyp_m);
-  R gammas = gammai * gammad / (gammad * (R(1) - fexp_i) + gammai * fexp_i);
-  gammai = g;
-  gammad = g;
+  const R gamman = G.t(T_GU, ii, jj);
+  const R gammas = G.t(T_GU, ii, jj - 1);
   R di = G.met(M_DXP, ii), dd = G.met(M_DXP, ii + 1), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   const R dxu = G.met(M_DXU, ii), dyu = G.met(M_DYU, jj);
-  const size_t c0 = G.at(ii, jj);
-  R temp_int = fexp_i * T[G.at(ii + 1, jj)] + (R(1) - fexp_i) * T[c0];
-  R AI = (gammai * dyu / di * plaw(ui * di / gammai) + dmax0(ui * dyu));
-  R AD = (gammad * dyu / dd * plaw(ud * dd / gammad) + dmax0(-ud * dyu));
-  R BS = (gammas * dxu / ds * plaw(vs * ds / gammas) + dmax0(vs * dxu));
-  R BN = (gamman * dxu / dn * plaw(vn * dn / gamman) + dmax0(-vn * dxu));
-  const R fl = flin ? flin[c0] : R(0);
-  const R fc = fcon ? fcon[c0] : R(0);
+  const int c0 = G.at(ii, jj);
+  R temp_int = fexp_i * ldg(T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(T, c0);
+  R AI = (G.t(T_CU1, ii, jj) * plaw(ui * di / g) + dmax0(ui * dyu));
+  R AD = (G.t(T_CU1, ii + 1, jj) * plaw(ud * dd / g) + dmax0(-ud * dyu));
+  R BS = (G.t(T_CU2, ii, jj - 1) * plaw(vs * ds / gammas) + dmax0(vs * dxu));
+  R BN = (G.t(T_CU2, ii, jj) * plaw(vn * dn / gamman) + dmax0(-vn * dxu));
+  const R fl = flin ? ldg(flin, c0) : R(0);
+  const R fc = fcon ? ldg(fcon, c0) : R(0);
   R AC = AI + AD + BS + BN - dxu * dyu * fl + dxu * dyu / G.dt;
-  return AI * u[G.at(ii - 1, jj)] - AC * u[c0] + AD * u[G.at(ii + 1, jj)] + BS * u[G.at(ii, jj - 1)] +
-         BN * u[G.at(ii, jj + 1)] - dxu * dyu * G.Ri * temp_int + dxu * dyu * fc + dxu * dyu * u_ant[c0] / G.dt +
-         (p[c0] - p[G.at(ii + 1, jj)]) * dyu;
+  return AI * ldg(u, G.at(ii - 1, jj)) - AC * ldg(u, c0) + AD * ldg(u, G.at(ii + 1, jj)) + BS * ldg(u, G.at(ii, jj - 1)) +
+         BN * ldg(u, G.at(ii, jj + 1)) - dxu * dyu * G.Ri * temp_int + dxu * dyu * fc + dxu * dyu * ldg(u_ant, c0) / G.dt +
+         (ldg(p, c0) - ldg(p, G.at(ii + 1, jj))) * dyu;
 }
 
 // ---------------------------------------------------------------------------
 // Line solvers on a line staged in shared memory.
-// Row r of the (padded) line lives in chunk lane = r / m at slot r % m;
-// arrays are [32][mp] with mp odd, so the 32 lanes walking their chunks
+// Row r of the (padded) line lives in chunk r / m at slot r % m; each row
+// array is [G][mp] with mp odd, so G threads walking their chunks in step
 // hit distinct banks.
 // ---------------------------------------------------------------------------
 
@@ -407,17 +409,32 @@ __device__ void thomas_exact(R* sa, R* sb, R* sc, R* sd, int n, int m, int mp) {
   }
 }
 
+// Reduced-system solvers of the partitioned line solve
+enum ReducedSolve { RS_PCR = 0, RS_WARP = 1 };
+
+__host__ __device__ constexpr int warp_chunk(int G) { return (2 * G + 31) / 32 < 3 ? 3 : (2 * G + 31) / 32; }
+
+// Shared-memory footprint (elements) of one line: the four row arrays of G
+// chunks (pitch mp), plus the reduced system: for RS_PCR two buffers of the
+// 2G normalised rows (a, c, d), for RS_WARP four [32][m2|1] arrays; room
+// for the larger of the two.
+__host__ __device__ constexpr size_t line_smem_elems(int G, int mp) {
+  return (size_t)4 * G * mp +
+         ((size_t)12 * G > (size_t)4 * 32 * (warp_chunk(G) | 1) ? (size_t)12 * G : (size_t)4 * 32 * (warp_chunk(G) | 1));
+}
+
 template <class R>
 __device__ __forceinline__ R shfl_up_r(R x, int d) { return __shfl_up_sync(0xffffffffu, x, d); }
 template <class R>
 __device__ __forceinline__ R shfl_dn_r(R x, int d) { return __shfl_down_sync(0xffffffffu, x, d); }
 
-// One warp per line: every lane eliminates its chunk of m >= 3 rows down to
-// two rows coupled to the neighbouring chunks (forward and backward
-// "modified Thomas" sweeps), the warp solves the 64-row reduced system by
-// parallel cyclic reduction with register shuffles, and every lane
-// back-substitutes its chunk.  (Thomas-PCR hybrid of Laszlo, Giles and
-// Appleyard, ACM TOMS 42(4) 2016.)  Must be called by all 32 lanes.
+// One warp solves one system staged as [32][mp] chunks of m >= 3 rows:
+// every lane eliminates its chunk down to two rows coupled to the
+// neighbouring chunks (forward and backward "modified Thomas" sweeps), the
+// warp solves the 64-row reduced system by parallel cyclic reduction with
+// register shuffles, and every lane back-substitutes its chunk.  (Thomas-PCR
+// hybrid of Laszlo, Giles and Appleyard, ACM TOMS 42(4) 2016.)  Must be
+// called by all 32 lanes.
 template <class R>
 __device__ void thomas_pcr_warp(R* sa, R* sb, R* sc, R* sd, int m, int mp) {
   const int lane = threadIdx.x & 31;
@@ -491,6 +508,120 @@ __device__ void thomas_pcr_warp(R* sa, R* sb, R* sc, R* sd, int m, int mp) {
   d[0] = x0;
   for (int k = 1; k < m - 1; ++k) d[k] = d[k] - a[k] * x0 - c[k] * xl;
   d[m - 1] = xl;
+}
+
+
+// Partitioned line solve of the TL lines staged in shared memory, G threads
+// per line (thread t: line t / G, chunk k = t % G, rows k*m .. k*m+m-1 at
+// offset k*mp of the line's row arrays).  Every thread eliminates its chunk
+// (m >= 3 rows) down to two rows coupled only to the neighbouring chunks'
+// end rows (a forward and a backward "modified Thomas" sweep); the 2G
+// reduced rows of each line are then solved either by parallel cyclic
+// reduction over all G threads in shared memory (RS_PCR, log2(2G) steps) or
+// by one warp per line with the warp Thomas-PCR hybrid (RS_WARP); finally
+// every thread back-substitutes its chunk.  This is the Thomas-PCR hybrid of
+// Laszlo, Giles and Appleyard (ACM TOMS 42(4), 2016) applied twice.  The
+// solution replaces the right-hand side.  Called by all TL*G threads;
+// threads of lines with `active` false only take part in the barriers.
+template <class R, int G>
+__device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active, int rs) {
+  const int k = threadIdx.x % G;
+  R* a = line + k * mp;
+  R* b = a + (size_t)G * mp;
+  R* c = b + (size_t)G * mp;
+  R* d = c + (size_t)G * mp;
+  R* red = line + (size_t)4 * G * mp;
+  constexpr int M2 = warp_chunk(G);
+  constexpr int M2P = M2 | 1;
+  R eA = R(0), eC = R(0), eD = R(0), oA = R(0), oC = R(0), oD = R(0);
+  if (active) {
+    // forward: rows 1..m-1 -> x_k + a'_k x_0 + c'_k x_{k+1} = d'_k
+    const R a0 = a[0], b0 = b[0], c0 = c[0], d0 = d[0];
+    R inv = R(1) / b[1];
+    R ap = a[1] * inv, cp = c[1] * inv, dp = d[1] * inv;
+    a[1] = ap; c[1] = cp; d[1] = dp;
+    for (int i = 2; i < m; ++i) {
+      const R ai = a[i];
+      const R r = R(1) / fma(-ai, cp, b[i]);
+      ap = -ai * ap * r;
+      dp = fma(-ai, dp, d[i]) * r;
+      cp = c[i] * r;
+      a[i] = ap; c[i] = cp; d[i] = dp;
+    }
+    // backward: rows m-3..1 -> x_i + a''_i x_0 + c''_i x_{m-1} = d''_i
+    R an = a[m - 2], cn = c[m - 2], dn = d[m - 2];
+    for (int i = m - 3; i >= 1; --i) {
+      const R ci = c[i];
+      dn = fma(-ci, dn, d[i]);
+      an = fma(-ci, an, a[i]);
+      cn = -ci * cn;
+      a[i] = an; c[i] = cn; d[i] = dn;
+    }
+    // reduced rows 2k (chunk's first row) and 2k+1 (its last row), unit diagonal
+    const R r0 = R(1) / fma(-c0, an, b0);
+    eA = a0 * r0; eC = -c0 * cn * r0; eD = fma(-c0, dn, d0) * r0;
+    oA = ap; oC = cp; oD = dp;
+  }
+  R x0, xl;
+  if (rs == RS_PCR) {
+    R* A[2] = {red, red + 6 * G};
+    R* C[2] = {red + 2 * G, red + 8 * G};
+    R* D[2] = {red + 4 * G, red + 10 * G};
+    if (active) {
+      A[0][2 * k] = eA; C[0][2 * k] = eC; D[0][2 * k] = eD;
+      A[0][2 * k + 1] = oA; C[0][2 * k + 1] = oC; D[0][2 * k + 1] = oD;
+    }
+    __syncthreads();
+    int cur = 0;
+#pragma unroll 1
+    for (int s = 1; s < 2 * G; s <<= 1) {
+      if (active) {
+        const R* Ac = A[cur]; const R* Cc = C[cur]; const R* Dc = D[cur];
+        R* An = A[cur ^ 1]; R* Cn = C[cur ^ 1]; R* Dn = D[cur ^ 1];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int i = k + q * G;
+          const R ai = Ac[i], ci = Cc[i], di = Dc[i];
+          R alo = R(0), clo = R(0), dlo = R(0), ahi = R(0), chi = R(0), dhi = R(0);
+          if (i - s >= 0) { alo = Ac[i - s]; clo = Cc[i - s]; dlo = Dc[i - s]; }
+          if (i + s < 2 * G) { ahi = Ac[i + s]; chi = Cc[i + s]; dhi = Dc[i + s]; }
+          const R r = R(1) / fma(-ci, ahi, fma(-ai, clo, R(1)));
+          An[i] = -ai * alo * r;
+          Cn[i] = -ci * chi * r;
+          Dn[i] = fma(-ci, dhi, fma(-ai, dlo, di)) * r;
+        }
+      }
+      __syncthreads();
+      cur ^= 1;
+    }
+    x0 = D[cur][2 * k];
+    xl = D[cur][2 * k + 1];
+  } else {
+    // reduced system in the warp solver's [32][M2P] chunk layout
+    constexpr int ARR2 = 32 * M2P;
+    auto off = [](int q) { return (q / M2) * M2P + q % M2; };
+    if (active) {
+      int o = off(2 * k);
+      red[o] = eA; red[o + ARR2] = R(1); red[o + 2 * ARR2] = eC; red[o + 3 * ARR2] = eD;
+      o = off(2 * k + 1);
+      red[o] = oA; red[o + ARR2] = R(1); red[o + 2 * ARR2] = oC; red[o + 3 * ARR2] = oD;
+    }
+    // identity rows pad the reduced system to 32*M2 rows
+    for (int q = 2 * G + k; q < 32 * M2; q += G) {
+      const int o = off(q);
+      red[o] = R(0); red[o + ARR2] = R(1); red[o + 2 * ARR2] = R(0); red[o + 3 * ARR2] = R(0);
+    }
+    __syncthreads();
+    if (k < 32 && active) thomas_pcr_warp(red, red + ARR2, red + 2 * ARR2, red + 3 * ARR2, M2, M2P);
+    __syncthreads();
+    x0 = red[3 * ARR2 + off(2 * k)];
+    xl = red[3 * ARR2 + off(2 * k + 1)];
+  }
+  if (active) {
+    d[0] = x0;
+    for (int i = 1; i < m - 1; ++i) d[i] = fma(-c[i], xl, fma(-a[i], x0, d[i]));
+    d[m - 1] = xl;
+  }
 }
 
 }  // namespace ixb

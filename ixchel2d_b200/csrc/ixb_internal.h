@@ -18,13 +18,26 @@ struct SweepShape {
   int line_hi;    // last solved line
   int nfull;      // lines of the field (unsolved ones are copied)
   int tl;         // lines per CTA
-  int nt;         // threads per CTA
-  int m, mp;      // chunk rows per lane, padded pitch
+  int g;          // threads per line
+  int nt;         // threads per CTA (tl * g)
+  int m, mp;      // chunk rows per thread, padded pitch
+  int rs;         // reduced-system solver (RS_PCR / RS_WARP)
   size_t smem;    // dynamic shared memory bytes
   int grid;       // CTAs
 };
 
-SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl_override, int nt_override);
+// Shape of sweep `eq` with tl lines per CTA and g threads per line
+// (tl * g = 128 or 256; chunks of max(3, ceil(n/g)) rows).
+SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl, int g);
+
+// per-equation sweep launchers (ixb_sweep_{u,v,p,t}.cu)
+template <class R, int EQ>
+cudaError_t sweep_launch(int solver, const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st);
+template <class R, int EQ>
+cudaError_t sweep_smem_limit(int bytes);
+template <class R, int EQ>
+int sweep_blocks_per_sm(int solver, const SweepShape& s);
+int sweep_occupancy(int eq, int solver, const SweepShape& s);
 int max_sweep_lines(int mi, int nj);
 
 // kernel launchers (ixb_kernels.cu); return cudaError_t
@@ -39,6 +52,7 @@ int residual_grid(int mi, int nj);
 cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,
                                int vertical, int k0, int k1, double* out2, cudaStream_t st);
 cudaError_t sweep_set_smem_limits();
+cudaError_t launch_tables_f64(const Geo<double>& G, double* met, double* tab, cudaStream_t st);
 
 // batched standalone tridiagonal solvers (ixb_tridiag.cu)
 cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,

@@ -1,216 +1,76 @@
-// ixb_kernels.cu -- sm_100a kernels of the SIMPLE outer iteration.
-//
-// One fused kernel per line sweep replaces the reference's four OpenACC
-// regions per sweep (assembly, impone_cond_frontera, tridiagonal, scatter;
-// e.g. source/main.f90:420-484): a CTA owns TL adjacent lines, assembles
-// their rows straight from the fields into shared memory (coalesced along
-// ii), applies the boundary rows from a per-line table, solves each line
-// with one warp, and writes the solution to the ping-pong output buffer,
-// reducing the convergence norm of the pass on the way out.
+// ixb_kernels.cu -- the non-sweep kernels of the SIMPLE outer iteration
+// (p/u/v correction, u residual, Nusselt number, mesh-constant tables), the
+// launch shape of the sweeps and their dispatch to the per-equation
+// translation units.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
 #include "ixb_internal.h"
+#include "ixb_reduce.cuh"
 
 namespace ixb {
 
 // ---------------------------------------------------------------------------
-// reductions (fixed order: deterministic run to run)
+// mesh-constant tables (see ixb_device.cuh), one thread per (ii,jj);
+// operands in the reference's order (-fmad=false build)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-__device__ double block_sum(double v) {
-  __shared__ double red[32];
-  v = warp_sum(v);
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  double s = 0.0;
-  if (w == 0) {
-    s = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
-    s = warp_sum(s);
-  }
-  return s;  // valid in thread 0
-}
-
-// Publish this CTA's partial; the last CTA to arrive sums all partials in
-// CTA order and stores sqrt(sum).
-__device__ void finish_norm(const NormSlot& ns, double block_total) {
-  __shared__ int is_last;
-  if (threadIdx.x == 0) {
-    ns.partials[blockIdx.x] = block_total;
-    __threadfence();
-    const unsigned prev = atomicAdd(ns.counter, 1u);
-    is_last = (prev == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (is_last && threadIdx.x < 32) {
-    __threadfence();
-    double s = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) s += __ldcg(ns.partials + i);
-    s = warp_sum(s);
-    if (threadIdx.x == 0) {
-      *ns.result = sqrt(s);
-      *ns.counter = 0u;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// per-equation assembly dispatch
-// ---------------------------------------------------------------------------
-template <int EQ>
-struct EqIsX { static constexpr bool value = (EQ & 1) != 0; };
-
-template <class R, int EQ>
-__device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj,
-                                                double& acc_bo) {
-  if constexpr (EQ == EQ_UY) {
-    return assemble_uy(G, io, ii, jj);
-  } else if constexpr (EQ == EQ_UX) {
-    R au;
-    Row<R> r = assemble_ux(G, io, ii, jj, au);
-    io.aux[G.at(ii, jj)] = au;
-    return r;
-  } else if constexpr (EQ == EQ_VY) {
-    return assemble_vy(G, io, ii, jj);
-  } else if constexpr (EQ == EQ_VX) {
-    R av;
-    Row<R> r = assemble_vx(G, io, ii, jj, av);
-    io.aux[G.at(ii, jj)] = av;
-    return r;
-  } else if constexpr (EQ == EQ_PY) {
-    return assemble_py(G, io, ii, jj);
-  } else if constexpr (EQ == EQ_PX) {
-    R bo;
-    Row<R> r = assemble_px(G, io, ii, jj, bo);
-    io.aux[G.at(ii, jj)] = bo;
-    acc_bo += (double)bo * (double)bo;
-    return r;
-  } else if constexpr (EQ == EQ_TY) {
-    return assemble_ty(G, io, ii, jj);
-  } else {
-    return assemble_tx(G, io, ii, jj);
-  }
-}
-
-// Boundary rows of impone_cond_frontera (source/mod_cond_frontera.f90:280-416):
-// first row of a line: diri (0,1,0|val), neum (0,-1,1|val);
-// last row: diri (0,1,0|val), neum (-1,1,0|val).  p' rows are hard-coded
-// Dirichlet 0 (main.f90:789-800, 845-856).
 template <class R>
-__device__ __forceinline__ Row<R> bc_first_row(const BCEntry* t, int L) {
-  if (!t) return Row<R>{R(0), R(1), R(0), R(0)};
-  const BCEntry e = t[L];
-  if (e.type == 2) return Row<R>{R(0), R(-1), R(1), R(e.val)};
-  return Row<R>{R(0), R(1), R(0), R(e.val)};
+__global__ void table1d_kernel(Geo<R> G, R* met) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const R ge = G.ge;
+  if (k >= 1 && k <= G.mi) met[M_HXU * G.mstride + k] = hmean(ge, ge, G.met(M_FEXU, k));
+  if (k >= 1 && k <= G.nj) met[M_HYV * G.mstride + k] = hmean(ge, ge, G.met(M_FEYV, k));
 }
+
 template <class R>
-__device__ __forceinline__ Row<R> bc_last_row(const BCEntry* t, int L) {
-  if (!t) return Row<R>{R(0), R(1), R(0), R(0)};
-  const BCEntry e = t[L];
-  if (e.type == 2) return Row<R>{R(-1), R(1), R(0), R(e.val)};
-  return Row<R>{R(0), R(1), R(0), R(e.val)};
+__global__ void table2d_kernel(Geo<R> G, R* tab) {
+  const int ii = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = 1 + blockIdx.y;
+  if (ii > G.mi + 1 || jj > G.nj + 1) return;
+  const size_t c0 = G.at(ii, jj);
+  auto T = [&](int w) -> R& { return tab[w * G.tstride + c0]; };
+  const R g = G.gm;
+  auto combo = [](R h, R f) { return h * h / (h * (R(1) - f) + h * f); };
+  // u (ensambla_velu_x :462-479, :512-526)
+  if (ii <= G.mi && jj <= G.nj) {
+    const R hy = hmean(g, g, G.met(M_FEYP, jj));
+    const R gamman = combo(hy, G.met(M_FEXP, ii));
+    T(T_GU) = gamman;
+    T(T_CU2) = gamman * G.met(M_DXU, ii) / G.met(M_DYV, jj);
+  }
+  if (ii >= 2 && ii <= G.mi && jj >= 2 && jj <= G.nj) T(T_CU1) = g * G.met(M_DYU, jj) / G.met(M_DXP, ii);
+  // v (ensambla_velv_x :833-850, :880-894)
+  if (ii <= G.mi && jj <= G.nj) {
+    const R hx = hmean(g, g, G.met(M_FEXP, ii));
+    T(T_GV) = combo(hx, G.met(M_FEYP, jj));
+  }
+  if (ii >= 2 && ii <= G.mi + 1 && jj <= G.nj) {
+    const R hx = hmean(g, g, G.met(M_FEXP, ii - 1));
+    const R gammai = combo(hx, G.met(M_FEYP, jj));
+    T(T_CV1) = gammai * G.met(M_DYV, jj) / G.met(M_DXU, ii - 1);
+  }
+  if (ii >= 2 && ii <= G.mi && jj >= 2 && jj <= G.nj) T(T_CV2) = g * G.met(M_DXV, ii) / G.met(M_DYP, jj);
+  // T (ensambla_energia_x :230-259, fexu/feyv bound to fexpo/feypo)
+  const R ge = G.ge;
+  if (ii >= 2 && ii <= G.mi + 1 && jj >= 2 && jj <= G.nj) {
+    const R gammai = hmean(ge, ge, G.met(M_FEXU, ii - 1));
+    T(T_CT1) = gammai * G.met(M_DYP, jj) / G.met(M_DXU, ii - 1);
+  }
+  if (ii >= 2 && ii <= G.mi && jj <= G.nj) {
+    const R gamman = hmean(ge, ge, G.met(M_FEYV, jj));
+    T(T_CT2) = gamman * G.met(M_DXP, ii) / G.met(M_DYV, jj);
+  }
 }
 
-// ---------------------------------------------------------------------------
-// fused sweep kernel
-// ---------------------------------------------------------------------------
-template <class R, int EQ, int SOLVER, int TL>
-__global__ void __launch_bounds__(512) sweep_kernel(const Geo<R> G, const SweepIO<R> io, const int n,
-                                                    const int line_lo, const int line_hi, const int nfull) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sm = reinterpret_cast<R*>(smem_raw);
-  constexpr bool X = EqIsX<EQ>::value;
-  const int m = io.m, mp = io.mp;
-  const int npad = 32 * m;
-  const int chunk = 32 * mp;
-  const int L0 = 1 + blockIdx.x * TL;
-  const int NT = blockDim.x;
-  double acc_bo = 0.0;
-
-  // phase 1: assemble every row of the solved lines into shared memory
-  for (int idx = threadIdx.x; idx < TL * npad; idx += NT) {
-    int l, r;
-    if (X) { l = idx / npad; r = idx - l * npad; }
-    else { l = idx % TL; r = idx / TL; }
-    const int L = L0 + l;
-    if (L < line_lo || L > line_hi) continue;
-    Row<R> row;
-    if (r >= n) row = Row<R>{R(0), R(1), R(0), R(0)};  // identity padding
-    else if (r == 0) row = bc_first_row<R>(io.bc_first, L);
-    else if (r == n - 1) row = bc_last_row<R>(io.bc_last, L);
-    else {
-      const int ii = X ? r + 1 : L;
-      const int jj = X ? L : r + 1;
-      row = assemble_cell<R, EQ>(G, io, ii, jj, acc_bo);
-    }
-    const int lane = r / m;
-    const int o = lane * mp + (r - lane * m);
-    R* base = sm + l * 4 * chunk;
-    base[o] = row.a;
-    base[chunk + o] = row.b;
-    base[2 * chunk + o] = row.c;
-    base[3 * chunk + o] = row.d;
-  }
-  __syncthreads();
-
-  // phase 2: one warp per line
-  {
-    const int w = threadIdx.x >> 5;
-    if (w < TL) {
-      const int L = L0 + w;
-      if (L >= line_lo && L <= line_hi) {
-        R* base = sm + w * 4 * chunk;
-        if (SOLVER == IXB_SOLVER_EXACT) {
-          if ((threadIdx.x & 31) == 0) thomas_exact(base, base + chunk, base + 2 * chunk, base + 3 * chunk, n, m, mp);
-        } else {
-          thomas_pcr_warp(base, base + chunk, base + 2 * chunk, base + 3 * chunk, m, mp);
-        }
-      }
-    }
-  }
-  __syncthreads();
-
-  // phase 3: write the new field (unsolved lines keep their values) and
-  // accumulate ||new - prev|| over the interior rows of the solved lines
-  double acc = 0.0;
-  for (int idx = threadIdx.x; idx < TL * n; idx += NT) {
-    int l, r;
-    if (X) { l = idx / n; r = idx - l * n; }
-    else { l = idx % TL; r = idx / TL; }
-    const int L = L0 + l;
-    if (L > nfull) continue;
-    const int ii = X ? r + 1 : L;
-    const int jj = X ? L : r + 1;
-    const size_t g = G.at(ii, jj);
-    R x;
-    if (L >= line_lo && L <= line_hi) {
-      const int lane = r / m;
-      x = sm[l * 4 * chunk + 3 * chunk + lane * mp + (r - lane * m)];
-      if (io.nrm0.partials && r >= 1 && r <= n - 2) {
-        const double dv = (double)x - (io.prev ? (double)io.prev[g] : 0.0);
-        acc += dv * dv;
-      }
-    } else {
-      x = io.in ? io.in[g] : R(0);
-    }
-    io.out[g] = x;
-  }
-  if (io.nrm0.partials) {
-    const double s = block_sum(acc);
-    finish_norm(io.nrm0, s);
-  }
-  if (io.nrm1.partials) {
-    const double s = block_sum(acc_bo);
-    finish_norm(io.nrm1, s);
-  }
+cudaError_t launch_tables_f64(const Geo<double>& G, double* met, double* tab, cudaStream_t st) {
+  const int n1 = std::max(G.mi, G.nj) + 1;
+  table1d_kernel<double><<<(n1 + 127) / 128, 128, 0, st>>>(G, met);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 grid((G.mi + 1 + 127) / 128, G.nj + 1);
+  table2d_kernel<double><<<grid, 128, 0, st>>>(G, tab);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -301,7 +161,7 @@ __global__ void nusselt_kernel(const Geo<double> G, const double* __restrict__ T
 // ---------------------------------------------------------------------------
 int max_sweep_lines(int mi, int nj) { return std::max(mi, nj) + 2; }
 
-SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl_override, int nt_override) {
+SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl, int g) {
   SweepShape s{};
   switch (eq) {
     case EQ_UY: s.n = nj + 1; s.line_lo = 2; s.line_hi = mi - 1; s.nfull = mi; break;
@@ -313,57 +173,30 @@ SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl_override, 
     case EQ_TY: s.n = nj + 1; s.line_lo = 2; s.line_hi = mi; s.nfull = mi + 1; break;
     default:    s.n = mi + 1; s.line_lo = 2; s.line_hi = nj; s.nfull = nj + 1; break;
   }
-  s.m = std::max(3, (s.n + 31) / 32);
-  s.mp = s.m | 1;
-  const bool x = (eq & 1) != 0;
-  int tl = x ? 1 : 4;
-  if (tl_override > 0) tl = tl_override;
-  const size_t per_line = (size_t)4 * 32 * s.mp * real_bytes;
-  while (tl > 1 && per_line * tl > 200 * 1024) tl >>= 1;
   s.tl = tl;
-  int nt = x ? (s.n > 256 ? 256 : 128) : std::max(128, 32 * tl);
-  if (nt_override > 0) nt = nt_override;
-  nt = std::max(nt, 32 * tl);
-  nt = std::min(nt, 512);
-  s.nt = nt;
-  s.smem = per_line * tl;
+  s.g = g;
+  s.nt = tl * g;
+  s.m = std::max(3, (s.n + g - 1) / g);
+  s.mp = s.m | 1;
+  s.rs = RS_PCR;
+  s.smem = line_smem_elems(g, s.mp) * real_bytes * tl;
   s.grid = (s.nfull + tl - 1) / tl;
   return s;
 }
 
-template <class R, int EQ, int SOLVER, int TL>
-static cudaError_t launch_one(const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st) {
-  sweep_kernel<R, EQ, SOLVER, TL><<<s.grid, s.nt, s.smem, st>>>(G, io, s.n, s.line_lo, s.line_hi, s.nfull);
-  return cudaGetLastError();
+int sweep_occupancy(int eq, int solver, const SweepShape& s) {
+  switch (eq) {
+    case EQ_UY: return sweep_blocks_per_sm<double, EQ_UY>(solver, s);
+    case EQ_UX: return sweep_blocks_per_sm<double, EQ_UX>(solver, s);
+    case EQ_VY: return sweep_blocks_per_sm<double, EQ_VY>(solver, s);
+    case EQ_VX: return sweep_blocks_per_sm<double, EQ_VX>(solver, s);
+    case EQ_PY: return sweep_blocks_per_sm<double, EQ_PY>(solver, s);
+    case EQ_PX: return sweep_blocks_per_sm<double, EQ_PX>(solver, s);
+    case EQ_TY: return sweep_blocks_per_sm<double, EQ_TY>(solver, s);
+    default:    return sweep_blocks_per_sm<double, EQ_TX>(solver, s);
+  }
 }
 
-// Raise the dynamic shared-memory limit of every sweep instantiation once
-// (outside any stream capture).
-template <class R, int EQ, int SOLVER>
-static cudaError_t smem_limit_eq(int bytes) {
-  cudaError_t e = cudaSuccess;
-  auto set = [&](auto k) {
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  };
-  set(sweep_kernel<R, EQ, SOLVER, 1>);
-  set(sweep_kernel<R, EQ, SOLVER, 2>);
-  set(sweep_kernel<R, EQ, SOLVER, 4>);
-  set(sweep_kernel<R, EQ, SOLVER, 8>);
-  return e;
-}
-template <class R, int SOLVER>
-static cudaError_t smem_limit_all(int bytes) {
-  cudaError_t e = cudaSuccess;
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_UY, SOLVER>(bytes);
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_UX, SOLVER>(bytes);
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_VY, SOLVER>(bytes);
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_VX, SOLVER>(bytes);
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_PY, SOLVER>(bytes);
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_PX, SOLVER>(bytes);
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_TY, SOLVER>(bytes);
-  if (e == cudaSuccess) e = smem_limit_eq<R, EQ_TX, SOLVER>(bytes);
-  return e;
-}
 cudaError_t sweep_set_smem_limits() {
   static int done = 0;
   if (done) return cudaSuccess;
@@ -372,43 +205,32 @@ cudaError_t sweep_set_smem_limits() {
   if (e != cudaSuccess) return e;
   e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
-  const int bytes = optin - 1024;  // leave room for the static reduction buffers
-  e = smem_limit_all<double, IXB_SOLVER_HYBRID>(bytes);
-  if (e == cudaSuccess) e = smem_limit_all<double, IXB_SOLVER_EXACT>(bytes);
+  const int bytes = optin - 1024;  // room for the static reduction buffers
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_UY>(bytes);
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_UX>(bytes);
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_VY>(bytes);
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_VX>(bytes);
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_PY>(bytes);
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_PX>(bytes);
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_TY>(bytes);
+  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_TX>(bytes);
   if (e == cudaSuccess) done = 1;
   return e;
 }
 
-template <class R, int EQ, int SOLVER>
-static cudaError_t launch_tl(const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st) {
-  switch (s.tl) {
-    case 1: return launch_one<R, EQ, SOLVER, 1>(s, G, io, st);
-    case 2: return launch_one<R, EQ, SOLVER, 2>(s, G, io, st);
-    case 4: return launch_one<R, EQ, SOLVER, 4>(s, G, io, st);
-    case 8: return launch_one<R, EQ, SOLVER, 8>(s, G, io, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-template <class R, int SOLVER>
-static cudaError_t launch_eq(int eq, const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st) {
-  switch (eq) {
-    case EQ_UY: return launch_tl<R, EQ_UY, SOLVER>(s, G, io, st);
-    case EQ_UX: return launch_tl<R, EQ_UX, SOLVER>(s, G, io, st);
-    case EQ_VY: return launch_tl<R, EQ_VY, SOLVER>(s, G, io, st);
-    case EQ_VX: return launch_tl<R, EQ_VX, SOLVER>(s, G, io, st);
-    case EQ_PY: return launch_tl<R, EQ_PY, SOLVER>(s, G, io, st);
-    case EQ_PX: return launch_tl<R, EQ_PX, SOLVER>(s, G, io, st);
-    case EQ_TY: return launch_tl<R, EQ_TY, SOLVER>(s, G, io, st);
-    case EQ_TX: return launch_tl<R, EQ_TX, SOLVER>(s, G, io, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
                              const SweepIO<double>& io, cudaStream_t st) {
-  if (solver == IXB_SOLVER_EXACT) return launch_eq<double, IXB_SOLVER_EXACT>(eq, s, G, io, st);
-  return launch_eq<double, IXB_SOLVER_HYBRID>(eq, s, G, io, st);
+  switch (eq) {
+    case EQ_UY: return sweep_launch<double, EQ_UY>(solver, s, G, io, st);
+    case EQ_UX: return sweep_launch<double, EQ_UX>(solver, s, G, io, st);
+    case EQ_VY: return sweep_launch<double, EQ_VY>(solver, s, G, io, st);
+    case EQ_VX: return sweep_launch<double, EQ_VX>(solver, s, G, io, st);
+    case EQ_PY: return sweep_launch<double, EQ_PY>(solver, s, G, io, st);
+    case EQ_PX: return sweep_launch<double, EQ_PX>(solver, s, G, io, st);
+    case EQ_TY: return sweep_launch<double, EQ_TY>(solver, s, G, io, st);
+    case EQ_TX: return sweep_launch<double, EQ_TX>(solver, s, G, io, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,

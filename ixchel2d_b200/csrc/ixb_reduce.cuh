@@ -1,0 +1,58 @@
+// ixb_reduce.cuh -- deterministic block and grid reductions of the
+// convergence norms (fixed summation order, so results repeat bit for bit).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ixb_device.cuh"
+
+namespace ixb {
+
+// ---------------------------------------------------------------------------
+// reductions (fixed order: deterministic run to run)
+// ---------------------------------------------------------------------------
+static __device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+static __device__ double block_sum(double v) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (w == 0) {
+    s = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+    s = warp_sum(s);
+  }
+  return s;  // valid in thread 0
+}
+
+// Publish this CTA's partial; the last CTA to arrive sums all partials in
+// CTA order (every thread of that CTA loads its share in one round trip)
+// and stores sqrt(sum).
+static __device__ void finish_norm(const NormSlot& ns, double block_total) {
+  __shared__ int is_last;
+  if (threadIdx.x == 0) {
+    ns.partials[blockIdx.x] = block_total;
+    __threadfence();
+    const unsigned prev = atomicAdd(ns.counter, 1u);
+    is_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (is_last) {
+    __threadfence();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(ns.partials + i);
+    s = block_sum(s);
+    if (threadIdx.x == 0) {
+      *ns.result = sqrt(s);
+      *ns.counter = 0u;
+    }
+  }
+}
+
+}  // namespace ixb

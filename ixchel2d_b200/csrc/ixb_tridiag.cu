@@ -2,9 +2,10 @@
 // batched form of tridiagonal (source/mod_solucionador.f90:25-47).
 //
 // layout 0 (each system contiguous, like the reference's x-lines): a CTA
-// stages TL systems into shared memory with coalesced loads, one warp per
-// system solves (exact sequential Thomas or the warp Thomas-PCR hybrid),
-// and the solution is written back coalesced.
+// stages TL systems into shared memory with coalesced loads, G = 256/TL
+// threads per system solve it (the chunked Thomas-PCR hybrid, or the exact
+// sequential Thomas on one thread), and the solution is written back
+// coalesced.
 //
 // layout 1 (systems interleaved, row i of system s at i*nsys+s, like the
 // y-lines of a column-major field): one thread per system walks the rows;
@@ -20,15 +21,16 @@
 
 namespace ixb {
 
-template <class R, int SOLVER, int TL>
-__global__ void __launch_bounds__(256) tri_contig_kernel(const R* __restrict__ a, const R* __restrict__ b,
-                                                         const R* __restrict__ c, const R* __restrict__ d,
-                                                         R* x, int n, int nsys, int m, int mp) {
+template <class R, int SOLVER, int TL, int G>
+__global__ void __launch_bounds__(TL * G) tri_contig_kernel(const R* __restrict__ a, const R* __restrict__ b,
+                                                            const R* __restrict__ c, const R* __restrict__ d,
+                                                            R* x, int n, int nsys, int m, int mp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
-  const int npad = 32 * m, chunk = 32 * mp;
+  const int npad = G * m;
+  const size_t LS = line_smem_elems(G, mp), arr = (size_t)G * mp;
   const long long s0 = (long long)blockIdx.x * TL;
-  for (int idx = threadIdx.x; idx < TL * npad; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < TL * npad; idx += TL * G) {
     const int l = idx / npad, r = idx - l * npad;
     const long long s = s0 + l;
     if (s >= nsys) continue;
@@ -40,28 +42,28 @@ __global__ void __launch_bounds__(256) tri_contig_kernel(const R* __restrict__ a
       rc = r == n - 1 ? R(0) : c[g];
       rd = d[g];
     }
-    const int lane = r / m;
-    const int o = lane * mp + (r - lane * m);
-    R* base = sm + l * 4 * chunk;
-    base[o] = ra; base[chunk + o] = rb; base[2 * chunk + o] = rc; base[3 * chunk + o] = rd;
+    const int ch = r / m;
+    const size_t o = (size_t)l * LS + (size_t)ch * mp + (r - ch * m);
+    sm[o] = ra; sm[o + arr] = rb; sm[o + 2 * arr] = rc; sm[o + 3 * arr] = rd;
   }
   __syncthreads();
-  const int w = threadIdx.x >> 5;
-  if (w < TL && s0 + w < nsys) {
-    R* base = sm + w * 4 * chunk;
+  {
+    const int l = threadIdx.x / G;
+    const bool active = s0 + l < nsys;
+    R* line = sm + (size_t)l * LS;
     if (SOLVER == IXB_SOLVER_EXACT) {
-      if ((threadIdx.x & 31) == 0) thomas_exact(base, base + chunk, base + 2 * chunk, base + 3 * chunk, n, m, mp);
+      if (active && threadIdx.x % G == 0) thomas_exact(line, line + arr, line + 2 * arr, line + 3 * arr, n, m, mp);
     } else {
-      thomas_pcr_warp(base, base + chunk, base + 2 * chunk, base + 3 * chunk, m, mp);
+      chunk_solve<R, G>(line, m, mp, active, RS_WARP);
     }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < TL * n; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < TL * n; idx += TL * G) {
     const int l = idx / n, r = idx - l * n;
     const long long s = s0 + l;
     if (s >= nsys) continue;
-    const int lane = r / m;
-    x[(size_t)s * n + r] = sm[l * 4 * chunk + 3 * chunk + lane * mp + (r - lane * m)];
+    const int ch = r / m;
+    x[(size_t)s * n + r] = sm[(size_t)l * LS + 3 * arr + (size_t)ch * mp + (r - ch * m)];
   }
 }
 
@@ -121,12 +123,11 @@ __global__ void __launch_bounds__(128) tri_inter_kernel(const R* __restrict__ a,
 template <class R, int SOLVER, int TL>
 static cudaError_t contig_tl(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, int m, int mp,
                              size_t smem, cudaStream_t st) {
-  auto k = tri_contig_kernel<R, SOLVER, TL>;
+  auto k = tri_contig_kernel<R, SOLVER, TL, 256 / TL>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int grid = (nsys + TL - 1) / TL;
-  const int nt = std::max(128, 32 * TL);
-  k<<<grid, nt, smem, st>>>(a, b, c, d, x, n, nsys, m, mp);
+  k<<<grid, 256, smem, st>>>(a, b, c, d, x, n, nsys, m, mp);
   return cudaGetLastError();
 }
 
@@ -134,20 +135,21 @@ template <class R, int SOLVER>
 static cudaError_t tridiag_impl(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, int layout,
                                 cudaStream_t st) {
   if (layout == 0) {
-    const int m = std::max(3, (n + 31) / 32);
+    int g = 32;
+    while (g < 256 && 3 * g < n) g <<= 1;
+    const int tl = 256 / g;
+    const int m = std::max(3, (n + g - 1) / g);
     const int mp = m | 1;
-    const size_t per = (size_t)4 * 32 * mp * sizeof(R);
+    const size_t smem = line_smem_elems(g, mp) * sizeof(R) * tl;
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (per > (size_t)optin) return cudaErrorInvalidValue;  // line too long for one CTA
-    int tl = 1;
-    while (tl < 8 && per * tl * 2 <= 96 * 1024 && tl * 2 <= nsys) tl *= 2;
+    if (smem > (size_t)optin) return cudaErrorInvalidValue;  // line too long for one CTA
     switch (tl) {
-      case 1: return contig_tl<R, SOLVER, 1>(a, b, c, d, x, n, nsys, m, mp, per, st);
-      case 2: return contig_tl<R, SOLVER, 2>(a, b, c, d, x, n, nsys, m, mp, per * 2, st);
-      case 4: return contig_tl<R, SOLVER, 4>(a, b, c, d, x, n, nsys, m, mp, per * 4, st);
-      default: return contig_tl<R, SOLVER, 8>(a, b, c, d, x, n, nsys, m, mp, per * 8, st);
+      case 1: return contig_tl<R, SOLVER, 1>(a, b, c, d, x, n, nsys, m, mp, smem, st);
+      case 2: return contig_tl<R, SOLVER, 2>(a, b, c, d, x, n, nsys, m, mp, smem, st);
+      case 4: return contig_tl<R, SOLVER, 4>(a, b, c, d, x, n, nsys, m, mp, smem, st);
+      default: return contig_tl<R, SOLVER, 8>(a, b, c, d, x, n, nsys, m, mp, smem, st);
     }
   }
   R* work = nullptr;

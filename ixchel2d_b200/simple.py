@@ -124,6 +124,18 @@ class Simple2D:
         F.check(F.lib.ixb_nusselt_y(self.h, i0, i1, C.byref(a), C.byref(b)), "ixb_nusselt_y")
         return a.value, b.value
 
+    SHAPES = ((1, 128), (1, 256), (2, 64), (2, 128), (4, 32), (4, 64), (8, 32))
+
+    def set_sweep_shape(self, sweep: int, lines_per_cta: int = 0, threads_per_line: int = 0):
+        F.check(F.lib.ixb_set_sweep_shape(self.h, sweep, lines_per_cta, threads_per_line), "ixb_set_sweep_shape")
+
+    def autotune(self, reps: int = 5, flush_bytes: int = 0) -> dict:
+        """Pick the fastest launch shape of every sweep; returns {sweep: (lines_per_cta, threads_per_line, ms)}."""
+        chosen = (C.c_int * 16)()
+        ms = np.zeros(8)
+        F.check(F.lib.ixb_autotune(self.h, reps, flush_bytes, chosen, F.dptr(ms)), "ixb_autotune")
+        return {k: (chosen[2 * k], chosen[2 * k + 1], float(ms[k])) for k in range(8)}
+
     def set_stream(self, stream_handle: int):
         """Launch on an external cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
         F.check(F.lib.ixb_set_stream(self.h, C.c_void_p(stream_handle)), "ixb_set_stream")

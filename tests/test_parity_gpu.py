@@ -115,6 +115,35 @@ def test_natural_cavity_64_two_thousand_iterations():
     assert abs(ng[0] - no[0]) < 1e-10 and abs(ng[1] - no[1]) < 1e-10
 
 
+@pytest.mark.parametrize("shape", Simple2D.SHAPES)
+def test_every_launch_shape_keeps_parity(shape):
+    case = cases.lid_driven_mixed(45, 29)
+    g, o = _pair(case)
+    for k in range(8):
+        g.set_sweep_shape(k, *shape)
+    g.iterations(60)
+    o.iterations(60)
+    gs, os_ = g.download(), o.get_state()
+    for k in STATE:
+        assert relerr(gs[k], os_[k]) < HYBRID_TOL, (k, relerr(gs[k], os_[k]))
+
+
+def test_autotune_then_parity():
+    case = cases.natural_cavity(40, 36, Ra=1e5)
+    g, o = _pair(case)
+    before = g.download()
+    chosen = g.autotune(reps=2)
+    after = g.download()
+    for k in STATE:
+        assert np.array_equal(before[k], after[k]), k  # state restored
+    assert all((c[0], c[1]) in Simple2D.SHAPES for c in chosen.values())
+    g.iterations(80)
+    o.iterations(80)
+    gs, os_ = g.download(), o.get_state()
+    for k in STATE:
+        assert relerr(gs[k], os_[k]) < HYBRID_TOL, k
+
+
 def test_graph_and_host_driven_loops_agree(monkeypatch):
     case = cases.natural_cavity(20, 24, Ra=1e4)
     over = dict(conv_u=2e-3, conv_p=5e-3, conv_t=1e-3, iter_ecuaci_max=3, iter_simple_max=6,
