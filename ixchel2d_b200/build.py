@@ -49,7 +49,11 @@ def _stale(src: Path, obj: Path, newest_header: float) -> bool:
 
 def _compile(src: Path, obj: Path, extra: list[str]) -> tuple[Path, str]:
     if src.suffix == ".cu":
-        cmd = [_nvcc(), *ARCH, *NVFLAGS, *extra, "-c", str(src), "-o", str(obj)]
+        flags = list(NVFLAGS)
+        if src.stem.endswith("_fast"):
+            # the fast (tolerance-checked) kernels may contract a*b+c into FMA
+            flags[flags.index("-fmad=false")] = "-fmad=true"
+        cmd = [_nvcc(), *ARCH, *flags, *extra, "-c", str(src), "-o", str(obj)]
     else:
         cmd = [HOST_CXX, *CXXFLAGS, "-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -103,6 +103,8 @@ Geo<double> make_geo(const ixb_handle* h) {
   G.gm = h->prm.gamma_momen; G.ge = h->prm.gamma_energ; G.Ri = h->prm.Ri; G.Riy = h->prm.Riy;
   G.dt = h->prm.dt; G.rel_vel = h->prm.rel_vel; G.rel_pres = h->prm.rel_pres; G.rel_ener = h->prm.rel_ener;
   G.p_update = h->prm.p_update;
+  G.inv_gm = 1.0 / G.gm; G.inv_dt = 1.0 / G.dt; G.inv_rel_vel = 1.0 / G.rel_vel;
+  G.inv_rel_pres = 1.0 / G.rel_pres; G.inv_rel_ener = 1.0 / G.rel_ener;
   return G;
 }
 
@@ -193,14 +195,15 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
 
 int correct(ixb_handle* h) {
   Geo<double> G = make_geo(h);
-  CK(launch_correct_f64(G, h->u[h->cu], h->v[h->cv], h->p, h->pc[h->cpc], h->au, h->av, h->stream));
+  CK(launch_correct_f64(G, h->u[h->cu], h->v[h->cv], h->p, h->pc[h->cpc], h->au, h->av,
+                         h->prm.solver == IXB_SOLVER_HYBRID, h->stream));
   return IXB_OK;
 }
 
 int residual(ixb_handle* h) {
   Geo<double> G = make_geo(h);
   CK(launch_residual_f64(G, h->u[h->cu], h->v[h->cv], h->T[h->cT], h->p, h->u_ant, h->fcon[0], h->flin[0],
-                         h->resu, slot(h, N_RES), h->stream));
+                         h->resu, slot(h, N_RES), h->prm.solver == IXB_SOLVER_HYBRID, h->stream));
   return IXB_OK;
 }
 

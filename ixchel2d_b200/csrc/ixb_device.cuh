@@ -19,8 +19,12 @@ namespace ixb {
 
 // metric arrays inside one device buffer, each `mstride` long, 1-based.
 // M_HXU/M_HYV are the energy equation's face diffusivities
-// hmean(ge,ge,fexu(k)) / hmean(ge,ge,feyv(k)), filled by the table kernel.
-enum Metric { M_DXP = 0, M_DYP, M_DXU, M_DYU, M_DXV, M_DYV, M_FEXP, M_FEYP, M_FEXU, M_FEYV, M_HXU, M_HYV, M_COUNT };
+// hmean(ge,ge,fexu(k)) / hmean(ge,ge,feyv(k)), M_RHXU/M_RHYV their
+// reciprocals (fast form), filled by the table kernel.
+enum Metric {
+  M_DXP = 0, M_DYP, M_DXU, M_DYU, M_DXV, M_DYV, M_FEXP, M_FEYP, M_FEXU, M_FEYV,
+  M_HXU, M_HYV, M_RHXU, M_RHYV, M_COUNT
+};
 
 // Mesh-constant 2-D tables (field layout).  With the uniform diffusion
 // coefficients of the reference (main.f90:226-239) every harmonic face
@@ -36,7 +40,8 @@ enum Metric { M_DXP = 0, M_DYP, M_DXU, M_DYU, M_DXV, M_DYV, M_FEXP, M_FEYP, M_FE
 //   T_CV2(ii,jj)  v: gammas*deltaxv/ds; BN conductance = T_CV2(ii,jj+1)
 //   T_CT1(ii,jj)  T: gammai*deltayp/di; AD conductance = T_CT1(ii+1,jj)
 //   T_CT2(ii,jj)  T: gamman*deltaxp/dn; BS conductance = T_CT2(ii,jj-1)
-enum Table { T_GU = 0, T_CU1, T_CU2, T_GV, T_CV1, T_CV2, T_CT1, T_CT2, T_COUNT };
+//   T_RGU, T_RGV  1/T_GU, 1/T_GV (fast form: Peclet numbers by multiplication)
+enum Table { T_GU = 0, T_CU1, T_CU2, T_GV, T_CV1, T_CV2, T_CT1, T_CT2, T_RGU, T_RGV, T_COUNT };
 
 // sweeps: the eight line-solve phases of main.f90
 enum Eq { EQ_UY = 0, EQ_UX, EQ_VY, EQ_VX, EQ_PY, EQ_PX, EQ_TY, EQ_TX, EQ_COUNT };
@@ -66,6 +71,7 @@ struct Geo {
   const R* m;      // M_COUNT 1-D arrays
   const R* tab;    // T_COUNT 2-D tables
   R gm, ge, Ri, Riy, dt, rel_vel, rel_pres, rel_ener, p_update;
+  R inv_gm, inv_dt, inv_rel_vel, inv_rel_pres, inv_rel_ener;  // fast form
   __device__ __forceinline__ R met(int which, int k) const { return __ldg(m + which * mstride + k); }
   __device__ __forceinline__ int at(int ii, int jj) const { return (jj - 1) * LD + (ii - 1); }
   __device__ __forceinline__ R t(int which, int ii, int jj) const { return __ldg(tab + which * tstride + at(ii, jj)); }
@@ -110,13 +116,36 @@ __device__ __forceinline__ R hmean(R g1, R g2, R f) {
   return (g1 * g2) / (g1 * (R(1) - f) + g2 * f);
 }
 
+// Reciprocal for the fast form: Newton-Raphson refinement
+// r <- r + r(1 - x r) of a hardware reciprocal estimate (two steps for
+// binary64, one for binary32).
+__device__ __forceinline__ double fast_rcp(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  r = fma(r, fma(-x, r, 1.0), r);
+  r = fma(r, fma(-x, r, 1.0), r);
+  return r;
+}
+__device__ __forceinline__ float fast_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return fmaf(r, fmaf(-x, r, 1.0f), r);
+}
+
+// a / b.  EXACT (FAST=false): the IEEE quotient of the reference.  FAST:
+// a * rb with rb ~ 1/b precomputed (or, when rb is not given, estimated).
+template <bool FAST, class R>
+__device__ __forceinline__ R qdiv(R a, R b, R rb) { if constexpr (FAST) return a * rb; else return a / b; }
+template <bool FAST, class R>
+__device__ __forceinline__ R qdiv(R a, R b) { if constexpr (FAST) return a * fast_rcp(b); else return a / b; }
+
 // ---------------------------------------------------------------------------
 // u momentum (ensambla_velu_x/_y, source/mod_ec_momento.f90:365-724)
 // ---------------------------------------------------------------------------
 // The four neighbour coefficients of the u row (:512-526), face velocities
 // interpolated as in :447-455, diffusivities and conductances from the
 // tables (gammai = gammad = gamma_momen).
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<R>& io, const R* u, int ii, int jj,
                                         R& AI, R& AD, R& BS, R& BN, R& deltax, R& deltay, R& temp_int) {
   const R* v = io.v;
@@ -127,53 +156,62 @@ __device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<R>& io, c
   R vn = fexp_i * ldg(v, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj));
   R vs = fexp_i * ldg(v, G.at(ii + 1, jj - 1)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj - 1));
   const R g = G.gm;
-  const R gamman = G.t(T_GU, ii, jj);
-  const R gammas = G.t(T_GU, ii, jj - 1);
+  R gamman, gammas, rgn = R(0), rgs = R(0);
+  if constexpr (FAST) {
+    rgn = G.t(T_RGU, ii, jj);
+    rgs = G.t(T_RGU, ii, jj - 1);
+    gamman = gammas = R(0);
+  } else {
+    gamman = G.t(T_GU, ii, jj);
+    gammas = G.t(T_GU, ii, jj - 1);
+  }
   R di = G.met(M_DXP, ii), dd = G.met(M_DXP, ii + 1), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   deltax = G.met(M_DXU, ii);
   deltay = G.met(M_DYU, jj);
   temp_int = fexp_i * ldg(io.T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(io.T, G.at(ii, jj));
-  AI = -(G.t(T_CU1, ii, jj) * plaw(ui * di / g) + dmax0(ui * deltay));
-  AD = -(G.t(T_CU1, ii + 1, jj) * plaw(ud * dd / g) + dmax0(-ud * deltay));
-  BS = -(G.t(T_CU2, ii, jj - 1) * plaw(vs * ds / gammas) + dmax0(vs * deltax));
-  BN = -(G.t(T_CU2, ii, jj) * plaw(vn * dn / gamman) + dmax0(-vn * deltax));
+  AI = -(G.t(T_CU1, ii, jj) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * deltay));
+  AD = -(G.t(T_CU1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) + dmax0(-ud * deltay));
+  BS = -(G.t(T_CU2, ii, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) + dmax0(vs * deltax));
+  BN = -(G.t(T_CU2, ii, jj) * plaw(qdiv<FAST>(vn * dn, gamman, rgn)) + dmax0(-vn * deltax));
 }
 
 // X form (ensambla_velu_x): a=AI c=AD b=AC d=Rx, aux = au = AC*rel
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_ux(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& au) {
   const R* u = io.in;
   R AI, AD, BS, BN, dx, dy, tint;
-  u_parts(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
+  u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
   const R flin = io.flin ? ldg(io.flin, c0) : R(0);
   const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
-  r.b = (-AI - AD - BS - BN - dx * dy * flin + dx * dy / G.dt) / G.rel_vel;
+  r.b = qdiv<FAST>(-AI - AD - BS - BN - dx * dy * flin + qdiv<FAST>(dx * dy, G.dt, G.inv_dt), G.rel_vel,
+                   G.inv_rel_vel);
   r.d = -BS * ldg(u, G.at(ii, jj - 1)) - BN * ldg(u, G.at(ii, jj + 1)) - dx * dy * G.Ri * tint + dx * dy * fcon +
-        dx * dy * ldg(io.u_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
+        qdiv<FAST>(dx * dy * ldg(io.u_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
         r.b * (R(1) - G.rel_vel) * ldg(u, c0);
   au = r.b * G.rel_vel;
   return r;
 }
 
 // Y form (ensambla_velu_y): a=BS c=BN b=BC d=Ry
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_uy(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
   const R* u = io.in;
   R AI, AD, BS, BN, dx, dy, tint;
-  u_parts(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
+  u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
   const R flin = io.flin ? ldg(io.flin, c0) : R(0);
   const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
-  r.b = (-AI - AD - BS - BN - dx * dy * flin + dx * dy / G.dt) / G.rel_vel;
+  r.b = qdiv<FAST>(-AI - AD - BS - BN - dx * dy * flin + qdiv<FAST>(dx * dy, G.dt, G.inv_dt), G.rel_vel,
+                   G.inv_rel_vel);
   r.d = -AI * ldg(u, G.at(ii - 1, jj)) - AD * ldg(u, G.at(ii + 1, jj)) - dx * dy * G.Ri * tint + dx * dy * fcon +
-        dx * dy * ldg(io.u_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
+        qdiv<FAST>(dx * dy * ldg(io.u_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
         r.b * (R(1) - G.rel_vel) * ldg(u, c0);
   return r;
 }
@@ -181,7 +219,7 @@ __device__ __forceinline__ Row<R> assemble_uy(const Geo<R>& G, const SweepIO<R>&
 // ---------------------------------------------------------------------------
 // v momentum (ensambla_velv_x/_y, source/mod_ec_momento.f90:736-1098)
 // ---------------------------------------------------------------------------
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<R>& io, const R* v, int ii, int jj,
                                         R& AI, R& AD, R& BS, R& BN, R& temp_int) {
   const R* u = io.u;
@@ -192,22 +230,29 @@ __device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<R>& io, c
   R vn = feyv_j * ldg(v, G.at(ii, jj + 1)) + (R(1) - feyv_j) * ldg(v, G.at(ii, jj));
   R vs = feyv_m * ldg(v, G.at(ii, jj)) + (R(1) - feyv_m) * ldg(v, G.at(ii, jj - 1));
   const R g = G.gm;  // gamman = gammas = gamma_momen (:854-858)
-  const R gammad = G.t(T_GV, ii, jj);
-  const R gammai = G.t(T_GV, ii - 1, jj);
+  R gammad, gammai, rgd = R(0), rgi = R(0);
+  if constexpr (FAST) {
+    rgd = G.t(T_RGV, ii, jj);
+    rgi = G.t(T_RGV, ii - 1, jj);
+    gammad = gammai = R(0);
+  } else {
+    gammad = G.t(T_GV, ii, jj);
+    gammai = G.t(T_GV, ii - 1, jj);
+  }
   R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYP, jj), dn = G.met(M_DYP, jj + 1);
   const R dyv = G.met(M_DYV, jj), dxv = G.met(M_DXV, ii);
   temp_int = feyp_j * ldg(io.T, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ldg(io.T, G.at(ii, jj));
-  AI = -(G.t(T_CV1, ii, jj) * plaw(ui * di / gammai) + dmax0(ui * dyv));
-  AD = -(G.t(T_CV1, ii + 1, jj) * plaw(ud * dd / gammad) + dmax0(-ud * dyv));
-  BS = -(G.t(T_CV2, ii, jj) * plaw(vs * ds / g) + dmax0(vs * dxv));
-  BN = -(G.t(T_CV2, ii, jj + 1) * plaw(vn * dn / g) + dmax0(-vn * dxv));
+  AI = -(G.t(T_CV1, ii, jj) * plaw(qdiv<FAST>(ui * di, gammai, rgi)) + dmax0(ui * dyv));
+  AD = -(G.t(T_CV1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, gammad, rgd)) + dmax0(-ud * dyv));
+  BS = -(G.t(T_CV2, ii, jj) * plaw(qdiv<FAST>(vs * ds, g, G.inv_gm)) + dmax0(vs * dxv));
+  BN = -(G.t(T_CV2, ii, jj + 1) * plaw(qdiv<FAST>(vn * dn, g, G.inv_gm)) + dmax0(-vn * dxv));
 }
 
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_vx(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& av) {
   const R* v = io.in;
   R AI, AD, BS, BN, tint;
-  v_parts(G, io, v, ii, jj, AI, AD, BS, BN, tint);
+  v_parts<FAST>(G, io, v, ii, jj, AI, AD, BS, BN, tint);
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
@@ -216,19 +261,19 @@ __device__ __forceinline__ Row<R> assemble_vx(const Geo<R>& G, const SweepIO<R>&
   Row<R> r;
   r.a = AI;
   r.c = AD;
-  r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_vel;
+  r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_vel, G.inv_rel_vel);
   r.d = -BS * ldg(v, G.at(ii, jj - 1)) - BN * ldg(v, G.at(ii, jj + 1)) - dxdy * G.Riy * tint + dxdy * fcon +
-        dxdy * ldg(io.v_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
+        qdiv<FAST>(dxdy * ldg(io.v_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
         r.b * (R(1) - G.rel_vel) * ldg(v, c0);
   av = r.b * G.rel_vel;
   return r;
 }
 
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
   const R* v = io.in;
   R AI, AD, BS, BN, tint;
-  v_parts(G, io, v, ii, jj, AI, AD, BS, BN, tint);
+  v_parts<FAST>(G, io, v, ii, jj, AI, AD, BS, BN, tint);
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
@@ -237,9 +282,9 @@ __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<R>&
   Row<R> r;
   r.a = BS;
   r.c = BN;
-  r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_vel;
+  r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_vel, G.inv_rel_vel);
   r.d = -AI * ldg(v, G.at(ii - 1, jj)) - AD * ldg(v, G.at(ii + 1, jj)) - dxdy * G.Riy * tint + dxdy * fcon +
-        dxdy * ldg(io.v_ant, c0) / G.dt + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
+        qdiv<FAST>(dxdy * ldg(io.v_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
         r.b * (R(1) - G.rel_vel) * ldg(v, c0);
   return r;
 }
@@ -248,28 +293,35 @@ __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<R>&
 // energy (ensambla_energia_x/_y, source/mod_ec_energia.f90:119-443).  The
 // calls in main.f90:989 and :1060 bind fexu/feyv to the dummies fexpo/feypo.
 // ---------------------------------------------------------------------------
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ void t_parts(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& AI, R& AD,
                                         R& BS, R& BN) {
   const R ud = ldg(io.u, G.at(ii, jj)), ui = ldg(io.u, G.at(ii - 1, jj));
   const R vn = ldg(io.v, G.at(ii, jj)), vs = ldg(io.v, G.at(ii, jj - 1));
   const R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
-  const R gammad = G.met(M_HXU, ii);
-  const R gammai = G.met(M_HXU, ii - 1);
-  const R gamman = G.met(M_HYV, jj);
-  const R gammas = G.met(M_HYV, jj - 1);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
-  AI = -(G.t(T_CT1, ii, jj) * plaw(ui * di / gammai) + dmax0(ui * dyp));
-  AD = -(G.t(T_CT1, ii + 1, jj) * plaw(ud * dd / gammad) + dmax0(-ud * dyp));
-  BS = -(G.t(T_CT2, ii, jj - 1) * plaw(vs * ds / gammas) + dmax0(vs * dxp));
-  BN = -(G.t(T_CT2, ii, jj) * plaw(vn * dn / gamman) + dmax0(-vn * dxp));
+  if constexpr (FAST) {
+    AI = -(G.t(T_CT1, ii, jj) * plaw(ui * di * G.met(M_RHXU, ii - 1)) + dmax0(ui * dyp));
+    AD = -(G.t(T_CT1, ii + 1, jj) * plaw(ud * dd * G.met(M_RHXU, ii)) + dmax0(-ud * dyp));
+    BS = -(G.t(T_CT2, ii, jj - 1) * plaw(vs * ds * G.met(M_RHYV, jj - 1)) + dmax0(vs * dxp));
+    BN = -(G.t(T_CT2, ii, jj) * plaw(vn * dn * G.met(M_RHYV, jj)) + dmax0(-vn * dxp));
+  } else {
+    const R gammad = G.met(M_HXU, ii);
+    const R gammai = G.met(M_HXU, ii - 1);
+    const R gamman = G.met(M_HYV, jj);
+    const R gammas = G.met(M_HYV, jj - 1);
+    AI = -(G.t(T_CT1, ii, jj) * plaw(ui * di / gammai) + dmax0(ui * dyp));
+    AD = -(G.t(T_CT1, ii + 1, jj) * plaw(ud * dd / gammad) + dmax0(-ud * dyp));
+    BS = -(G.t(T_CT2, ii, jj - 1) * plaw(vs * ds / gammas) + dmax0(vs * dxp));
+    BN = -(G.t(T_CT2, ii, jj) * plaw(vn * dn / gamman) + dmax0(-vn * dxp));
+  }
 }
 
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_tx(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
   const R* T = io.in;
   R AI, AD, BS, BN;
-  t_parts(G, io, ii, jj, AI, AD, BS, BN);
+  t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
   const R flin = io.flin ? ldg(io.flin, c0) : R(0);
@@ -277,17 +329,17 @@ __device__ __forceinline__ Row<R> assemble_tx(const Geo<R>& G, const SweepIO<R>&
   Row<R> r;
   r.a = AI;
   r.c = AD;
-  r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_ener;
-  r.d = -BS * ldg(T, G.at(ii, jj - 1)) - BN * ldg(T, G.at(ii, jj + 1)) + dxdy * fcon + dxdy * ldg(io.T_ant, c0) / G.dt +
-        r.b * (R(1) - G.rel_ener) * ldg(T, c0);
+  r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_ener, G.inv_rel_ener);
+  r.d = -BS * ldg(T, G.at(ii, jj - 1)) - BN * ldg(T, G.at(ii, jj + 1)) + dxdy * fcon +
+        qdiv<FAST>(dxdy * ldg(io.T_ant, c0), G.dt, G.inv_dt) + r.b * (R(1) - G.rel_ener) * ldg(T, c0);
   return r;
 }
 
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
   const R* T = io.in;
   R AI, AD, BS, BN;
-  t_parts(G, io, ii, jj, AI, AD, BS, BN);
+  t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
   const R flin = io.flin ? ldg(io.flin, c0) : R(0);
@@ -295,9 +347,9 @@ __device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<R>&
   Row<R> r;
   r.a = BS;
   r.c = BN;
-  r.b = (-AI - AD - BS - BN - dxdy * flin + dxdy / G.dt) / G.rel_ener;
-  r.d = -AI * ldg(T, G.at(ii - 1, jj)) - AD * ldg(T, G.at(ii + 1, jj)) + dxdy * fcon + dxdy * ldg(io.T_ant, c0) / G.dt +
-        r.b * (R(1) - G.rel_ener) * ldg(T, c0);
+  r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_ener, G.inv_rel_ener);
+  r.d = -AI * ldg(T, G.at(ii - 1, jj)) - AD * ldg(T, G.at(ii + 1, jj)) + dxdy * fcon +
+        qdiv<FAST>(dxdy * ldg(io.T_ant, c0), G.dt, G.inv_dt) + r.b * (R(1) - G.rel_ener) * ldg(T, c0);
   return r;
 }
 
@@ -309,36 +361,36 @@ __device__ __forceinline__ R pc_at(const SweepIO<R>& io, const Geo<R>& G, int ii
   return io.in ? ldg(io.in, G.at(ii, jj)) : R(0);
 }
 
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& bo) {
   const int c0 = G.at(ii, jj);
   const R ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
   const R ai = ldg(io.au, G.at(ii - 1, jj)), ad = ldg(io.au, c0), as = ldg(io.av, G.at(ii, jj - 1)), an = ldg(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   Row<R> r;
-  r.a = -dyp * dyp / ai;
-  r.c = -dyp * dyp / ad;
-  const R BS = -dxp * dxp / as;
-  const R BN = -dxp * dxp / an;
-  r.b = (-r.a - r.c - BS - BN) / G.rel_pres;
+  r.a = -qdiv<FAST>(dyp * dyp, ai);
+  r.c = -qdiv<FAST>(dyp * dyp, ad);
+  const R BS = -qdiv<FAST>(dxp * dxp, as);
+  const R BN = -qdiv<FAST>(dxp * dxp, an);
+  r.b = qdiv<FAST>(-r.a - r.c - BS - BN, G.rel_pres, G.inv_rel_pres);
   bo = (ui - ud) * dyp + (vs - vn) * dxp;
   r.d = -BS * pc_at(io, G, ii, jj - 1) - BN * pc_at(io, G, ii, jj + 1) + bo +
         (R(1) - G.rel_pres) * r.b * pc_at(io, G, ii, jj);
   return r;
 }
 
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
   const int c0 = G.at(ii, jj);
   const R ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
   const R ai = ldg(io.au, G.at(ii - 1, jj)), ad = ldg(io.au, c0), as = ldg(io.av, G.at(ii, jj - 1)), an = ldg(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
-  const R AI = -dyp * dyp / ai;
-  const R AD = -dyp * dyp / ad;
+  const R AI = -qdiv<FAST>(dyp * dyp, ai);
+  const R AD = -qdiv<FAST>(dyp * dyp, ad);
   Row<R> r;
-  r.a = -dxp * dxp / as;
-  r.c = -dxp * dxp / an;
-  r.b = (-AI - AD - r.a - r.c) / G.rel_pres;
+  r.a = -qdiv<FAST>(dxp * dxp, as);
+  r.c = -qdiv<FAST>(dxp * dxp, an);
+  r.b = qdiv<FAST>(-AI - AD - r.a - r.c, G.rel_pres, G.inv_rel_pres);
   const R bo = (ui - ud) * dyp + (vs - vn) * dxp;
   r.d = -AI * pc_at(io, G, ii - 1, jj) - AD * pc_at(io, G, ii + 1, jj) + bo +
         (R(1) - G.rel_pres) * r.b * pc_at(io, G, ii, jj);
@@ -350,7 +402,7 @@ __device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<R>&
 // uniform gamma the reference's different south numerator (:1208) has the
 // same value as in ensambla_velu_x, so it shares the u tables.
 // ---------------------------------------------------------------------------
-template <class R>
+template <bool FAST, class R>
 __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v, const R* T, const R* p,
                                         const R* u_ant, const R* fcon, const R* flin, int ii, int jj) {
   const R fexu_i = G.met(M_FEXU, ii), fexu_m = G.met(M_FEXU, ii - 1);
@@ -360,21 +412,29 @@ __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v,
   R vn = fexp_i * ldg(v, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj));
   R vs = fexp_i * ldg(v, G.at(ii + 1, jj - 1)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj - 1));
   const R g = G.gm;
-  const R gamman = G.t(T_GU, ii, jj);
-  const R gammas = G.t(T_GU, ii, jj - 1);
+  R gamman, gammas, rgn = R(0), rgs = R(0);
+  if constexpr (FAST) {
+    rgn = G.t(T_RGU, ii, jj);
+    rgs = G.t(T_RGU, ii, jj - 1);
+    gamman = gammas = R(0);
+  } else {
+    gamman = G.t(T_GU, ii, jj);
+    gammas = G.t(T_GU, ii, jj - 1);
+  }
   R di = G.met(M_DXP, ii), dd = G.met(M_DXP, ii + 1), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   const R dxu = G.met(M_DXU, ii), dyu = G.met(M_DYU, jj);
   const int c0 = G.at(ii, jj);
   R temp_int = fexp_i * ldg(T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(T, c0);
-  R AI = (G.t(T_CU1, ii, jj) * plaw(ui * di / g) + dmax0(ui * dyu));
-  R AD = (G.t(T_CU1, ii + 1, jj) * plaw(ud * dd / g) + dmax0(-ud * dyu));
-  R BS = (G.t(T_CU2, ii, jj - 1) * plaw(vs * ds / gammas) + dmax0(vs * dxu));
-  R BN = (G.t(T_CU2, ii, jj) * plaw(vn * dn / gamman) + dmax0(-vn * dxu));
+  R AI = (G.t(T_CU1, ii, jj) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * dyu));
+  R AD = (G.t(T_CU1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) + dmax0(-ud * dyu));
+  R BS = (G.t(T_CU2, ii, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) + dmax0(vs * dxu));
+  R BN = (G.t(T_CU2, ii, jj) * plaw(qdiv<FAST>(vn * dn, gamman, rgn)) + dmax0(-vn * dxu));
   const R fl = flin ? ldg(flin, c0) : R(0);
   const R fc = fcon ? ldg(fcon, c0) : R(0);
-  R AC = AI + AD + BS + BN - dxu * dyu * fl + dxu * dyu / G.dt;
-  return AI * ldg(u, G.at(ii - 1, jj)) - AC * ldg(u, c0) + AD * ldg(u, G.at(ii + 1, jj)) + BS * ldg(u, G.at(ii, jj - 1)) +
-         BN * ldg(u, G.at(ii, jj + 1)) - dxu * dyu * G.Ri * temp_int + dxu * dyu * fc + dxu * dyu * ldg(u_ant, c0) / G.dt +
+  R AC = AI + AD + BS + BN - dxu * dyu * fl + qdiv<FAST>(dxu * dyu, G.dt, G.inv_dt);
+  return AI * ldg(u, G.at(ii - 1, jj)) - AC * ldg(u, c0) + AD * ldg(u, G.at(ii + 1, jj)) +
+         BS * ldg(u, G.at(ii, jj - 1)) + BN * ldg(u, G.at(ii, jj + 1)) - dxu * dyu * G.Ri * temp_int +
+         dxu * dyu * fc + qdiv<FAST>(dxu * dyu * ldg(u_ant, c0), G.dt, G.inv_dt) +
          (ldg(p, c0) - ldg(p, G.at(ii + 1, jj))) * dyu;
 }
 
@@ -520,8 +580,9 @@ __device__ void thomas_pcr_warp(R* sa, R* sb, R* sc, R* sd, int m, int mp) {
 // reduction over all G threads in shared memory (RS_PCR, log2(2G) steps) or
 // by one warp per line with the warp Thomas-PCR hybrid (RS_WARP); finally
 // every thread back-substitutes its chunk.  This is the Thomas-PCR hybrid of
-// Laszlo, Giles and Appleyard (ACM TOMS 42(4), 2016) applied twice.  The
-// solution replaces the right-hand side.  Called by all TL*G threads;
+// Laszlo, Giles and Appleyard (ACM TOMS 42(4), 2016) applied twice.
+// Reciprocals use fast_rcp (two Newton steps).  The solution replaces the
+// right-hand side.  Called by all TL*G threads;
 // threads of lines with `active` false only take part in the barriers.
 template <class R, int G>
 __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active, int rs) {
@@ -537,12 +598,12 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
   if (active) {
     // forward: rows 1..m-1 -> x_k + a'_k x_0 + c'_k x_{k+1} = d'_k
     const R a0 = a[0], b0 = b[0], c0 = c[0], d0 = d[0];
-    R inv = R(1) / b[1];
+    R inv = fast_rcp(b[1]);
     R ap = a[1] * inv, cp = c[1] * inv, dp = d[1] * inv;
     a[1] = ap; c[1] = cp; d[1] = dp;
     for (int i = 2; i < m; ++i) {
       const R ai = a[i];
-      const R r = R(1) / fma(-ai, cp, b[i]);
+      const R r = fast_rcp(fma(-ai, cp, b[i]));
       ap = -ai * ap * r;
       dp = fma(-ai, dp, d[i]) * r;
       cp = c[i] * r;
@@ -558,7 +619,7 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
       a[i] = an; c[i] = cn; d[i] = dn;
     }
     // reduced rows 2k (chunk's first row) and 2k+1 (its last row), unit diagonal
-    const R r0 = R(1) / fma(-c0, an, b0);
+    const R r0 = fast_rcp(fma(-c0, an, b0));
     eA = a0 * r0; eC = -c0 * cn * r0; eD = fma(-c0, dn, d0) * r0;
     oA = ap; oC = cp; oD = dp;
   }
@@ -585,7 +646,7 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
           R alo = R(0), clo = R(0), dlo = R(0), ahi = R(0), chi = R(0), dhi = R(0);
           if (i - s >= 0) { alo = Ac[i - s]; clo = Cc[i - s]; dlo = Dc[i - s]; }
           if (i + s < 2 * G) { ahi = Ac[i + s]; chi = Cc[i + s]; dhi = Dc[i + s]; }
-          const R r = R(1) / fma(-ci, ahi, fma(-ai, clo, R(1)));
+          const R r = fast_rcp(fma(-ci, ahi, fma(-ai, clo, R(1))));
           An[i] = -ai * alo * r;
           Cn[i] = -ci * chi * r;
           Dn[i] = fma(-ci, dhi, fma(-ai, dlo, di)) * r;

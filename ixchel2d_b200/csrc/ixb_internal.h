@@ -30,13 +30,13 @@ struct SweepShape {
 // (tl * g = 128 or 256; chunks of max(3, ceil(n/g)) rows).
 SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl, int g);
 
-// per-equation sweep launchers (ixb_sweep_{u,v,p,t}.cu)
-template <class R, int EQ>
-cudaError_t sweep_launch(int solver, const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st);
-template <class R, int EQ>
-cudaError_t sweep_smem_limit(int bytes);
-template <class R, int EQ>
-int sweep_blocks_per_sm(int solver, const SweepShape& s);
+// per-sweep launchers (ixb_sweep_<eq>.cu: exact, ixb_sweep_<eq>_fast.cu: hybrid)
+template <class R, int EQ, int SOLVER>
+cudaError_t sweep_launch_solver(const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st);
+template <class R, int EQ, int SOLVER>
+cudaError_t sweep_smem_limit_solver(int bytes);
+template <class R, int EQ, int SOLVER>
+int sweep_blocks_per_sm_solver(const SweepShape& s);
 int sweep_occupancy(int eq, int solver, const SweepShape& s);
 int max_sweep_lines(int mi, int nj);
 
@@ -44,10 +44,10 @@ int max_sweep_lines(int mi, int nj);
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
                              const SweepIO<double>& io, cudaStream_t st);
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
-                               const double* au, const double* av, cudaStream_t st);
+                               const double* au, const double* av, int fast, cudaStream_t st);
 cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const double* v, const double* T,
                                 const double* p, const double* u_ant, const double* fcon, const double* flin,
-                                double* resu, NormSlot ns, cudaStream_t st);
+                                double* resu, NormSlot ns, int fast, cudaStream_t st);
 int residual_grid(int mi, int nj);
 cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,
                                int vertical, int k0, int k1, double* out2, cudaStream_t st);

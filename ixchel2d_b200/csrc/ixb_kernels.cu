@@ -19,8 +19,16 @@ template <class R>
 __global__ void table1d_kernel(Geo<R> G, R* met) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const R ge = G.ge;
-  if (k >= 1 && k <= G.mi) met[M_HXU * G.mstride + k] = hmean(ge, ge, G.met(M_FEXU, k));
-  if (k >= 1 && k <= G.nj) met[M_HYV * G.mstride + k] = hmean(ge, ge, G.met(M_FEYV, k));
+  if (k >= 1 && k <= G.mi) {
+    const R h = hmean(ge, ge, G.met(M_FEXU, k));
+    met[M_HXU * G.mstride + k] = h;
+    met[M_RHXU * G.mstride + k] = R(1) / h;
+  }
+  if (k >= 1 && k <= G.nj) {
+    const R h = hmean(ge, ge, G.met(M_FEYV, k));
+    met[M_HYV * G.mstride + k] = h;
+    met[M_RHYV * G.mstride + k] = R(1) / h;
+  }
 }
 
 template <class R>
@@ -37,6 +45,7 @@ __global__ void table2d_kernel(Geo<R> G, R* tab) {
     const R hy = hmean(g, g, G.met(M_FEYP, jj));
     const R gamman = combo(hy, G.met(M_FEXP, ii));
     T(T_GU) = gamman;
+    T(T_RGU) = R(1) / gamman;
     T(T_CU2) = gamman * G.met(M_DXU, ii) / G.met(M_DYV, jj);
   }
   if (ii >= 2 && ii <= G.mi && jj >= 2 && jj <= G.nj) T(T_CU1) = g * G.met(M_DYU, jj) / G.met(M_DXP, ii);
@@ -44,6 +53,7 @@ __global__ void table2d_kernel(Geo<R> G, R* tab) {
   if (ii <= G.mi && jj <= G.nj) {
     const R hx = hmean(g, g, G.met(M_FEXP, ii));
     T(T_GV) = combo(hx, G.met(M_FEYP, jj));
+    T(T_RGV) = R(1) / T(T_GV);
   }
   if (ii >= 2 && ii <= G.mi + 1 && jj <= G.nj) {
     const R hx = hmean(g, g, G.met(M_FEXP, ii - 1));
@@ -76,7 +86,7 @@ cudaError_t launch_tables_f64(const Geo<double>& G, double* met, double* tab, cu
 // ---------------------------------------------------------------------------
 // pressure and velocity correction, main.f90:931-962
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, bool FAST>
 __global__ void correct_kernel(const Geo<R> G, R* __restrict__ u, R* __restrict__ v, R* __restrict__ p,
                                const R* __restrict__ pc, const R* __restrict__ au, const R* __restrict__ av) {
   const int ni = G.mi - 1;  // ii = 2..mi
@@ -87,14 +97,14 @@ __global__ void correct_kernel(const Geo<R> G, R* __restrict__ u, R* __restrict_
   const int jj = 2 + idx / ni;
   const size_t c0 = G.at(ii, jj);
   p[c0] = p[c0] + G.p_update * pc[c0];
-  if (ii <= G.mi - 1) u[c0] = u[c0] + G.met(M_DYU, jj) * (pc[c0] - pc[G.at(ii + 1, jj)]) / au[c0];
-  if (jj <= G.nj - 1) v[c0] = v[c0] + G.met(M_DXV, ii) * (pc[c0] - pc[G.at(ii, jj + 1)]) / av[c0];
+  if (ii <= G.mi - 1) u[c0] = u[c0] + qdiv<FAST>(G.met(M_DYU, jj) * (pc[c0] - pc[G.at(ii + 1, jj)]), au[c0]);
+  if (jj <= G.nj - 1) v[c0] = v[c0] + qdiv<FAST>(G.met(M_DXV, ii) * (pc[c0] - pc[G.at(ii, jj + 1)]), av[c0]);
 }
 
 // ---------------------------------------------------------------------------
 // u residual and its norm, main.f90:1169-1199
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, bool FAST>
 __global__ void __launch_bounds__(256) residual_kernel(const Geo<R> G, const R* __restrict__ u,
                                                        const R* __restrict__ v, const R* __restrict__ T,
                                                        const R* __restrict__ p, const R* __restrict__ u_ant,
@@ -106,7 +116,7 @@ __global__ void __launch_bounds__(256) residual_kernel(const Geo<R> G, const R* 
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     const int ii = 2 + idx % ni;
     const int jj = 2 + idx / ni;
-    const R r = residual_u(G, u, v, T, p, u_ant, fcon, flin, ii, jj);
+    const R r = residual_u<FAST>(G, u, v, T, p, u_ant, fcon, flin, ii, jj);
     resu[G.at(ii, jj)] = r;
     acc += (double)r * (double)r;
   }
@@ -184,17 +194,23 @@ SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl, int g) {
   return s;
 }
 
-int sweep_occupancy(int eq, int solver, const SweepShape& s) {
-  switch (eq) {
-    case EQ_UY: return sweep_blocks_per_sm<double, EQ_UY>(solver, s);
-    case EQ_UX: return sweep_blocks_per_sm<double, EQ_UX>(solver, s);
-    case EQ_VY: return sweep_blocks_per_sm<double, EQ_VY>(solver, s);
-    case EQ_VX: return sweep_blocks_per_sm<double, EQ_VX>(solver, s);
-    case EQ_PY: return sweep_blocks_per_sm<double, EQ_PY>(solver, s);
-    case EQ_PX: return sweep_blocks_per_sm<double, EQ_PX>(solver, s);
-    case EQ_TY: return sweep_blocks_per_sm<double, EQ_TY>(solver, s);
-    default:    return sweep_blocks_per_sm<double, EQ_TX>(solver, s);
+#define IXB_EQ_SWITCH(...)                                  \
+  switch (eq) {                                               \
+    case EQ_UY: { constexpr int E_ = EQ_UY; __VA_ARGS__; }           \
+    case EQ_UX: { constexpr int E_ = EQ_UX; __VA_ARGS__; }           \
+    case EQ_VY: { constexpr int E_ = EQ_VY; __VA_ARGS__; }           \
+    case EQ_VX: { constexpr int E_ = EQ_VX; __VA_ARGS__; }           \
+    case EQ_PY: { constexpr int E_ = EQ_PY; __VA_ARGS__; }           \
+    case EQ_PX: { constexpr int E_ = EQ_PX; __VA_ARGS__; }           \
+    case EQ_TY: { constexpr int E_ = EQ_TY; __VA_ARGS__; }           \
+    default: { constexpr int E_ = EQ_TX; __VA_ARGS__; }              \
   }
+
+int sweep_occupancy(int eq, int solver, const SweepShape& s) {
+  if (solver == IXB_SOLVER_EXACT) {
+    IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, IXB_SOLVER_EXACT>(s))
+  }
+  IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, IXB_SOLVER_HYBRID>(s))
 }
 
 cudaError_t sweep_set_smem_limits() {
@@ -206,38 +222,32 @@ cudaError_t sweep_set_smem_limits() {
   e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
   const int bytes = optin - 1024;  // room for the static reduction buffers
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_UY>(bytes);
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_UX>(bytes);
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_VY>(bytes);
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_VX>(bytes);
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_PY>(bytes);
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_PX>(bytes);
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_TY>(bytes);
-  if (e == cudaSuccess) e = sweep_smem_limit<double, EQ_TX>(bytes);
+  for (int eq = 0; eq < EQ_COUNT && e == cudaSuccess; ++eq) {
+    auto f = [&]() -> cudaError_t {
+      IXB_EQ_SWITCH(cudaError_t r = sweep_smem_limit_solver<double, E_, IXB_SOLVER_EXACT>(bytes);
+                    if (r == cudaSuccess) r = sweep_smem_limit_solver<double, E_, IXB_SOLVER_HYBRID>(bytes);
+                    return r)
+    };
+    e = f();
+  }
   if (e == cudaSuccess) done = 1;
   return e;
 }
 
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
                              const SweepIO<double>& io, cudaStream_t st) {
-  switch (eq) {
-    case EQ_UY: return sweep_launch<double, EQ_UY>(solver, s, G, io, st);
-    case EQ_UX: return sweep_launch<double, EQ_UX>(solver, s, G, io, st);
-    case EQ_VY: return sweep_launch<double, EQ_VY>(solver, s, G, io, st);
-    case EQ_VX: return sweep_launch<double, EQ_VX>(solver, s, G, io, st);
-    case EQ_PY: return sweep_launch<double, EQ_PY>(solver, s, G, io, st);
-    case EQ_PX: return sweep_launch<double, EQ_PX>(solver, s, G, io, st);
-    case EQ_TY: return sweep_launch<double, EQ_TY>(solver, s, G, io, st);
-    case EQ_TX: return sweep_launch<double, EQ_TX>(solver, s, G, io, st);
-    default: return cudaErrorInvalidValue;
+  if (solver == IXB_SOLVER_EXACT) {
+    IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_EXACT>(s, G, io, st))
   }
+  IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_HYBRID>(s, G, io, st))
 }
 
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
-                               const double* au, const double* av, cudaStream_t st) {
+                               const double* au, const double* av, int fast, cudaStream_t st) {
   const int total = (G.mi - 1) * (G.nj - 1);
   const int bs = 256;
-  correct_kernel<double><<<(total + bs - 1) / bs, bs, 0, st>>>(G, u, v, p, pc, au, av);
+  if (fast) correct_kernel<double, true><<<(total + bs - 1) / bs, bs, 0, st>>>(G, u, v, p, pc, au, av);
+  else correct_kernel<double, false><<<(total + bs - 1) / bs, bs, 0, st>>>(G, u, v, p, pc, au, av);
   return cudaGetLastError();
 }
 
@@ -248,8 +258,11 @@ int residual_grid(int mi, int nj) {
 
 cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const double* v, const double* T,
                                 const double* p, const double* u_ant, const double* fcon, const double* flin,
-                                double* resu, NormSlot ns, cudaStream_t st) {
-  residual_kernel<double><<<residual_grid(G.mi, G.nj), 256, 0, st>>>(G, u, v, T, p, u_ant, fcon, flin, resu, ns);
+                                double* resu, NormSlot ns, int fast, cudaStream_t st) {
+  if (fast)
+    residual_kernel<double, true><<<residual_grid(G.mi, G.nj), 256, 0, st>>>(G, u, v, T, p, u_ant, fcon, flin, resu, ns);
+  else
+    residual_kernel<double, false><<<residual_grid(G.mi, G.nj), 256, 0, st>>>(G, u, v, T, p, u_ant, fcon, flin, resu, ns);
   return cudaGetLastError();
 }
 

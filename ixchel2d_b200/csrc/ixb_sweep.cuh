@@ -25,35 +25,35 @@ namespace ixb {
 template <int EQ>
 struct EqIsX { static constexpr bool value = (EQ & 1) != 0; };
 
-template <class R, int EQ>
+template <class R, int EQ, bool FAST>
 __device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj,
                                                 double& acc_bo) {
   if constexpr (EQ == EQ_UY) {
-    return assemble_uy(G, io, ii, jj);
+    return assemble_uy<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_UX) {
     R au;
-    Row<R> r = assemble_ux(G, io, ii, jj, au);
+    Row<R> r = assemble_ux<FAST>(G, io, ii, jj, au);
     io.aux[G.at(ii, jj)] = au;
     return r;
   } else if constexpr (EQ == EQ_VY) {
-    return assemble_vy(G, io, ii, jj);
+    return assemble_vy<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_VX) {
     R av;
-    Row<R> r = assemble_vx(G, io, ii, jj, av);
+    Row<R> r = assemble_vx<FAST>(G, io, ii, jj, av);
     io.aux[G.at(ii, jj)] = av;
     return r;
   } else if constexpr (EQ == EQ_PY) {
-    return assemble_py(G, io, ii, jj);
+    return assemble_py<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_PX) {
     R bo;
-    Row<R> r = assemble_px(G, io, ii, jj, bo);
+    Row<R> r = assemble_px<FAST>(G, io, ii, jj, bo);
     io.aux[G.at(ii, jj)] = bo;
     acc_bo += (double)bo * (double)bo;
     return r;
   } else if constexpr (EQ == EQ_TY) {
-    return assemble_ty(G, io, ii, jj);
+    return assemble_ty<FAST>(G, io, ii, jj);
   } else {
-    return assemble_tx(G, io, ii, jj);
+    return assemble_tx<FAST>(G, io, ii, jj);
   }
 }
 
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(TL * G) sweep_kernel(const Geo<R> G_, const Sw
     else {
       const int ii = X ? r + 1 : L;
       const int jj = X ? L : r + 1;
-      row = assemble_cell<R, EQ>(Gm, io, ii, jj, acc_bo);
+      row = assemble_cell<R, EQ, SOLVER == IXB_SOLVER_HYBRID>(Gm, io, ii, jj, acc_bo);
     }
     const int ch = r / m;
     const int o = l * LS + ch * mp + (r - ch * m);
@@ -190,7 +190,7 @@ static cudaError_t sweep_launch_one(const SweepShape& s, const Geo<R>& Gm, const
 }
 
 template <class R, int EQ, int SOLVER>
-static cudaError_t sweep_launch_shape(const SweepShape& s, const Geo<R>& Gm, const SweepIO<R>& io, cudaStream_t st) {
+cudaError_t sweep_launch_solver(const SweepShape& s, const Geo<R>& Gm, const SweepIO<R>& io, cudaStream_t st) {
 #define IXB_CASE_(TL_, G_) \
   if (s.tl == TL_ && s.g == G_) return sweep_launch_one<R, EQ, SOLVER, TL_, G_>(s, Gm, io, st);
   IXB_SWEEP_SHAPES(IXB_CASE_)
@@ -198,43 +198,34 @@ static cudaError_t sweep_launch_shape(const SweepShape& s, const Geo<R>& Gm, con
   return cudaErrorInvalidValue;
 }
 
-template <class R, int EQ>
-cudaError_t sweep_launch(int solver, const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st) {
-  if (solver == IXB_SOLVER_EXACT) return sweep_launch_shape<R, EQ, IXB_SOLVER_EXACT>(s, G, io, st);
-  return sweep_launch_shape<R, EQ, IXB_SOLVER_HYBRID>(s, G, io, st);
-}
-
-template <class R, int EQ>
-cudaError_t sweep_smem_limit(int bytes) {
+template <class R, int EQ, int SOLVER>
+cudaError_t sweep_smem_limit_solver(int bytes) {
   cudaError_t e = cudaSuccess;
   auto set = [&](auto k) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   };
-#define IXB_SET_(TL_, G_)                                   \
-  set(sweep_kernel<R, EQ, IXB_SOLVER_HYBRID, TL_, G_, 3>); \
-  set(sweep_kernel<R, EQ, IXB_SOLVER_HYBRID, TL_, G_, 0>); \
-  set(sweep_kernel<R, EQ, IXB_SOLVER_EXACT, TL_, G_, 0>);
+#define IXB_SET_(TL_, G_)                        \
+  if (SOLVER == IXB_SOLVER_HYBRID)             \
+    set(sweep_kernel<R, EQ, SOLVER, TL_, G_, 3>); \
+  set(sweep_kernel<R, EQ, SOLVER, TL_, G_, 0>);
   IXB_SWEEP_SHAPES(IXB_SET_)
 #undef IXB_SET_
   return e;
 }
 
 // Resident CTAs per SM of the kernel a shape launches (0 if it cannot run).
-template <class R, int EQ>
-int sweep_blocks_per_sm(int solver, const SweepShape& s) {
+template <class R, int EQ, int SOLVER>
+int sweep_blocks_per_sm_solver(const SweepShape& s) {
   int nb = 0;
   cudaError_t e = cudaErrorInvalidValue;
-#define IXB_OCC_(TL_, G_)                                                                                      \
-  if (s.tl == TL_ && s.g == G_) {                                                                              \
-    if (solver == IXB_SOLVER_EXACT)                                                                          \
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, IXB_SOLVER_EXACT, TL_, G_, 0>, \
-                                                        TL_ * G_, s.smem);                                     \
-    else if (s.m == 3)                                                                                       \
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, IXB_SOLVER_HYBRID, TL_, G_, 3>, \
-                                                        TL_ * G_, s.smem);                                     \
+#define IXB_OCC_(TL_, G_)                                                                                    \
+  if (s.tl == TL_ && s.g == G_) {                                                                            \
+    if (SOLVER == IXB_SOLVER_HYBRID && s.m == 3)                                                             \
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, SOLVER, TL_, G_, 3>,         \
+                                                        TL_ * G_, s.smem);                                   \
     else                                                                                                     \
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, IXB_SOLVER_HYBRID, TL_, G_, 0>, \
-                                                        TL_ * G_, s.smem);                                     \
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, SOLVER, TL_, G_, 0>,         \
+                                                        TL_ * G_, s.smem);                                   \
   }
   IXB_SWEEP_SHAPES(IXB_OCC_)
 #undef IXB_OCC_

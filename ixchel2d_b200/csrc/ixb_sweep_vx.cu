@@ -1,9 +1,9 @@
-// Instantiation of the fused sweep kernel for EQ_VX (one translation unit per sweep).
+// Sweep kernel EQ_VX with the reference-order assembly and the sequential Thomas solve (bit-identical to the reference).
 #include "ixb_sweep.cuh"
 
 namespace ixb {
-template cudaError_t sweep_launch<double, EQ_VX>(int, const SweepShape&, const Geo<double>&, const SweepIO<double>&,
-                                                     cudaStream_t);
-template cudaError_t sweep_smem_limit<double, EQ_VX>(int);
-template int sweep_blocks_per_sm<double, EQ_VX>(int, const SweepShape&);
+template cudaError_t sweep_launch_solver<double, EQ_VX, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&,
+                                                                     const SweepIO<double>&, cudaStream_t);
+template cudaError_t sweep_smem_limit_solver<double, EQ_VX, IXB_SOLVER_EXACT>(int);
+template int sweep_blocks_per_sm_solver<double, EQ_VX, IXB_SOLVER_EXACT>(const SweepShape&);
 }  // namespace ixb
