@@ -319,13 +319,30 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def run_profile_phases():
+    """Profiling driver (no timing, no JSON): the benchmark case, three outer
+    iterations, then one launch of each of the ten phases in order
+    (u-y, u-x, v-y, v-x, p'-y, p'-x, correction, T-y, T-x, residual)."""
+    from ixchel2d_b200 import Simple2D
+    sim = Simple2D.from_case(make_case())
+    sim.iterations(3)
+    for k in range(10):
+        sim.phase(k)
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--profile-phases", action="store_true",
+                    help="run the profiling driver instead of the benchmark")
     args = ap.parse_args()
+    if args.profile_phases:
+        run_profile_phases()
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

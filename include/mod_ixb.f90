@@ -1,0 +1,125 @@
+!
+! mod_ixb.f90 -- ISO_C_BINDING interface of libixb (include/ixb.h) for the
+! Ixchel2D Fortran driver.  A maintainer adds this module to
+! source/CMakeLists.txt's SOURCE_FILES, links libixb.so, and replaces the
+! ALGORITMO_SIMPLE body of source/main.f90:395-1217 (and the !$acc data
+! region of :356-389 / :1277) by the calls shown in INTEGRATION.md.
+!
+! The derived types mirror the C structs field by field (bind(C)); arrays
+! keep the reference's Fortran shapes and are passed by reference.
+!
+module ixb
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: IXB_OK = 0, IXB_EINVAL = 1, IXB_ECUDA = 2, IXB_ENONFINITE = 3
+  integer(c_int), parameter :: IXB_ETIMEOUT = 4, IXB_EBC = 5, IXB_ESTATE = 6, IXB_EIO = 7
+  integer(c_int), parameter :: IXB_ENOMEM = 8
+  integer(c_int), parameter :: IXB_PREC_FP64 = 0, IXB_PREC_FP32_REFINED = 1
+  integer(c_int), parameter :: IXB_SOLVER_HYBRID = 0, IXB_SOLVER_EXACT = 1
+  integer(c_int), parameter :: IXB_VAR_U = 0, IXB_VAR_V = 1, IXB_VAR_T = 2
+  integer(c_int), parameter :: IXB_BC_OTHER = 0, IXB_BC_DIRI = 1, IXB_BC_NEUM = 2
+
+  type, bind(C) :: ixb_params
+     real(c_double) :: gamma_momen, gamma_energ, Ri, Riy, dt
+     real(c_double) :: rel_vel, rel_pres, rel_ener
+     real(c_double) :: conv_u, conv_p, conv_t, conv_resi, conv_paso
+     real(c_double) :: p_update
+     integer(c_int) :: iter_ecuaci_max, iter_simple_max, solver
+     integer(c_int) :: reserved(5)
+  end type ixb_params
+
+  type, bind(C) :: ixb_bc_side
+     integer(c_int) :: side, ndivis
+     integer(c_int) :: type(15)
+     real(c_double) :: value(15)
+     integer(c_int) :: index(16)
+  end type ixb_bc_side
+
+  type, bind(C) :: ixb_report
+     real(c_double) :: maxbo, residuo, err_u, err_p, err_t
+     integer(c_int64_t) :: n_simple, n_momen, n_pres, n_ener
+     integer(c_int) :: exit_code, status
+  end type ixb_report
+
+  interface
+     integer(c_int) function ixb_create(mi, nj, prec_mode, h) bind(C, name="ixb_create")
+       import :: c_int, c_ptr
+       integer(c_int), value :: mi, nj, prec_mode
+       type(c_ptr) :: h
+     end function ixb_create
+
+     integer(c_int) function ixb_destroy(h) bind(C, name="ixb_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function ixb_destroy
+
+     integer(c_int) function ixb_set_mesh(h, xu, yv, xp, yp) bind(C, name="ixb_set_mesh")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(in) :: xu(*), yv(*), xp(*), yp(*)
+     end function ixb_set_mesh
+
+     integer(c_int) function ixb_set_params(h, p) bind(C, name="ixb_set_params")
+       import :: c_int, c_ptr, ixb_params
+       type(c_ptr), value :: h
+       type(ixb_params), intent(in) :: p
+     end function ixb_set_params
+
+     integer(c_int) function ixb_set_bc(h, var, sides) bind(C, name="ixb_set_bc")
+       import :: c_int, c_ptr, ixb_bc_side
+       type(c_ptr), value :: h
+       integer(c_int), value :: var
+       type(ixb_bc_side), intent(in) :: sides(4)
+     end function ixb_set_bc
+
+     integer(c_int) function ixb_set_sources(h, var, fcon, flin) bind(C, name="ixb_set_sources")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: var
+       real(c_double), intent(in) :: fcon(*), flin(*)
+     end function ixb_set_sources
+
+     integer(c_int) function ixb_upload_state(h, u, v, p, T, u_ant, v_ant, T_ant) &
+          bind(C, name="ixb_upload_state")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(in) :: u(*), v(*), p(*), T(*), u_ant(*), v_ant(*), T_ant(*)
+     end function ixb_upload_state
+
+     integer(c_int) function ixb_download_state(h, u, v, p, T, u_ant, v_ant, T_ant) &
+          bind(C, name="ixb_download_state")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: u(*), v(*), p(*), T(*), u_ant(*), v_ant(*), T_ant(*)
+     end function ixb_download_state
+
+     integer(c_int) function ixb_simple_loop(h, rep) bind(C, name="ixb_simple_loop")
+       import :: c_int, c_ptr, ixb_report
+       type(c_ptr), value :: h
+       type(ixb_report), intent(out) :: rep
+     end function ixb_simple_loop
+
+     integer(c_int) function ixb_step(h, rep) bind(C, name="ixb_step")
+       import :: c_int, c_ptr, ixb_report
+       type(c_ptr), value :: h
+       type(ixb_report), intent(out) :: rep
+     end function ixb_step
+
+     integer(c_int) function ixb_nusselt_y(h, i0, i1, nu0, nu1) bind(C, name="ixb_nusselt_y")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: i0, i1
+       real(c_double), intent(out) :: nu0, nu1
+     end function ixb_nusselt_y
+
+     integer(c_int) function ixb_read_bc_file(path, xx, mm, yy, nn, sides) bind(C, name="ixb_read_bc_file")
+       import :: c_int, c_char, c_double, ixb_bc_side
+       character(kind=c_char), intent(in) :: path(*)
+       real(c_double), intent(in) :: xx(*), yy(*)
+       integer(c_int), value :: mm, nn
+       type(ixb_bc_side), intent(out) :: sides(4)
+     end function ixb_read_bc_file
+  end interface
+
+end module ixb
