@@ -196,6 +196,29 @@ int ixb_tridiag_f64(const double* a, const double* b, const double* c, const dou
 int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float* d, float* x, int n,
                     int nsys, int layout, int solver, void* stream);
 
+/* Allocation-free form of ixb_tridiag_f64 (no counterpart in the reference),
+ * for callers that cannot let a library allocate device memory during their
+ * run: e.g. a driver whose GPU memory is owned by its OpenACC runtime or by a
+ * pool reserved at start-up, a solver sharing a GPU under a fixed memory
+ * budget, or a loop that must avoid the implicit synchronisation an
+ * allocation can cause.  Same arguments and results as ixb_tridiag_f64; it
+ * calls no cudaMalloc/cudaFree or other allocating routine.
+ * - layout 0 needs no scratch (systems are staged in shared memory).
+ * - layout 1 keeps its scratch in a fixed 8 MiB array that belongs to the
+ *   library's device image (one per GPU that loads the library, held until
+ *   the process exits): n*nsys must not exceed IXB_NOALLOC_MAX_ELEMS, larger
+ *   calls return IXB_EINVAL without launching anything.
+ * - The first layout-1 call on a device looks up the array's device address
+ *   (cudaGetSymbolAddress) with that device current; make that first call
+ *   before any stream capture on the device.
+ * - Every call shares the one array; nothing in it needs to start at zero
+ *   (each element is written before it is read), but calls whose kernels
+ *   overlap on the GPU (different streams, or different host threads) race
+ *   on it: serialise them. */
+#define IXB_NOALLOC_MAX_ELEMS (1 << 20)
+int ixb_tridiag_f64_noalloc(const double* a, const double* b, const double* c, const double* d, double* x, int n,
+                            int nsys, int layout, int solver, void* stream);
+
 /* ---- host-side inputs (no GPU needed) ---- */
 /* lectura_cond_frontera index rule (source/mod_cond_frontera.f90:114-238):
  * for side 0/2 ('a'/'c') the divisions are located on `yy` (nn entries), for

@@ -15,6 +15,7 @@ _PKG = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("IXB_LIB", _PKG / "libixb.so"))
 
 OK, EINVAL, ECUDA, ENONFINITE, ETIMEOUT, EBC, ESTATE, EIO, ENOMEM = range(9)
+NOALLOC_MAX_ELEMS = 1 << 20
 PREC_FP64, PREC_FP32_REFINED = 0, 1
 SOLVER_HYBRID, SOLVER_EXACT = 0, 1
 VAR_U, VAR_V, VAR_T = 0, 1, 2
@@ -87,6 +88,7 @@ SIGNATURES = [
     ("ixb_nusselt_x", C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp]),
     ("ixb_tridiag_f64", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     ("ixb_tridiag_f32", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
+    ("ixb_tridiag_f64_noalloc", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     ("ixb_bc_locate", C.c_int, [C.c_int, C.c_int, _dp, C.POINTER(C.c_int), _dp, _dp, C.c_int, _dp, C.c_int,
                                 C.POINTER(BCSide)]),
     ("ixb_read_bc_file", C.c_int, [C.c_char_p, _dp, C.c_int, _dp, C.c_int, C.POINTER(BCSide)]),

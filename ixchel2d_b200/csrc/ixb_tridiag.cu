@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "ixb_internal.h"
 
@@ -174,3 +175,75 @@ cudaError_t tridiag_f32(const float* a, const float* b, const float* c, const fl
 }
 
 }  // namespace ixb
+
+// ===========================================================================
+// Allocation-free variant of ixb_tridiag_f64.
+//
+// Some callers cannot let a library allocate device memory while they run:
+// a Fortran driver whose GPU memory is owned by its OpenACC runtime or by a
+// pool it reserved at start-up, a solver sharing a GPU under a fixed memory
+// budget where an allocation in mid-run can fail, or a loop that must not
+// pay the implicit synchronisation that cudaMalloc/cudaFree may cause.  For
+// them, the interleaved layout keeps its scratch in a fixed array that is
+// part of this library's device image (allocated by the driver together
+// with the library's code, once per GPU, and held until the process exits).
+// ===========================================================================
+namespace ixb {
+namespace {
+
+// Scratch of the interleaved solve: IXB_NOALLOC_MAX_ELEMS doubles (8 MiB).
+__device__ __align__(256) double g_noalloc_scratch[IXB_NOALLOC_MAX_ELEMS];
+
+constexpr int kMaxDevices = 64;
+double* g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+// Device address of the scratch array for the current device.  In host code
+// the name g_noalloc_scratch denotes a host-side shadow, not device memory,
+// so the address is looked up once per device with that device current.
+cudaError_t noalloc_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace ixb
+
+extern "C" int ixb_tridiag_f64_noalloc(const double* a, const double* b, const double* c, const double* d, double* x,
+                                       int n, int nsys, int layout, int solver, void* stream) {
+  using namespace ixb;
+  if (!a || !b || !c || !d || !x || n < 1 || nsys < 1 || (layout != 0 && layout != 1)) return IXB_EINVAL;
+  if (solver != IXB_SOLVER_HYBRID && solver != IXB_SOLVER_EXACT) return IXB_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (layout == 0) {
+    // contiguous systems are staged in shared memory: no scratch at all
+    e = solver == IXB_SOLVER_EXACT ? tridiag_impl<double, IXB_SOLVER_EXACT>(a, b, c, d, x, n, nsys, 0, st)
+                                   : tridiag_impl<double, IXB_SOLVER_HYBRID>(a, b, c, d, x, n, nsys, 0, st);
+  } else {
+    if ((size_t)n * (size_t)nsys > (size_t)IXB_NOALLOC_MAX_ELEMS) return IXB_EINVAL;
+    double* work = nullptr;
+    e = noalloc_scratch(&work);
+    if (e == cudaSuccess) {
+      // every work[] element is written before it is read: nothing to clear
+      if (solver == IXB_SOLVER_EXACT)
+        tri_inter_kernel<double, IXB_SOLVER_EXACT><<<(nsys + 127) / 128, 128, 0, st>>>(a, b, c, d, x, work, n, nsys);
+      else
+        tri_inter_kernel<double, IXB_SOLVER_HYBRID><<<(nsys + 127) / 128, 128, 0, st>>>(a, b, c, d, x, work, n, nsys);
+      e = cudaGetLastError();
+    }
+  }
+  if (e == cudaErrorInvalidValue) return IXB_EINVAL;
+  return e == cudaSuccess ? IXB_OK : IXB_ECUDA;
+}
