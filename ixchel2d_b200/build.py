@@ -50,8 +50,9 @@ def _stale(src: Path, obj: Path, newest_header: float) -> bool:
 def _compile(src: Path, obj: Path, extra: list[str]) -> tuple[Path, str]:
     if src.suffix == ".cu":
         flags = list(NVFLAGS)
-        if src.stem.endswith("_fast"):
-            # the fast (tolerance-checked) kernels may contract a*b+c into FMA
+        if src.stem.endswith(("_fast", "_mixed")):
+            # the fast and mixed-precision (tolerance-checked) kernels may
+            # contract a*b+c into FMA
             flags[flags.index("-fmad=false")] = "-fmad=true"
         cmd = [_nvcc(), *ARCH, *flags, *extra, "-c", str(src), "-o", str(obj)]
     else:

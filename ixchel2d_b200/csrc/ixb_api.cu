@@ -65,6 +65,8 @@ struct ixb_handle {
   double* metrics = nullptr;
   int mstride = 0;
   double* tables = nullptr;  // T_COUNT mesh-constant 2-D tables
+  float* metrics32 = nullptr;  // binary32 copies (IXB_PREC_FP32_REFINED)
+  float* tables32 = nullptr;
   bool tables_dirty = true;
   double *xp_d = nullptr, *yp_d = nullptr;
   std::vector<double> xu, yv, xp, yp;
@@ -99,7 +101,7 @@ namespace {
 Geo<double> make_geo(const ixb_handle* h) {
   Geo<double> G{};
   G.mi = h->mi; G.nj = h->nj; G.LD = h->LD; G.mstride = h->mstride; G.m = h->metrics;
-  G.tstride = h->fsz; G.tab = h->tables;
+  G.tstride = h->fsz; G.tab = h->tables; G.m64 = h->metrics;
   G.gm = h->prm.gamma_momen; G.ge = h->prm.gamma_energ; G.Ri = h->prm.Ri; G.Riy = h->prm.Riy;
   G.dt = h->prm.dt; G.rel_vel = h->prm.rel_vel; G.rel_pres = h->prm.rel_pres; G.rel_ener = h->prm.rel_ener;
   G.p_update = h->prm.p_update;
@@ -107,6 +109,28 @@ Geo<double> make_geo(const ixb_handle* h) {
   G.inv_rel_pres = 1.0 / G.rel_pres; G.inv_rel_ener = 1.0 / G.rel_ener;
   return G;
 }
+
+// binary32 view of the mesh for the mixed-precision sweeps (the binary64
+// metrics stay reachable for the mass source b_o)
+Geo<float> make_geo32(const ixb_handle* h) {
+  const Geo<double> D = make_geo(h);
+  Geo<float> G{};
+  G.mi = D.mi; G.nj = D.nj; G.LD = D.LD; G.mstride = D.mstride; G.tstride = D.tstride;
+  G.m = h->metrics32; G.m64 = h->metrics; G.tab = h->tables32;
+  G.gm = (float)D.gm; G.ge = (float)D.ge; G.Ri = (float)D.Ri; G.Riy = (float)D.Riy; G.dt = (float)D.dt;
+  G.rel_vel = (float)D.rel_vel; G.rel_pres = (float)D.rel_pres; G.rel_ener = (float)D.rel_ener;
+  G.p_update = (float)D.p_update;
+  G.inv_gm = (float)D.inv_gm; G.inv_dt = (float)D.inv_dt; G.inv_rel_vel = (float)D.inv_rel_vel;
+  G.inv_rel_pres = (float)D.inv_rel_pres; G.inv_rel_ener = (float)D.inv_rel_ener;
+  return G;
+}
+
+// line-solve form of the sweeps: the handle's precision picks the mixed form
+// in place of the binary64 hybrid one
+int solver_form(const ixb_handle* h) {
+  return (h->prec == IXB_PREC_FP32_REFINED && h->prm.solver == IXB_SOLVER_HYBRID) ? SOLVER_MIXED : h->prm.solver;
+}
+int real_bytes(const ixb_handle* h) { return solver_form(h) == SOLVER_MIXED ? 4 : 8; }
 
 NormSlot slot(ixb_handle* h, int k) {
   return NormSlot{h->partials + (size_t)k * h->pstride, h->counters + k, h->norms + k};
@@ -125,6 +149,10 @@ int ensure_tables(ixb_handle* h) {
   if (!h->tables_dirty) return IXB_OK;
   Geo<double> G = make_geo(h);
   CK(launch_tables_f64(G, h->metrics, h->tables, h->stream));
+  if (h->metrics32) {
+    CK(launch_narrow_f32(h->metrics, h->metrics32, (size_t)M_COUNT * h->mstride, h->stream));
+    CK(launch_narrow_f32(h->tables, h->tables32, (size_t)T_COUNT * h->fsz, h->stream));
+  }
   CK(cudaStreamSynchronize(h->stream));
   h->tables_dirty = false;
   return IXB_OK;
@@ -139,8 +167,8 @@ void pick_shape(ixb_handle* h, int eq) {
   int best = -1;
   long long best_key = 0;
   for (int k = 0; k < 7; ++k) {
-    SweepShape s = sweep_shape(eq, h->mi, h->nj, 8, kShapes[k][0], kShapes[k][1]);
-    const int occ = sweep_occupancy(eq, h->prm.solver, s);
+    SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), kShapes[k][0], kShapes[k][1]);
+    const int occ = sweep_occupancy(eq, solver_form(h), s);
     if (occ <= 0) continue;
     const long long waves = (s.grid + (long long)occ * h->nsm - 1) / ((long long)occ * h->nsm);
     const long long key = waves * 1000000LL + (long long)s.m * 1000 + (256 - s.nt);
@@ -155,7 +183,7 @@ void pick_shape(ixb_handle* h, int eq) {
 int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
   Geo<double> G = make_geo(h);
   if (h->shape_tl[eq] == 0) pick_shape(h, eq);
-  SweepShape s = sweep_shape(eq, h->mi, h->nj, 8, h->shape_tl[eq], h->shape_g[eq]);
+  SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), h->shape_tl[eq], h->shape_g[eq]);
   SweepIO<double> io{};
   io.u = h->u[h->cu]; io.v = h->v[h->cv]; io.T = h->T[h->cT]; io.p = h->p; io.pc = h->pc[h->cpc];
   io.u_ant = h->u_ant; io.v_ant = h->v_ant; io.T_ant = h->T_ant;
@@ -188,7 +216,8 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
     if (eq == EQ_PX) { io.nrm0 = slot(h, N_DP); io.nrm1 = slot(h, N_BO); }
     if (eq == EQ_TX) io.nrm0 = slot(h, N_DT);
   }
-  CK(launch_sweep_f64(eq, h->prm.solver, s, G, io, h->stream));
+  const Geo<float> Gf = h->metrics32 ? make_geo32(h) : Geo<float>{};
+  CK(launch_sweep_f64(eq, solver_form(h), s, G, Gf, io, h->stream));
   *cur ^= 1;
   return IXB_OK;
 }
@@ -499,6 +528,8 @@ void free_all(ixb_handle* h) {
                      &h->fcon[0], &h->fcon[1], &h->fcon[2], &h->flin[0], &h->flin[1], &h->flin[2],
                      &h->metrics, &h->tables, &h->xp_d, &h->yp_d, &h->partials, &h->norms, &h->nu_d};
   for (auto b : bufs) if (*b) cudaFree(*b);
+  if (h->metrics32) cudaFree(h->metrics32);
+  if (h->tables32) cudaFree(h->tables32);
   if (h->bc) cudaFree(h->bc);
   if (h->counters) cudaFree(h->counters);
   if (h->ctl_d) cudaFree(h->ctl_d);
@@ -568,7 +599,7 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   *out = nullptr;
   // a line of up to 6000 rows (chunks of <= 24 rows per thread) fits one CTA's shared memory
   if (mi < 4 || nj < 4 || mi > 6000 || nj > 6000) return IXB_EINVAL;
-  if (prec_mode != IXB_PREC_FP64) return IXB_EINVAL;  // binary32 mode: see ixb_create_refined
+  if (prec_mode != IXB_PREC_FP64 && prec_mode != IXB_PREC_FP32_REFINED) return IXB_EINVAL;
   ixb_handle* h = new (std::nothrow) ixb_handle();
   if (!h) return IXB_ENOMEM;
   h->mi = mi; h->nj = nj; h->prec = prec_mode;
@@ -596,6 +627,10 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   if (cudaMemset(h->metrics, 0, (size_t)M_COUNT * h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ECUDA);
   if (cudaMalloc(&h->tables, (size_t)T_COUNT * fb) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMemset(h->tables, 0, (size_t)T_COUNT * fb) != cudaSuccess) return fail(IXB_ECUDA);
+  if (prec_mode == IXB_PREC_FP32_REFINED) {
+    if (cudaMalloc(&h->metrics32, (size_t)M_COUNT * h->mstride * sizeof(float)) != cudaSuccess) return fail(IXB_ENOMEM);
+    if (cudaMalloc(&h->tables32, (size_t)T_COUNT * h->fsz * sizeof(float)) != cudaSuccess) return fail(IXB_ENOMEM);
+  }
   if (cudaMalloc(&h->xp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMalloc(&h->yp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   h->bcstride = std::max(mi, nj) + 3;
@@ -934,8 +969,8 @@ int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads
   for (; k < 7; ++k)
     if (kShapes[k][0] == lines_per_cta && kShapes[k][1] == threads_per_line) break;
   if (k == 7) return IXB_EINVAL;
-  SweepShape s = sweep_shape(sweep, h->mi, h->nj, 8, lines_per_cta, threads_per_line);
-  if (sweep_occupancy(sweep, h->prm.solver, s) <= 0) return IXB_EINVAL;
+  SweepShape s = sweep_shape(sweep, h->mi, h->nj, real_bytes(h), lines_per_cta, threads_per_line);
+  if (sweep_occupancy(sweep, solver_form(h), s) <= 0) return IXB_EINVAL;
   h->shape_tl[sweep] = lines_per_cta;
   h->shape_g[sweep] = threads_per_line;
   h->graph_dirty = true;

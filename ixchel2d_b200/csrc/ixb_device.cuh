@@ -63,16 +63,30 @@ struct NormSlot {        // deterministic two-level sum of squares
 // and the compiler may batch the loads ahead of the shared-memory stores.
 template <class R>
 __device__ __forceinline__ R ldg(const R* p, int i) { return __ldg(p + i); }
+// the same load converted to the assembly's arithmetic type (a no-op when
+// the field and the arithmetic are both binary64)
+template <class R, class F>
+__device__ __forceinline__ R ld(const F* p, int i) { return R(__ldg(p + i)); }
+// ... saturated at 1e38 when narrowed to binary32: au/av hold the
+// reference's 1e40 "no coefficient" marker (main.f90:309-310) on boundary
+// nodes, which would otherwise become an infinity
+template <class R, class F>
+__device__ __forceinline__ R ld_sat(const F* p, int i) {
+  if constexpr (sizeof(R) < sizeof(F)) return R(fmin(__ldg(p + i), F(1e38)));
+  else return R(__ldg(p + i));
+}
 
 template <class R>
 struct Geo {
   int mi, nj, LD, mstride;
   int tstride;     // elements per 2-D table (fields stay below 2^31 elements)
   const R* m;      // M_COUNT 1-D arrays
+  const double* m64;  // the same arrays in binary64 (== m when R is double)
   const R* tab;    // T_COUNT 2-D tables
   R gm, ge, Ri, Riy, dt, rel_vel, rel_pres, rel_ener, p_update;
   R inv_gm, inv_dt, inv_rel_vel, inv_rel_pres, inv_rel_ener;  // fast form
   __device__ __forceinline__ R met(int which, int k) const { return __ldg(m + which * mstride + k); }
+  __device__ __forceinline__ double met64(int which, int k) const { return __ldg(m64 + which * mstride + k); }
   __device__ __forceinline__ int at(int ii, int jj) const { return (jj - 1) * LD + (ii - 1); }
   __device__ __forceinline__ R t(int which, int ii, int jj) const { return __ldg(tab + which * tstride + at(ii, jj)); }
 };
@@ -98,16 +112,24 @@ struct SweepIO {
 template <class R>
 struct Row { R a, b, c, d; };
 
+// math on either binary32 or binary64 operands without promotion
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fabsT(float x) { return fabsf(x); }
+__device__ __forceinline__ double fabsT(double x) { return fabs(x); }
+__device__ __forceinline__ float fmaxT(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmaxT(double a, double b) { return fmax(a, b); }
+
 // DMAX1(0, (1 - 0.1|P|)**5): the integer power as binary powering x*((x*x)*(x*x))
 template <class R>
 __device__ __forceinline__ R plaw(R pe) {
-  R t = R(1) - R(0.1) * fabs(pe);
+  R t = R(1) - R(0.1) * fabsT(pe);
   R t2 = t * t;
   R t5 = t * (t2 * t2);
-  return fmax(R(0), t5);
+  return fmaxT(R(0), t5);
 }
 template <class R>
-__device__ __forceinline__ R dmax0(R x) { return fmax(R(0), x); }
+__device__ __forceinline__ R dmax0(R x) { return fmaxT(R(0), x); }
 
 // harmonic face interpolation g1*g2/(g1*(1-f)+g2*f) of the reference
 // (e.g. source/mod_ec_momento.f90:462-465) with its operand order
@@ -145,16 +167,16 @@ __device__ __forceinline__ R qdiv(R a, R b) { if constexpr (FAST) return a * fas
 // The four neighbour coefficients of the u row (:512-526), face velocities
 // interpolated as in :447-455, diffusivities and conductances from the
 // tables (gammai = gammad = gamma_momen).
-template <bool FAST, class R>
-__device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<R>& io, const R* u, int ii, int jj,
+template <bool FAST, class R, class F>
+__device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<F>& io, const F* u, int ii, int jj,
                                         R& AI, R& AD, R& BS, R& BN, R& deltax, R& deltay, R& temp_int) {
-  const R* v = io.v;
+  const F* v = io.v;
   const R fexu_i = G.met(M_FEXU, ii), fexu_m = G.met(M_FEXU, ii - 1);
   const R fexp_i = G.met(M_FEXP, ii);
-  R ud = fexu_i * ldg(u, G.at(ii + 1, jj)) + (R(1) - fexu_i) * ldg(u, G.at(ii, jj));
-  R ui = fexu_m * ldg(u, G.at(ii, jj)) + (R(1) - fexu_m) * ldg(u, G.at(ii - 1, jj));
-  R vn = fexp_i * ldg(v, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj));
-  R vs = fexp_i * ldg(v, G.at(ii + 1, jj - 1)) + (R(1) - fexp_i) * ldg(v, G.at(ii, jj - 1));
+  R ud = fexu_i * ld<R>(u, G.at(ii + 1, jj)) + (R(1) - fexu_i) * ld<R>(u, G.at(ii, jj));
+  R ui = fexu_m * ld<R>(u, G.at(ii, jj)) + (R(1) - fexu_m) * ld<R>(u, G.at(ii - 1, jj));
+  R vn = fexp_i * ld<R>(v, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ld<R>(v, G.at(ii, jj));
+  R vs = fexp_i * ld<R>(v, G.at(ii + 1, jj - 1)) + (R(1) - fexp_i) * ld<R>(v, G.at(ii, jj - 1));
   const R g = G.gm;
   R gamman, gammas, rgn = R(0), rgs = R(0);
   if constexpr (FAST) {
@@ -168,7 +190,7 @@ __device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<R>& io, c
   R di = G.met(M_DXP, ii), dd = G.met(M_DXP, ii + 1), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   deltax = G.met(M_DXU, ii);
   deltay = G.met(M_DYU, jj);
-  temp_int = fexp_i * ldg(io.T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(io.T, G.at(ii, jj));
+  temp_int = fexp_i * ld<R>(io.T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ld<R>(io.T, G.at(ii, jj));
   AI = -(G.t(T_CU1, ii, jj) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * deltay));
   AD = -(G.t(T_CU1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) + dmax0(-ud * deltay));
   BS = -(G.t(T_CU2, ii, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) + dmax0(vs * deltax));
@@ -176,59 +198,59 @@ __device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<R>& io, c
 }
 
 // X form (ensambla_velu_x): a=AI c=AD b=AC d=Rx, aux = au = AC*rel
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_ux(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& au) {
-  const R* u = io.in;
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_ux(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj, R& au) {
+  const F* u = io.in;
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
-  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
   r.b = qdiv<FAST>(-AI - AD - BS - BN - dx * dy * flin + qdiv<FAST>(dx * dy, G.dt, G.inv_dt), G.rel_vel,
                    G.inv_rel_vel);
-  r.d = -BS * ldg(u, G.at(ii, jj - 1)) - BN * ldg(u, G.at(ii, jj + 1)) - dx * dy * G.Ri * tint + dx * dy * fcon +
-        qdiv<FAST>(dx * dy * ldg(io.u_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
-        r.b * (R(1) - G.rel_vel) * ldg(u, c0);
+  r.d = -BS * ld<R>(u, G.at(ii, jj - 1)) - BN * ld<R>(u, G.at(ii, jj + 1)) - dx * dy * G.Ri * tint + dx * dy * fcon +
+        qdiv<FAST>(dx * dy * ld<R>(io.u_ant, c0), G.dt, G.inv_dt) + (ld<R>(io.p, c0) - ld<R>(io.p, G.at(ii + 1, jj))) * dy +
+        r.b * (R(1) - G.rel_vel) * ld<R>(u, c0);
   au = r.b * G.rel_vel;
   return r;
 }
 
 // Y form (ensambla_velu_y): a=BS c=BN b=BC d=Ry
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_uy(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
-  const R* u = io.in;
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_uy(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
+  const F* u = io.in;
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
-  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
   r.b = qdiv<FAST>(-AI - AD - BS - BN - dx * dy * flin + qdiv<FAST>(dx * dy, G.dt, G.inv_dt), G.rel_vel,
                    G.inv_rel_vel);
-  r.d = -AI * ldg(u, G.at(ii - 1, jj)) - AD * ldg(u, G.at(ii + 1, jj)) - dx * dy * G.Ri * tint + dx * dy * fcon +
-        qdiv<FAST>(dx * dy * ldg(io.u_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii + 1, jj))) * dy +
-        r.b * (R(1) - G.rel_vel) * ldg(u, c0);
+  r.d = -AI * ld<R>(u, G.at(ii - 1, jj)) - AD * ld<R>(u, G.at(ii + 1, jj)) - dx * dy * G.Ri * tint + dx * dy * fcon +
+        qdiv<FAST>(dx * dy * ld<R>(io.u_ant, c0), G.dt, G.inv_dt) + (ld<R>(io.p, c0) - ld<R>(io.p, G.at(ii + 1, jj))) * dy +
+        r.b * (R(1) - G.rel_vel) * ld<R>(u, c0);
   return r;
 }
 
 // ---------------------------------------------------------------------------
 // v momentum (ensambla_velv_x/_y, source/mod_ec_momento.f90:736-1098)
 // ---------------------------------------------------------------------------
-template <bool FAST, class R>
-__device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<R>& io, const R* v, int ii, int jj,
+template <bool FAST, class R, class F>
+__device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<F>& io, const F* v, int ii, int jj,
                                         R& AI, R& AD, R& BS, R& BN, R& temp_int) {
-  const R* u = io.u;
+  const F* u = io.u;
   const R feyp_j = G.met(M_FEYP, jj);
   const R feyv_j = G.met(M_FEYV, jj), feyv_m = G.met(M_FEYV, jj - 1);
-  R ud = feyp_j * ldg(u, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ldg(u, G.at(ii, jj));
-  R ui = feyp_j * ldg(u, G.at(ii - 1, jj + 1)) + (R(1) - feyp_j) * ldg(u, G.at(ii - 1, jj));
-  R vn = feyv_j * ldg(v, G.at(ii, jj + 1)) + (R(1) - feyv_j) * ldg(v, G.at(ii, jj));
-  R vs = feyv_m * ldg(v, G.at(ii, jj)) + (R(1) - feyv_m) * ldg(v, G.at(ii, jj - 1));
+  R ud = feyp_j * ld<R>(u, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ld<R>(u, G.at(ii, jj));
+  R ui = feyp_j * ld<R>(u, G.at(ii - 1, jj + 1)) + (R(1) - feyp_j) * ld<R>(u, G.at(ii - 1, jj));
+  R vn = feyv_j * ld<R>(v, G.at(ii, jj + 1)) + (R(1) - feyv_j) * ld<R>(v, G.at(ii, jj));
+  R vs = feyv_m * ld<R>(v, G.at(ii, jj)) + (R(1) - feyv_m) * ld<R>(v, G.at(ii, jj - 1));
   const R g = G.gm;  // gamman = gammas = gamma_momen (:854-858)
   R gammad, gammai, rgd = R(0), rgi = R(0);
   if constexpr (FAST) {
@@ -241,51 +263,51 @@ __device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<R>& io, c
   }
   R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYP, jj), dn = G.met(M_DYP, jj + 1);
   const R dyv = G.met(M_DYV, jj), dxv = G.met(M_DXV, ii);
-  temp_int = feyp_j * ldg(io.T, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ldg(io.T, G.at(ii, jj));
+  temp_int = feyp_j * ld<R>(io.T, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ld<R>(io.T, G.at(ii, jj));
   AI = -(G.t(T_CV1, ii, jj) * plaw(qdiv<FAST>(ui * di, gammai, rgi)) + dmax0(ui * dyv));
   AD = -(G.t(T_CV1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, gammad, rgd)) + dmax0(-ud * dyv));
   BS = -(G.t(T_CV2, ii, jj) * plaw(qdiv<FAST>(vs * ds, g, G.inv_gm)) + dmax0(vs * dxv));
   BN = -(G.t(T_CV2, ii, jj + 1) * plaw(qdiv<FAST>(vn * dn, g, G.inv_gm)) + dmax0(-vn * dxv));
 }
 
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_vx(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& av) {
-  const R* v = io.in;
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_vx(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj, R& av) {
+  const F* v = io.in;
   R AI, AD, BS, BN, tint;
   v_parts<FAST>(G, io, v, ii, jj, AI, AD, BS, BN, tint);
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
   r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_vel, G.inv_rel_vel);
-  r.d = -BS * ldg(v, G.at(ii, jj - 1)) - BN * ldg(v, G.at(ii, jj + 1)) - dxdy * G.Riy * tint + dxdy * fcon +
-        qdiv<FAST>(dxdy * ldg(io.v_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
-        r.b * (R(1) - G.rel_vel) * ldg(v, c0);
+  r.d = -BS * ld<R>(v, G.at(ii, jj - 1)) - BN * ld<R>(v, G.at(ii, jj + 1)) - dxdy * G.Riy * tint + dxdy * fcon +
+        qdiv<FAST>(dxdy * ld<R>(io.v_ant, c0), G.dt, G.inv_dt) + (ld<R>(io.p, c0) - ld<R>(io.p, G.at(ii, jj + 1))) * dxv +
+        r.b * (R(1) - G.rel_vel) * ld<R>(v, c0);
   av = r.b * G.rel_vel;
   return r;
 }
 
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
-  const R* v = io.in;
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
+  const F* v = io.in;
   R AI, AD, BS, BN, tint;
   v_parts<FAST>(G, io, v, ii, jj, AI, AD, BS, BN, tint);
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
   r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_vel, G.inv_rel_vel);
-  r.d = -AI * ldg(v, G.at(ii - 1, jj)) - AD * ldg(v, G.at(ii + 1, jj)) - dxdy * G.Riy * tint + dxdy * fcon +
-        qdiv<FAST>(dxdy * ldg(io.v_ant, c0), G.dt, G.inv_dt) + (ldg(io.p, c0) - ldg(io.p, G.at(ii, jj + 1))) * dxv +
-        r.b * (R(1) - G.rel_vel) * ldg(v, c0);
+  r.d = -AI * ld<R>(v, G.at(ii - 1, jj)) - AD * ld<R>(v, G.at(ii + 1, jj)) - dxdy * G.Riy * tint + dxdy * fcon +
+        qdiv<FAST>(dxdy * ld<R>(io.v_ant, c0), G.dt, G.inv_dt) + (ld<R>(io.p, c0) - ld<R>(io.p, G.at(ii, jj + 1))) * dxv +
+        r.b * (R(1) - G.rel_vel) * ld<R>(v, c0);
   return r;
 }
 
@@ -293,11 +315,11 @@ __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<R>&
 // energy (ensambla_energia_x/_y, source/mod_ec_energia.f90:119-443).  The
 // calls in main.f90:989 and :1060 bind fexu/feyv to the dummies fexpo/feypo.
 // ---------------------------------------------------------------------------
-template <bool FAST, class R>
-__device__ __forceinline__ void t_parts(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& AI, R& AD,
+template <bool FAST, class R, class F>
+__device__ __forceinline__ void t_parts(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj, R& AI, R& AD,
                                         R& BS, R& BN) {
-  const R ud = ldg(io.u, G.at(ii, jj)), ui = ldg(io.u, G.at(ii - 1, jj));
-  const R vn = ldg(io.v, G.at(ii, jj)), vs = ldg(io.v, G.at(ii, jj - 1));
+  const R ud = ld<R>(io.u, G.at(ii, jj)), ui = ld<R>(io.u, G.at(ii - 1, jj));
+  const R vn = ld<R>(io.v, G.at(ii, jj)), vs = ld<R>(io.v, G.at(ii, jj - 1));
   const R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   if constexpr (FAST) {
@@ -317,55 +339,65 @@ __device__ __forceinline__ void t_parts(const Geo<R>& G, const SweepIO<R>& io, i
   }
 }
 
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_tx(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
-  const R* T = io.in;
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_tx(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
+  const F* T = io.in;
   R AI, AD, BS, BN;
   t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
   r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_ener, G.inv_rel_ener);
-  r.d = -BS * ldg(T, G.at(ii, jj - 1)) - BN * ldg(T, G.at(ii, jj + 1)) + dxdy * fcon +
-        qdiv<FAST>(dxdy * ldg(io.T_ant, c0), G.dt, G.inv_dt) + r.b * (R(1) - G.rel_ener) * ldg(T, c0);
+  r.d = -BS * ld<R>(T, G.at(ii, jj - 1)) - BN * ld<R>(T, G.at(ii, jj + 1)) + dxdy * fcon +
+        qdiv<FAST>(dxdy * ld<R>(io.T_ant, c0), G.dt, G.inv_dt) + r.b * (R(1) - G.rel_ener) * ld<R>(T, c0);
   return r;
 }
 
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
-  const R* T = io.in;
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
+  const F* T = io.in;
   R AI, AD, BS, BN;
   t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = io.flin ? ldg(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ldg(io.fcon, c0) : R(0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
   r.b = qdiv<FAST>(-AI - AD - BS - BN - dxdy * flin + qdiv<FAST>(dxdy, G.dt, G.inv_dt), G.rel_ener, G.inv_rel_ener);
-  r.d = -AI * ldg(T, G.at(ii - 1, jj)) - AD * ldg(T, G.at(ii + 1, jj)) + dxdy * fcon +
-        qdiv<FAST>(dxdy * ldg(io.T_ant, c0), G.dt, G.inv_dt) + r.b * (R(1) - G.rel_ener) * ldg(T, c0);
+  r.d = -AI * ld<R>(T, G.at(ii - 1, jj)) - AD * ld<R>(T, G.at(ii + 1, jj)) + dxdy * fcon +
+        qdiv<FAST>(dxdy * ld<R>(io.T_ant, c0), G.dt, G.inv_dt) + r.b * (R(1) - G.rel_ener) * ld<R>(T, c0);
   return r;
 }
 
 // ---------------------------------------------------------------------------
 // pressure correction (ensambla_corr_pres_x/_y, source/mod_ec_momento.f90:145-355)
 // ---------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ R pc_at(const SweepIO<R>& io, const Geo<R>& G, int ii, int jj) {
-  return io.in ? ldg(io.in, G.at(ii, jj)) : R(0);
+template <class R, class F>
+__device__ __forceinline__ R pc_at(const SweepIO<F>& io, const Geo<R>& G, int ii, int jj) {
+  return io.in ? ld<R>(io.in, G.at(ii, jj)) : R(0);
 }
 
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj, R& bo) {
+// Mass source b_o = (u_w - u_e) dy + (v_s - v_n) dx of the p' rows, always
+// in the fields' precision (binary64) with binary64 metrics, whatever the
+// precision of the coefficients.
+template <class R, class F>
+__device__ __forceinline__ F mass_residual(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
   const int c0 = G.at(ii, jj);
-  const R ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
-  const R ai = ldg(io.au, G.at(ii - 1, jj)), ad = ldg(io.au, c0), as = ldg(io.av, G.at(ii, jj - 1)), an = ldg(io.av, c0);
+  const F ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
+  return (ui - ud) * F(G.met64(M_DYP, jj)) + (vs - vn) * F(G.met64(M_DXP, ii));
+}
+
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj, F& bo) {
+  const int c0 = G.at(ii, jj);
+  const R ai = ld_sat<R>(io.au, G.at(ii - 1, jj)), ad = ld_sat<R>(io.au, c0), as = ld_sat<R>(io.av, G.at(ii, jj - 1)),
+          an = ld_sat<R>(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   Row<R> r;
   r.a = -qdiv<FAST>(dyp * dyp, ai);
@@ -373,17 +405,17 @@ __device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<R>&
   const R BS = -qdiv<FAST>(dxp * dxp, as);
   const R BN = -qdiv<FAST>(dxp * dxp, an);
   r.b = qdiv<FAST>(-r.a - r.c - BS - BN, G.rel_pres, G.inv_rel_pres);
-  bo = (ui - ud) * dyp + (vs - vn) * dxp;
-  r.d = -BS * pc_at(io, G, ii, jj - 1) - BN * pc_at(io, G, ii, jj + 1) + bo +
-        (R(1) - G.rel_pres) * r.b * pc_at(io, G, ii, jj);
+  bo = mass_residual(G, io, ii, jj);
+  r.d = -BS * pc_at<R>(io, G, ii, jj - 1) - BN * pc_at<R>(io, G, ii, jj + 1) + R(bo) +
+        (R(1) - G.rel_pres) * r.b * pc_at<R>(io, G, ii, jj);
   return r;
 }
 
-template <bool FAST, class R>
-__device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj) {
+template <bool FAST, class R, class F>
+__device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
   const int c0 = G.at(ii, jj);
-  const R ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
-  const R ai = ldg(io.au, G.at(ii - 1, jj)), ad = ldg(io.au, c0), as = ldg(io.av, G.at(ii, jj - 1)), an = ldg(io.av, c0);
+  const R ai = ld_sat<R>(io.au, G.at(ii - 1, jj)), ad = ld_sat<R>(io.au, c0), as = ld_sat<R>(io.av, G.at(ii, jj - 1)),
+          an = ld_sat<R>(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   const R AI = -qdiv<FAST>(dyp * dyp, ai);
   const R AD = -qdiv<FAST>(dyp * dyp, ad);
@@ -391,9 +423,9 @@ __device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<R>&
   r.a = -qdiv<FAST>(dxp * dxp, as);
   r.c = -qdiv<FAST>(dxp * dxp, an);
   r.b = qdiv<FAST>(-AI - AD - r.a - r.c, G.rel_pres, G.inv_rel_pres);
-  const R bo = (ui - ud) * dyp + (vs - vn) * dxp;
-  r.d = -AI * pc_at(io, G, ii - 1, jj) - AD * pc_at(io, G, ii + 1, jj) + bo +
-        (R(1) - G.rel_pres) * r.b * pc_at(io, G, ii, jj);
+  const R bo = R(mass_residual(G, io, ii, jj));
+  r.d = -AI * pc_at<R>(io, G, ii - 1, jj) - AD * pc_at<R>(io, G, ii + 1, jj) + bo +
+        (R(1) - G.rel_pres) * r.b * pc_at<R>(io, G, ii, jj);
   return r;
 }
 
@@ -603,9 +635,9 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
     a[1] = ap; c[1] = cp; d[1] = dp;
     for (int i = 2; i < m; ++i) {
       const R ai = a[i];
-      const R r = fast_rcp(fma(-ai, cp, b[i]));
+      const R r = fast_rcp(fmaT(-ai, cp, b[i]));
       ap = -ai * ap * r;
-      dp = fma(-ai, dp, d[i]) * r;
+      dp = fmaT(-ai, dp, d[i]) * r;
       cp = c[i] * r;
       a[i] = ap; c[i] = cp; d[i] = dp;
     }
@@ -613,14 +645,14 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
     R an = a[m - 2], cn = c[m - 2], dn = d[m - 2];
     for (int i = m - 3; i >= 1; --i) {
       const R ci = c[i];
-      dn = fma(-ci, dn, d[i]);
-      an = fma(-ci, an, a[i]);
+      dn = fmaT(-ci, dn, d[i]);
+      an = fmaT(-ci, an, a[i]);
       cn = -ci * cn;
       a[i] = an; c[i] = cn; d[i] = dn;
     }
     // reduced rows 2k (chunk's first row) and 2k+1 (its last row), unit diagonal
-    const R r0 = fast_rcp(fma(-c0, an, b0));
-    eA = a0 * r0; eC = -c0 * cn * r0; eD = fma(-c0, dn, d0) * r0;
+    const R r0 = fast_rcp(fmaT(-c0, an, b0));
+    eA = a0 * r0; eC = -c0 * cn * r0; eD = fmaT(-c0, dn, d0) * r0;
     oA = ap; oC = cp; oD = dp;
   }
   R x0, xl;
@@ -646,10 +678,10 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
           R alo = R(0), clo = R(0), dlo = R(0), ahi = R(0), chi = R(0), dhi = R(0);
           if (i - s >= 0) { alo = Ac[i - s]; clo = Cc[i - s]; dlo = Dc[i - s]; }
           if (i + s < 2 * G) { ahi = Ac[i + s]; chi = Cc[i + s]; dhi = Dc[i + s]; }
-          const R r = fast_rcp(fma(-ci, ahi, fma(-ai, clo, R(1))));
+          const R r = fast_rcp(fmaT(-ci, ahi, fmaT(-ai, clo, R(1))));
           An[i] = -ai * alo * r;
           Cn[i] = -ci * chi * r;
-          Dn[i] = fma(-ci, dhi, fma(-ai, dlo, di)) * r;
+          Dn[i] = fmaT(-ci, dhi, fmaT(-ai, dlo, di)) * r;
         }
       }
       __syncthreads();
@@ -680,7 +712,7 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
   }
   if (active) {
     d[0] = x0;
-    for (int i = 1; i < m - 1; ++i) d[i] = fma(-c[i], xl, fma(-a[i], x0, d[i]));
+    for (int i = 1; i < m - 1; ++i) d[i] = fmaT(-c[i], xl, fmaT(-a[i], x0, d[i]));
     d[m - 1] = xl;
   }
 }

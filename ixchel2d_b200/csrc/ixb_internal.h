@@ -11,6 +11,11 @@ namespace ixb {
 
 enum NormId { N_DV = 0, N_DP, N_BO, N_DT, N_RES, N_COUNT };
 
+// Line-solve forms of the sweep kernels: IXB_SOLVER_HYBRID (0) and
+// IXB_SOLVER_EXACT (1) of the public ABI, plus the mixed-precision form a
+// handle created with IXB_PREC_FP32_REFINED runs in place of the hybrid one.
+constexpr int SOLVER_MIXED = 2;
+
 // launch shape of one sweep
 struct SweepShape {
   int n;          // rows per line
@@ -32,7 +37,8 @@ SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl, int g);
 
 // per-sweep launchers (ixb_sweep_<eq>.cu: exact, ixb_sweep_<eq>_fast.cu: hybrid)
 template <class R, int EQ, int SOLVER>
-cudaError_t sweep_launch_solver(const SweepShape& s, const Geo<R>& G, const SweepIO<R>& io, cudaStream_t st);
+cudaError_t sweep_launch_solver(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
+                                const SweepIO<R>& io, cudaStream_t st);
 template <class R, int EQ, int SOLVER>
 cudaError_t sweep_smem_limit_solver(int bytes);
 template <class R, int EQ, int SOLVER>
@@ -42,7 +48,7 @@ int max_sweep_lines(int mi, int nj);
 
 // kernel launchers (ixb_kernels.cu); return cudaError_t
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
-                             const SweepIO<double>& io, cudaStream_t st);
+                             const Geo<float>& Gf, const SweepIO<double>& io, cudaStream_t st);
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
                                const double* au, const double* av, int fast, cudaStream_t st);
 cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const double* v, const double* T,
@@ -53,6 +59,7 @@ cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const doub
                                int vertical, int k0, int k1, double* out2, cudaStream_t st);
 cudaError_t sweep_set_smem_limits();
 cudaError_t launch_tables_f64(const Geo<double>& G, double* met, double* tab, cudaStream_t st);
+cudaError_t launch_narrow_f32(const double* src, float* dst, size_t n, cudaStream_t st);
 
 // batched standalone tridiagonal solvers (ixb_tridiag.cu)
 cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,

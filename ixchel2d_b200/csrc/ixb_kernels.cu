@@ -210,6 +210,9 @@ int sweep_occupancy(int eq, int solver, const SweepShape& s) {
   if (solver == IXB_SOLVER_EXACT) {
     IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, IXB_SOLVER_EXACT>(s))
   }
+  if (solver == SOLVER_MIXED) {
+    IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, SOLVER_MIXED>(s))
+  }
   IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, IXB_SOLVER_HYBRID>(s))
 }
 
@@ -226,6 +229,7 @@ cudaError_t sweep_set_smem_limits() {
     auto f = [&]() -> cudaError_t {
       IXB_EQ_SWITCH(cudaError_t r = sweep_smem_limit_solver<double, E_, IXB_SOLVER_EXACT>(bytes);
                     if (r == cudaSuccess) r = sweep_smem_limit_solver<double, E_, IXB_SOLVER_HYBRID>(bytes);
+                    if (r == cudaSuccess) r = sweep_smem_limit_solver<double, E_, SOLVER_MIXED>(bytes);
                     return r)
     };
     e = f();
@@ -235,11 +239,25 @@ cudaError_t sweep_set_smem_limits() {
 }
 
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
-                             const SweepIO<double>& io, cudaStream_t st) {
+                             const Geo<float>& Gf, const SweepIO<double>& io, cudaStream_t st) {
   if (solver == IXB_SOLVER_EXACT) {
-    IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_EXACT>(s, G, io, st))
+    IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_EXACT>(s, G, Gf, io, st))
   }
-  IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_HYBRID>(s, G, io, st))
+  if (solver == SOLVER_MIXED) {
+    IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, SOLVER_MIXED>(s, G, Gf, io, st))
+  }
+  IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_HYBRID>(s, G, Gf, io, st))
+}
+
+__global__ void narrow_f32_kernel(const double* __restrict__ src, float* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
+cudaError_t launch_narrow_f32(const double* src, float* dst, size_t n, cudaStream_t st) {
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  if (n) narrow_f32_kernel<<<grid, 256, 0, st>>>(src, dst, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "ixb_internal.h"
 #include "ixb_reduce.cuh"
@@ -25,27 +26,27 @@ namespace ixb {
 template <int EQ>
 struct EqIsX { static constexpr bool value = (EQ & 1) != 0; };
 
-template <class R, int EQ, bool FAST>
-__device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<R>& io, int ii, int jj,
+template <class R, int EQ, bool FAST, class F>
+__device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj,
                                                 double& acc_bo) {
   if constexpr (EQ == EQ_UY) {
     return assemble_uy<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_UX) {
     R au;
     Row<R> r = assemble_ux<FAST>(G, io, ii, jj, au);
-    io.aux[G.at(ii, jj)] = au;
+    io.aux[G.at(ii, jj)] = F(au);
     return r;
   } else if constexpr (EQ == EQ_VY) {
     return assemble_vy<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_VX) {
     R av;
     Row<R> r = assemble_vx<FAST>(G, io, ii, jj, av);
-    io.aux[G.at(ii, jj)] = av;
+    io.aux[G.at(ii, jj)] = F(av);
     return r;
   } else if constexpr (EQ == EQ_PY) {
     return assemble_py<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_PX) {
-    R bo;
+    F bo;
     Row<R> r = assemble_px<FAST>(G, io, ii, jj, bo);
     io.aux[G.at(ii, jj)] = bo;
     acc_bo += (double)bo * (double)bo;
@@ -55,6 +56,28 @@ __device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<R
   } else {
     return assemble_tx<FAST>(G, io, ii, jj);
   }
+}
+
+// Arithmetic types of one sweep.  The binary64 solvers use binary64
+// throughout.  The mixed solver (handle precision IXB_PREC_FP32_REFINED)
+// stages and solves every line in binary32.  The u, v and T rows are
+// assembled in binary64 and turned into a defect correction (DC): the
+// binary64 residual d - A x of the current values is solved for in binary32
+// and the correction added back in binary64, so the fixed point of these
+// equations is the binary64 one.  The p' rows are assembled and solved in
+// binary32 (p' only steers the iteration; it vanishes at convergence), with
+// their mass source b_o evaluated in binary64.
+template <int SOLVER, int EQ>
+struct SweepTypes {
+  static constexpr bool MIX = SOLVER == SOLVER_MIXED;
+  static constexpr bool DC = MIX && EQ != EQ_PY && EQ != EQ_PX;
+  using S = typename std::conditional<MIX, float, double>::type;        // staged rows, line solve
+  using A = typename std::conditional<MIX && !DC, float, double>::type;  // coefficient assembly
+};
+
+template <class A>
+__host__ __device__ inline const Geo<A>& pick_geo(const Geo<double>& d, const Geo<float>& f) {
+  if constexpr (std::is_same<A, float>::value) return f; else return d;
 }
 
 // Boundary rows of impone_cond_frontera (source/mod_cond_frontera.f90:280-416):
@@ -80,13 +103,17 @@ __device__ __forceinline__ Row<R> bc_last_row(const BCEntry* t, int L) {
 // fused sweep kernel: TL lines per CTA, G threads per line (TL*G = 256)
 // ---------------------------------------------------------------------------
 template <class R, int EQ, int SOLVER, int TL, int G, int M>
-__global__ void __launch_bounds__(TL * G) sweep_kernel(const Geo<R> G_, const SweepIO<R> io, const int n,
-                                                       const int line_lo, const int line_hi, const int nfull) {
+__global__ void __launch_bounds__(TL * G)
+    sweep_kernel(const Geo<typename SweepTypes<SOLVER, EQ>::A> G_, const SweepIO<R> io, const int n,
+                 const int line_lo, const int line_hi, const int nfull) {
+  using ST = SweepTypes<SOLVER, EQ>;
+  using S = typename ST::S;
+  using A = typename ST::A;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sm = reinterpret_cast<R*>(smem_raw);
+  S* sm = reinterpret_cast<S*>(smem_raw);
   constexpr bool X = EqIsX<EQ>::value;
   constexpr int NT = TL * G;
-  const Geo<R>& Gm = G_;
+  const Geo<A>& Gm = G_;
   // M > 0: chunk length known at compile time (divisions by it become
   // multiply-shifts and the per-thread loops unroll)
   const int m = M > 0 ? M : io.m;
@@ -108,21 +135,32 @@ __global__ void __launch_bounds__(TL * G) sweep_kernel(const Geo<R> G_, const Sw
     else { l = idx % TL; r = idx / TL; }
     const int L = L0 + l;
     if (L < line_lo || L > line_hi) continue;
-    Row<R> row;
-    if (r >= n) row = Row<R>{R(0), R(1), R(0), R(0)};  // identity padding
-    else if (r == 0) row = bc_first_row<R>(io.bc_first, L);
-    else if (r == n - 1) row = bc_last_row<R>(io.bc_last, L);
+    Row<A> row;
+    if (r >= n) row = Row<A>{A(0), A(1), A(0), A(0)};  // identity padding
+    else if (r == 0) row = bc_first_row<A>(io.bc_first, L);
+    else if (r == n - 1) row = bc_last_row<A>(io.bc_last, L);
     else {
       const int ii = X ? r + 1 : L;
       const int jj = X ? L : r + 1;
-      row = assemble_cell<R, EQ, SOLVER == IXB_SOLVER_HYBRID>(Gm, io, ii, jj, acc_bo);
+      row = assemble_cell<A, EQ, SOLVER != IXB_SOLVER_EXACT>(Gm, io, ii, jj, acc_bo);
+    }
+    if constexpr (ST::DC) {
+      // defect correction: the row's binary64 residual at the current values
+      if (r < n) {
+        const int g = Gm.at(X ? r + 1 : L, X ? L : r + 1);
+        const int step = X ? 1 : Gm.LD;
+        double res = fma(-row.b, __ldg(io.in + g), row.d);
+        if (r > 0) res = fma(-row.a, __ldg(io.in + g - step), res);
+        if (r < n - 1) res = fma(-row.c, __ldg(io.in + g + step), res);
+        row.d = res;
+      }
     }
     const int ch = r / m;
     const int o = l * LS + ch * mp + (r - ch * m);
-    sm[o] = row.a;
-    sm[o + arr] = row.b;
-    sm[o + 2 * arr] = row.c;
-    sm[o + 3 * arr] = row.d;
+    sm[o] = S(row.a);
+    sm[o + arr] = S(row.b);
+    sm[o + 2 * arr] = S(row.c);
+    sm[o + 3 * arr] = S(row.d);
   }
   __syncthreads();
 
@@ -131,11 +169,11 @@ __global__ void __launch_bounds__(TL * G) sweep_kernel(const Geo<R> G_, const Sw
     const int l = threadIdx.x / G;
     const int L = L0 + l;
     const bool active = (L >= line_lo && L <= line_hi);
-    R* line = sm + l * LS;
-    if (SOLVER == IXB_SOLVER_EXACT) {
+    S* line = sm + l * LS;
+    if constexpr (SOLVER == IXB_SOLVER_EXACT) {
       if (active && threadIdx.x % G == 0) thomas_exact(line, line + arr, line + 2 * arr, line + 3 * arr, n, m, mp);
     } else {
-      chunk_solve<R, G>(line, m, mp, active, RS_PCR);
+      chunk_solve<S, G>(line, m, mp, active, RS_PCR);
     }
   }
   __syncthreads();
@@ -155,7 +193,9 @@ __global__ void __launch_bounds__(TL * G) sweep_kernel(const Geo<R> G_, const Sw
     R x;
     if (L >= line_lo && L <= line_hi) {
       const int ch = r / m;
-      x = sm[l * LS + 3 * arr + ch * mp + (r - ch * m)];
+      const S xs = sm[l * LS + 3 * arr + ch * mp + (r - ch * m)];
+      if constexpr (ST::DC) x = io.in[g] + R(xs);
+      else x = R(xs);
       if (io.nrm0.partials && r >= 1 && r <= n - 2) {
         const double dv = (double)x - (io.prev ? (double)io.prev[g] : 0.0);
         acc += dv * dv;
@@ -180,8 +220,10 @@ __global__ void __launch_bounds__(TL * G) sweep_kernel(const Geo<R> G_, const Sw
 #define IXB_SWEEP_SHAPES(X_) X_(1, 128) X_(1, 256) X_(2, 64) X_(2, 128) X_(4, 32) X_(4, 64) X_(8, 32)
 
 template <class R, int EQ, int SOLVER, int TL, int G>
-static cudaError_t sweep_launch_one(const SweepShape& s, const Geo<R>& Gm, const SweepIO<R>& io, cudaStream_t st) {
-  if (SOLVER == IXB_SOLVER_HYBRID && s.m == 3) {
+static cudaError_t sweep_launch_one(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
+                                    const SweepIO<R>& io, cudaStream_t st) {
+  const auto& Gm = pick_geo<typename SweepTypes<SOLVER, EQ>::A>(Gd, Gf);
+  if (SOLVER != IXB_SOLVER_EXACT && s.m == 3) {
     sweep_kernel<R, EQ, SOLVER, TL, G, 3><<<s.grid, TL * G, s.smem, st>>>(Gm, io, s.n, s.line_lo, s.line_hi, s.nfull);
   } else {
     sweep_kernel<R, EQ, SOLVER, TL, G, 0><<<s.grid, TL * G, s.smem, st>>>(Gm, io, s.n, s.line_lo, s.line_hi, s.nfull);
@@ -190,9 +232,10 @@ static cudaError_t sweep_launch_one(const SweepShape& s, const Geo<R>& Gm, const
 }
 
 template <class R, int EQ, int SOLVER>
-cudaError_t sweep_launch_solver(const SweepShape& s, const Geo<R>& Gm, const SweepIO<R>& io, cudaStream_t st) {
+cudaError_t sweep_launch_solver(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
+                                const SweepIO<R>& io, cudaStream_t st) {
 #define IXB_CASE_(TL_, G_) \
-  if (s.tl == TL_ && s.g == G_) return sweep_launch_one<R, EQ, SOLVER, TL_, G_>(s, Gm, io, st);
+  if (s.tl == TL_ && s.g == G_) return sweep_launch_one<R, EQ, SOLVER, TL_, G_>(s, Gd, Gf, io, st);
   IXB_SWEEP_SHAPES(IXB_CASE_)
 #undef IXB_CASE_
   return cudaErrorInvalidValue;
@@ -205,7 +248,7 @@ cudaError_t sweep_smem_limit_solver(int bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   };
 #define IXB_SET_(TL_, G_)                        \
-  if (SOLVER == IXB_SOLVER_HYBRID)             \
+  if (SOLVER != IXB_SOLVER_EXACT)              \
     set(sweep_kernel<R, EQ, SOLVER, TL_, G_, 3>); \
   set(sweep_kernel<R, EQ, SOLVER, TL_, G_, 0>);
   IXB_SWEEP_SHAPES(IXB_SET_)
@@ -220,7 +263,7 @@ int sweep_blocks_per_sm_solver(const SweepShape& s) {
   cudaError_t e = cudaErrorInvalidValue;
 #define IXB_OCC_(TL_, G_)                                                                                    \
   if (s.tl == TL_ && s.g == G_) {                                                                            \
-    if (SOLVER == IXB_SOLVER_HYBRID && s.m == 3)                                                             \
+    if (SOLVER != IXB_SOLVER_EXACT && s.m == 3)                                                              \
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, SOLVER, TL_, G_, 3>,         \
                                                         TL_ * G_, s.smem);                                   \
     else                                                                                                     \

@@ -3,7 +3,8 @@
 
 namespace ixb {
 template cudaError_t sweep_launch_solver<double, EQ_UX, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&,
-                                                                     const SweepIO<double>&, cudaStream_t);
+                                                                     const Geo<float>&, const SweepIO<double>&,
+                                                                     cudaStream_t);
 template cudaError_t sweep_smem_limit_solver<double, EQ_UX, IXB_SOLVER_HYBRID>(int);
 template int sweep_blocks_per_sm_solver<double, EQ_UX, IXB_SOLVER_HYBRID>(const SweepShape&);
 }  // namespace ixb

@@ -3,7 +3,8 @@
 
 namespace ixb {
 template cudaError_t sweep_launch_solver<double, EQ_VY, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&,
-                                                                     const SweepIO<double>&, cudaStream_t);
+                                                                     const Geo<float>&, const SweepIO<double>&,
+                                                                     cudaStream_t);
 template cudaError_t sweep_smem_limit_solver<double, EQ_VY, IXB_SOLVER_EXACT>(int);
 template int sweep_blocks_per_sm_solver<double, EQ_VY, IXB_SOLVER_EXACT>(const SweepShape&);
 }  // namespace ixb
