@@ -60,6 +60,11 @@ struct ixb_handle {
   double *p = nullptr, *u_ant = nullptr, *v_ant = nullptr, *T_ant = nullptr;
   double *au = nullptr, *av = nullptr, *b_o = nullptr, *resu = nullptr;
   double *fcon[3] = {}, *flin[3] = {};
+  double* zero = nullptr;  // a field of zeros: the sources of an equation without any
+  // rows of one sweep staged between its assembly and its line solve
+  void* stage = nullptr;
+  size_t stage_stride = 0;  // elements per row array
+  int stage_P = 0;          // row pitch of a line
   int cu = 0, cv = 0, cT = 0, cpc = 0;
   // mesh
   double* metrics = nullptr;
@@ -188,7 +193,6 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
   io.u = h->u[h->cu]; io.v = h->v[h->cv]; io.T = h->T[h->cT]; io.p = h->p; io.pc = h->pc[h->cpc];
   io.u_ant = h->u_ant; io.v_ant = h->v_ant; io.T_ant = h->T_ant;
   io.au = h->au; io.av = h->av;
-  io.m = s.m; io.mp = s.mp; io.rs = s.rs;
   int var = -1;
   int* cur = nullptr;
   double** buf = nullptr;
@@ -201,8 +205,10 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
   io.in = buf[*cur];
   io.out = buf[*cur ^ 1];
   io.prev = prev;
+  io.fcon = io.flin = h->zero;
   if (var >= 0) {
-    io.fcon = h->fcon[var]; io.flin = h->flin[var];
+    if (h->fcon[var]) io.fcon = h->fcon[var];
+    if (h->flin[var]) io.flin = h->flin[var];
     const bool x = (eq & 1) != 0;
     const BCEntry* base = h->bc + (size_t)var * 4 * h->bcstride;
     io.bc_first = base + (size_t)(x ? 0 : 1) * h->bcstride;
@@ -217,7 +223,8 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
     if (eq == EQ_TX) io.nrm0 = slot(h, N_DT);
   }
   const Geo<float> Gf = h->metrics32 ? make_geo32(h) : Geo<float>{};
-  CK(launch_sweep_f64(eq, solver_form(h), s, G, Gf, io, h->stream));
+  const StageBuf stage{h->stage, h->stage_stride, h->stage_P};
+  CK(launch_sweep_f64(eq, solver_form(h), s, G, Gf, io, stage, h->stream));
   *cur ^= 1;
   return IXB_OK;
 }
@@ -524,11 +531,12 @@ void free_all(ixb_handle* h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   double** bufs[] = {&h->u[0], &h->u[1], &h->v[0], &h->v[1], &h->T[0], &h->T[1], &h->pc[0], &h->pc[1],
-                     &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu,
+                     &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu, &h->zero,
                      &h->fcon[0], &h->fcon[1], &h->fcon[2], &h->flin[0], &h->flin[1], &h->flin[2],
                      &h->metrics, &h->tables, &h->xp_d, &h->yp_d, &h->partials, &h->norms, &h->nu_d};
   for (auto b : bufs) if (*b) cudaFree(*b);
   if (h->metrics32) cudaFree(h->metrics32);
+  if (h->stage) cudaFree(h->stage);
   if (h->tables32) cudaFree(h->tables32);
   if (h->bc) cudaFree(h->bc);
   if (h->counters) cudaFree(h->counters);
@@ -611,7 +619,7 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   h->own_stream = true;
   const size_t fb = h->fsz * sizeof(double);
   double** fields[] = {&h->u[0], &h->u[1], &h->v[0], &h->v[1], &h->T[0], &h->T[1], &h->pc[0], &h->pc[1],
-                       &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu};
+                       &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu, &h->zero};
   for (auto f : fields) {
     if (cudaMalloc(f, fb) != cudaSuccess) return fail(IXB_ENOMEM);
     if (cudaMemset(*f, 0, fb) != cudaSuccess) return fail(IXB_ECUDA);
@@ -636,7 +644,11 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   h->bcstride = std::max(mi, nj) + 3;
   if (cudaMalloc(&h->bc, (size_t)12 * h->bcstride * sizeof(BCEntry)) != cudaSuccess) return fail(IXB_ENOMEM);
   cudaMemset(h->bc, 0, (size_t)12 * h->bcstride * sizeof(BCEntry));
-  h->pstride = std::max(max_sweep_lines(mi, nj), residual_grid(mi, nj)) + 32;
+  h->pstride = std::max(std::max(max_sweep_lines(mi, nj), residual_grid(mi, nj)), kAsmGridCap) + 32;
+  // staged rows: up to max(mi, nj) + 2 lines of up to max(mi, nj) + 2 rows, binary64
+  h->stage_P = (std::max(mi, nj) + 2 + 31) / 32 * 32;
+  h->stage_stride = (size_t)max_sweep_lines(mi, nj) * h->stage_P;
+  if (cudaMalloc(&h->stage, 4 * h->stage_stride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMalloc(&h->partials, (size_t)N_COUNT * h->pstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMalloc(&h->counters, N_COUNT * sizeof(unsigned int)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMemset(h->counters, 0, N_COUNT * sizeof(unsigned int)) != cudaSuccess) return fail(IXB_ECUDA);

@@ -93,11 +93,11 @@ struct Geo {
 
 template <class R>
 struct SweepIO {
-  const R *u, *v, *T, *p, *pc;        // current fields (pc may be null: p' = 0)
+  const R *u, *v, *T, *p, *pc;        // current fields
   const R *u_ant, *v_ant, *T_ant;
   const R *au, *av;
-  const R *fcon, *flin;               // sources of this equation (null: zero)
-  const R* in;                        // swept field, current values (null: zero)
+  const R *fcon, *flin;               // sources of this equation (a zero field when none)
+  const R* in;                        // swept field, current values
   R* out;                             // swept field, new values
   const R* prev;                      // field at the start of the inner pass (null: zero)
   R* aux;                             // au (u-x), av (v-x), b_o (p'-x)
@@ -105,8 +105,6 @@ struct SweepIO {
   const BCEntry* bc_last;
   NormSlot nrm0;                      // ||out - prev|| over interior rows of solved lines
   NormSlot nrm1;                      // ||b_o|| (p'-x)
-  int m, mp;                          // rows per thread chunk, padded chunk pitch
-  int rs;                             // reduced-system solver (RS_PCR / RS_WARP)
 };
 
 template <class R>
@@ -204,8 +202,8 @@ __device__ __forceinline__ Row<R> assemble_ux(const Geo<R>& G, const SweepIO<F>&
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
-  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
+  const R flin = ld<R>(io.flin, c0);
+  const R fcon = ld<R>(io.fcon, c0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
@@ -225,8 +223,8 @@ __device__ __forceinline__ Row<R> assemble_uy(const Geo<R>& G, const SweepIO<F>&
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
-  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
+  const R flin = ld<R>(io.flin, c0);
+  const R fcon = ld<R>(io.fcon, c0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
@@ -278,8 +276,8 @@ __device__ __forceinline__ Row<R> assemble_vx(const Geo<R>& G, const SweepIO<F>&
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
+  const R flin = ld<R>(io.flin, c0);
+  const R fcon = ld<R>(io.fcon, c0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
@@ -299,8 +297,8 @@ __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<F>&
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
+  const R flin = ld<R>(io.flin, c0);
+  const R fcon = ld<R>(io.fcon, c0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
@@ -346,8 +344,8 @@ __device__ __forceinline__ Row<R> assemble_tx(const Geo<R>& G, const SweepIO<F>&
   t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
+  const R flin = ld<R>(io.flin, c0);
+  const R fcon = ld<R>(io.fcon, c0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
@@ -364,8 +362,8 @@ __device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<F>&
   t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);
-  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
+  const R flin = ld<R>(io.flin, c0);
+  const R fcon = ld<R>(io.fcon, c0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
@@ -380,7 +378,7 @@ __device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<F>&
 // ---------------------------------------------------------------------------
 template <class R, class F>
 __device__ __forceinline__ R pc_at(const SweepIO<F>& io, const Geo<R>& G, int ii, int jj) {
-  return io.in ? ld<R>(io.in, G.at(ii, jj)) : R(0);
+  return ld<R>(io.in, G.at(ii, jj));
 }
 
 // Mass source b_o = (u_w - u_e) dy + (v_s - v_n) dx of the p' rows, always
@@ -657,20 +655,19 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
   }
   R x0, xl;
   if (rs == RS_PCR) {
-    R* A[2] = {red, red + 6 * G};
-    R* C[2] = {red + 2 * G, red + 8 * G};
-    R* D[2] = {red + 4 * G, red + 10 * G};
+    // two buffers of the 2G rows (a | c | d), swapped every step
+    R* cur = red;
+    R* nxt = red + 6 * G;
     if (active) {
-      A[0][2 * k] = eA; C[0][2 * k] = eC; D[0][2 * k] = eD;
-      A[0][2 * k + 1] = oA; C[0][2 * k + 1] = oC; D[0][2 * k + 1] = oD;
+      cur[2 * k] = eA; cur[2 * G + 2 * k] = eC; cur[4 * G + 2 * k] = eD;
+      cur[2 * k + 1] = oA; cur[2 * G + 2 * k + 1] = oC; cur[4 * G + 2 * k + 1] = oD;
     }
     __syncthreads();
-    int cur = 0;
 #pragma unroll 1
     for (int s = 1; s < 2 * G; s <<= 1) {
       if (active) {
-        const R* Ac = A[cur]; const R* Cc = C[cur]; const R* Dc = D[cur];
-        R* An = A[cur ^ 1]; R* Cn = C[cur ^ 1]; R* Dn = D[cur ^ 1];
+        const R* Ac = cur; const R* Cc = cur + 2 * G; const R* Dc = cur + 4 * G;
+        R* An = nxt; R* Cn = nxt + 2 * G; R* Dn = nxt + 4 * G;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           const int i = k + q * G;
@@ -685,10 +682,10 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
         }
       }
       __syncthreads();
-      cur ^= 1;
+      R* t = cur; cur = nxt; nxt = t;
     }
-    x0 = D[cur][2 * k];
-    xl = D[cur][2 * k + 1];
+    x0 = cur[4 * G + 2 * k];
+    xl = cur[4 * G + 2 * k + 1];
   } else {
     // reduced system in the warp solver's [32][M2P] chunk layout
     constexpr int ARR2 = 32 * M2P;

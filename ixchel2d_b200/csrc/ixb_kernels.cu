@@ -206,14 +206,12 @@ SweepShape sweep_shape(int eq, int mi, int nj, int real_bytes, int tl, int g) {
     default: { constexpr int E_ = EQ_TX; __VA_ARGS__; }              \
   }
 
+// Orientation and defect-correction flag of the line solve of sweep `eq`.
+static bool eq_is_x(int eq) { return (eq & 1) != 0; }
+static bool eq_dc(int eq, int solver) { return solver == SOLVER_MIXED && eq != EQ_PY && eq != EQ_PX; }
+
 int sweep_occupancy(int eq, int solver, const SweepShape& s) {
-  if (solver == IXB_SOLVER_EXACT) {
-    IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, IXB_SOLVER_EXACT>(s))
-  }
-  if (solver == SOLVER_MIXED) {
-    IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, SOLVER_MIXED>(s))
-  }
-  IXB_EQ_SWITCH(return sweep_blocks_per_sm_solver<double, E_, IXB_SOLVER_HYBRID>(s))
+  return solve_blocks_per_sm(solver, eq_is_x(eq), eq_dc(eq, solver), s);
 }
 
 cudaError_t sweep_set_smem_limits() {
@@ -224,29 +222,33 @@ cudaError_t sweep_set_smem_limits() {
   if (e != cudaSuccess) return e;
   e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
-  const int bytes = optin - 1024;  // room for the static reduction buffers
-  for (int eq = 0; eq < EQ_COUNT && e == cudaSuccess; ++eq) {
-    auto f = [&]() -> cudaError_t {
-      IXB_EQ_SWITCH(cudaError_t r = sweep_smem_limit_solver<double, E_, IXB_SOLVER_EXACT>(bytes);
-                    if (r == cudaSuccess) r = sweep_smem_limit_solver<double, E_, IXB_SOLVER_HYBRID>(bytes);
-                    if (r == cudaSuccess) r = sweep_smem_limit_solver<double, E_, SOLVER_MIXED>(bytes);
-                    return r)
-    };
-    e = f();
-  }
+  e = solve_set_smem_limits(optin - 1024);  // room for the static reduction buffers
   if (e == cudaSuccess) done = 1;
   return e;
 }
 
+// One sweep: the cell-parallel assembly stages the rows of every solved
+// line in `buf`, then the line solve writes the field.
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
-                             const Geo<float>& Gf, const SweepIO<double>& io, cudaStream_t st) {
+                             const Geo<float>& Gf, const SweepIO<double>& io, const StageBuf& buf,
+                             cudaStream_t st) {
+  cudaError_t e;
   if (solver == IXB_SOLVER_EXACT) {
-    IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_EXACT>(s, G, Gf, io, st))
+    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, IXB_SOLVER_EXACT>(s, G, Gf, io, buf, st)) };
+    e = f();
+  } else if (solver == SOLVER_MIXED) {
+    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, SOLVER_MIXED>(s, G, Gf, io, buf, st)) };
+    e = f();
+  } else {
+    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, IXB_SOLVER_HYBRID>(s, G, Gf, io, buf, st)) };
+    e = f();
   }
-  if (solver == SOLVER_MIXED) {
-    IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, SOLVER_MIXED>(s, G, Gf, io, st))
-  }
-  IXB_EQ_SWITCH(return sweep_launch_solver<double, E_, IXB_SOLVER_HYBRID>(s, G, Gf, io, st))
+  if (e != cudaSuccess) return e;
+  SolveIO so{};
+  so.coef = buf.base; so.stride = buf.stride; so.P = buf.P;
+  so.in = io.in; so.out = io.out; so.prev = io.prev; so.nrm0 = io.nrm0;
+  so.LD = G.LD; so.m = s.m; so.mp = s.mp;
+  return solve_launch(solver, eq_is_x(eq), eq_dc(eq, solver), s, so, st);
 }
 
 __global__ void narrow_f32_kernel(const double* __restrict__ src, float* __restrict__ dst, size_t n) {

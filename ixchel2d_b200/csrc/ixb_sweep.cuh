@@ -1,14 +1,17 @@
-// ixb_sweep.cuh -- the fused line-sweep kernel (assembly + boundary rows +
-// partitioned line solve + write-back with the pass norm), included by the
-// per-equation translation units ixb_sweep_{u,v,p,t}.cu.
+// ixb_sweep.cuh -- the assembly half of a line sweep: every row of the
+// sweep's tridiagonal systems (coefficients, boundary rows, and for the
+// mixed-precision form the binary64 defect-correction residual) evaluated
+// cell-parallel and staged line-major for the line solver (ixb_solve.cu).
+// Included by the per-equation translation units ixb_sweep_<eq>[_fast|_mixed].cu.
 //
-// One fused kernel per line sweep replaces the reference's four OpenACC
-// regions per sweep (assembly, impone_cond_frontera, tridiagonal, scatter;
-// e.g. source/main.f90:420-484): a CTA owns TL adjacent lines, assembles
-// their rows straight from the fields into shared memory (coalesced along
-// ii), applies the boundary rows from a per-line table, solves the lines with
-// G = 256/TL threads each, and writes the solution to the ping-pong output
-// buffer, reducing the convergence norm of the pass on the way out.
+// A sweep of the reference is four OpenACC regions (assembly,
+// impone_cond_frontera, tridiagonal, scatter; e.g. source/main.f90:420-484).
+// Here it is two kernels: this cell-parallel assembly (one thread per cell,
+// loads coalesced along ii, enough warps to hide the latency of its ~30
+// stencil loads) writing rows a,b,c,d of every solved line contiguously, and
+// the partitioned line solve that reads them back coalesced.  y-sweep tiles
+// are transposed through shared memory so that both the field reads and the
+// row writes are coalesced.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -26,30 +29,34 @@ namespace ixb {
 template <int EQ>
 struct EqIsX { static constexpr bool value = (EQ & 1) != 0; };
 
+// Row of cell (ii,jj); the side outputs (au, av, b_o and the b_o norm) are
+// written only when `keep` is set.
 template <class R, int EQ, bool FAST, class F>
 __device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj,
-                                                double& acc_bo) {
+                                                double& acc_bo, bool keep) {
   if constexpr (EQ == EQ_UY) {
     return assemble_uy<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_UX) {
     R au;
     Row<R> r = assemble_ux<FAST>(G, io, ii, jj, au);
-    io.aux[G.at(ii, jj)] = F(au);
+    if (keep) io.aux[G.at(ii, jj)] = F(au);
     return r;
   } else if constexpr (EQ == EQ_VY) {
     return assemble_vy<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_VX) {
     R av;
     Row<R> r = assemble_vx<FAST>(G, io, ii, jj, av);
-    io.aux[G.at(ii, jj)] = F(av);
+    if (keep) io.aux[G.at(ii, jj)] = F(av);
     return r;
   } else if constexpr (EQ == EQ_PY) {
     return assemble_py<FAST>(G, io, ii, jj);
   } else if constexpr (EQ == EQ_PX) {
     F bo;
     Row<R> r = assemble_px<FAST>(G, io, ii, jj, bo);
-    io.aux[G.at(ii, jj)] = bo;
-    acc_bo += (double)bo * (double)bo;
+    if (keep) {
+      io.aux[G.at(ii, jj)] = bo;
+      acc_bo += (double)bo * (double)bo;
+    }
     return r;
   } else if constexpr (EQ == EQ_TY) {
     return assemble_ty<FAST>(G, io, ii, jj);
@@ -100,114 +107,104 @@ __device__ __forceinline__ Row<R> bc_last_row(const BCEntry* t, int L) {
 }
 
 // ---------------------------------------------------------------------------
-// fused sweep kernel: TL lines per CTA, G threads per line (TL*G = 256)
+// assembly kernel
 // ---------------------------------------------------------------------------
-template <class R, int EQ, int SOLVER, int TL, int G, int M>
-__global__ void __launch_bounds__(TL * G)
-    sweep_kernel(const Geo<typename SweepTypes<SOLVER, EQ>::A> G_, const SweepIO<R> io, const int n,
-                 const int line_lo, const int line_hi, const int nfull) {
+// Row of line L, position r (0-based along the line) of sweep EQ, or an
+// identity row outside the line.  Rows outside the interior are assembled
+// at the nearest interior cell and then replaced, so every load is in bounds
+// and no branch separates a thread's loads.
+template <int EQ, int SOLVER>
+__device__ __forceinline__ Row<typename SweepTypes<SOLVER, EQ>::A> staged_row(
+    const Geo<typename SweepTypes<SOLVER, EQ>::A>& Gm, const SweepIO<double>& io, int L, int r, int n, int line_lo,
+    int line_hi, bool valid, double& acc_bo) {
   using ST = SweepTypes<SOLVER, EQ>;
-  using S = typename ST::S;
   using A = typename ST::A;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S* sm = reinterpret_cast<S*>(smem_raw);
   constexpr bool X = EqIsX<EQ>::value;
-  constexpr int NT = TL * G;
-  const Geo<A>& Gm = G_;
-  // M > 0: chunk length known at compile time (divisions by it become
-  // multiply-shifts and the per-thread loops unroll)
-  const int m = M > 0 ? M : io.m;
-  const int mp = M > 0 ? (M | 1) : io.mp;
-  const int npad = G * m;
-  const int LS = (int)line_smem_elems(G, mp);
-  const int arr = G * mp;
-  const int L0 = 1 + blockIdx.x * TL;
+  const int Lc = min(max(L, line_lo), line_hi);
+  const int rc = min(max(r, 1), n - 2);
+  const bool interior = valid && r >= 1 && r <= n - 2;
+  Row<A> row = assemble_cell<A, EQ, SOLVER != IXB_SOLVER_EXACT>(Gm, io, X ? rc + 1 : Lc, X ? Lc : rc + 1, acc_bo,
+                                                                interior);
+  const Row<A> first = bc_first_row<A>(io.bc_first, Lc);
+  const Row<A> last = bc_last_row<A>(io.bc_last, Lc);
+  if (r == 0) row = first;
+  else if (r == n - 1) row = last;
+  if constexpr (ST::DC) {
+    // defect correction: the row's binary64 residual at the current values
+    const int rr = min(max(r, 0), n - 1);
+    const int g = Gm.at(X ? rr + 1 : Lc, X ? Lc : rr + 1);
+    const int step = X ? 1 : Gm.LD;
+    const double xm = __ldg(io.in + (rr > 0 ? g - step : g));
+    const double x0 = __ldg(io.in + g);
+    const double xp = __ldg(io.in + (rr < n - 1 ? g + step : g));
+    double res = fma(-row.b, x0, row.d);
+    res = fma(-row.a, xm, res);
+    res = fma(-row.c, xp, res);
+    row.d = res;
+  }
+  return row;
+}
+
+// x-sweep tiles: 64 consecutive rows of 4 lines, one cell per thread.
+// y-sweep tiles: 32 consecutive lines (adjacent ii) x 8 rows, one cell per
+// thread, written back through shared memory as 8-row runs of each line.
+constexpr int kAsmThreads = 256;
+constexpr int kAsmXR = 64, kAsmXL = 4;
+constexpr int kAsmYL = 32, kAsmYR = 8;
+
+__host__ __device__ constexpr int asm_tiles(bool x, int n, int nlines) {
+  return x ? ((n + kAsmXR - 1) / kAsmXR) * ((nlines + kAsmXL - 1) / kAsmXL)
+           : ((nlines + kAsmYL - 1) / kAsmYL) * ((n + kAsmYR - 1) / kAsmYR);
+}
+
+// Assemble the rows of lines line_lo..line_hi of sweep EQ into `co`
+// (line L at (L - line_lo) * P).  Grid-stride over tiles; the b_o norm
+// (p'-x) is reduced over the grid.
+template <int EQ, int SOLVER>
+__global__ void __launch_bounds__(kAsmThreads)
+    assemble_kernel(const Geo<typename SweepTypes<SOLVER, EQ>::A> G_, const SweepIO<double> io,
+                    const Coef<typename SweepTypes<SOLVER, EQ>::S> co, const int n, const int line_lo,
+                    const int line_hi) {
+  using S = typename SweepTypes<SOLVER, EQ>::S;
+  constexpr bool X = EqIsX<EQ>::value;
+  const int nl = line_hi - line_lo + 1;
+  const int ntiles = asm_tiles(X, n, nl);
   double acc_bo = 0.0;
-
-  // phase 1: assemble every row of the solved lines into shared memory;
-  // TL*npad = NT*m, so every thread handles exactly m rows
-#pragma unroll
-  for (int it = 0; it < (M > 0 ? M : 32); ++it) {  // m <= 25 (ixb_create bounds the grid)
-    if (M == 0 && it >= m) break;
-    const int idx = threadIdx.x + it * NT;
-    int l, r;
-    if (X) { l = TL == 1 ? 0 : idx / npad; r = idx - l * npad; }
-    else { l = idx % TL; r = idx / TL; }
-    const int L = L0 + l;
-    if (L < line_lo || L > line_hi) continue;
-    Row<A> row;
-    if (r >= n) row = Row<A>{A(0), A(1), A(0), A(0)};  // identity padding
-    else if (r == 0) row = bc_first_row<A>(io.bc_first, L);
-    else if (r == n - 1) row = bc_last_row<A>(io.bc_last, L);
-    else {
-      const int ii = X ? r + 1 : L;
-      const int jj = X ? L : r + 1;
-      row = assemble_cell<A, EQ, SOLVER != IXB_SOLVER_EXACT>(Gm, io, ii, jj, acc_bo);
-    }
-    if constexpr (ST::DC) {
-      // defect correction: the row's binary64 residual at the current values
-      if (r < n) {
-        const int g = Gm.at(X ? r + 1 : L, X ? L : r + 1);
-        const int step = X ? 1 : Gm.LD;
-        double res = fma(-row.b, __ldg(io.in + g), row.d);
-        if (r > 0) res = fma(-row.a, __ldg(io.in + g - step), res);
-        if (r < n - 1) res = fma(-row.c, __ldg(io.in + g + step), res);
-        row.d = res;
+  if constexpr (X) {
+    const int tr_n = (n + kAsmXR - 1) / kAsmXR;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      const int tl = tile / tr_n, tr = tile - tl * tr_n;
+      const int r = tr * kAsmXR + (threadIdx.x % kAsmXR);
+      const int L = line_lo + tl * kAsmXL + threadIdx.x / kAsmXR;
+      const bool valid = r < n && L <= line_hi;
+      const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
+      if (valid) {
+        const size_t o = (size_t)(L - line_lo) * co.P + r;
+        co.a[o] = S(row.a); co.b[o] = S(row.b); co.c[o] = S(row.c); co.d[o] = S(row.d);
       }
     }
-    const int ch = r / m;
-    const int o = l * LS + ch * mp + (r - ch * m);
-    sm[o] = S(row.a);
-    sm[o + arr] = S(row.b);
-    sm[o + 2 * arr] = S(row.c);
-    sm[o + 3 * arr] = S(row.d);
-  }
-  __syncthreads();
-
-  // phase 2: line solves
-  {
-    const int l = threadIdx.x / G;
-    const int L = L0 + l;
-    const bool active = (L >= line_lo && L <= line_hi);
-    S* line = sm + l * LS;
-    if constexpr (SOLVER == IXB_SOLVER_EXACT) {
-      if (active && threadIdx.x % G == 0) thomas_exact(line, line + arr, line + 2 * arr, line + 3 * arr, n, m, mp);
-    } else {
-      chunk_solve<S, G>(line, m, mp, active, RS_PCR);
-    }
-  }
-  __syncthreads();
-
-  // phase 3: write the new field (unsolved lines keep their values) and
-  // accumulate ||new - prev|| over the interior rows of the solved lines
-  double acc = 0.0;
-  for (int idx = threadIdx.x; idx < TL * n; idx += NT) {
-    int l, r;
-    if (X) { l = TL == 1 ? 0 : idx / n; r = idx - l * n; }
-    else { l = idx % TL; r = idx / TL; }
-    const int L = L0 + l;
-    if (L > nfull) continue;
-    const int ii = X ? r + 1 : L;
-    const int jj = X ? L : r + 1;
-    const int g = Gm.at(ii, jj);
-    R x;
-    if (L >= line_lo && L <= line_hi) {
-      const int ch = r / m;
-      const S xs = sm[l * LS + 3 * arr + ch * mp + (r - ch * m)];
-      if constexpr (ST::DC) x = io.in[g] + R(xs);
-      else x = R(xs);
-      if (io.nrm0.partials && r >= 1 && r <= n - 2) {
-        const double dv = (double)x - (io.prev ? (double)io.prev[g] : 0.0);
-        acc += dv * dv;
+  } else {
+    __shared__ S tile_s[4][kAsmYR][kAsmYL + 1];
+    const int tl_n = (nl + kAsmYL - 1) / kAsmYL;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      const int tr = tile / tl_n, tl = tile - tr * tl_n;
+      const int lo = threadIdx.x % kAsmYL, ro = threadIdx.x / kAsmYL;
+      const int L = line_lo + tl * kAsmYL + lo;  // adjacent ii in a warp: coalesced field reads
+      const int r = tr * kAsmYR + ro;
+      const bool valid = r < n && L <= line_hi;
+      const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
+      tile_s[0][ro][lo] = S(row.a); tile_s[1][ro][lo] = S(row.b);
+      tile_s[2][ro][lo] = S(row.c); tile_s[3][ro][lo] = S(row.d);
+      __syncthreads();
+      const int wl = threadIdx.x / kAsmYR, wr = threadIdx.x % kAsmYR;  // 8-row runs of one line
+      const int Lw = line_lo + tl * kAsmYL + wl, rw = tr * kAsmYR + wr;
+      if (Lw <= line_hi && rw < n) {
+        const size_t o = (size_t)(Lw - line_lo) * co.P + rw;
+        co.a[o] = tile_s[0][wr][wl]; co.b[o] = tile_s[1][wr][wl];
+        co.c[o] = tile_s[2][wr][wl]; co.d[o] = tile_s[3][wr][wl];
       }
-    } else {
-      x = io.in ? io.in[g] : R(0);
+      __syncthreads();
     }
-    io.out[g] = x;
-  }
-  if (io.nrm0.partials) {
-    const double s = block_sum(acc);
-    finish_norm(io.nrm0, s);
   }
   if (io.nrm1.partials) {
     const double s = block_sum(acc_bo);
@@ -215,64 +212,20 @@ __global__ void __launch_bounds__(TL * G)
   }
 }
 
-
-// Launch shapes (lines per CTA x threads per line); 128 or 256 threads.
-#define IXB_SWEEP_SHAPES(X_) X_(1, 128) X_(1, 256) X_(2, 64) X_(2, 128) X_(4, 32) X_(4, 64) X_(8, 32)
-
-template <class R, int EQ, int SOLVER, int TL, int G>
-static cudaError_t sweep_launch_one(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
-                                    const SweepIO<R>& io, cudaStream_t st) {
-  const auto& Gm = pick_geo<typename SweepTypes<SOLVER, EQ>::A>(Gd, Gf);
-  if (SOLVER != IXB_SOLVER_EXACT && s.m == 3) {
-    sweep_kernel<R, EQ, SOLVER, TL, G, 3><<<s.grid, TL * G, s.smem, st>>>(Gm, io, s.n, s.line_lo, s.line_hi, s.nfull);
-  } else {
-    sweep_kernel<R, EQ, SOLVER, TL, G, 0><<<s.grid, TL * G, s.smem, st>>>(Gm, io, s.n, s.line_lo, s.line_hi, s.nfull);
-  }
+template <int EQ, int SOLVER>
+cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
+                            const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st) {
+  using ST = SweepTypes<SOLVER, EQ>;
+  using S = typename ST::S;
+  const auto& Gm = pick_geo<typename ST::A>(Gd, Gf);
+  Coef<S> co;
+  S* base = static_cast<S*>(buf.base);
+  co.a = base; co.b = base + buf.stride; co.c = base + 2 * buf.stride; co.d = base + 3 * buf.stride;
+  co.P = buf.P;
+  const int tiles = asm_tiles(EqIsX<EQ>::value, s.n, s.line_hi - s.line_lo + 1);
+  const int grid = std::max(1, std::min(tiles, kAsmGridCap));
+  assemble_kernel<EQ, SOLVER><<<grid, kAsmThreads, 0, st>>>(Gm, io, co, s.n, s.line_lo, s.line_hi);
   return cudaGetLastError();
-}
-
-template <class R, int EQ, int SOLVER>
-cudaError_t sweep_launch_solver(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
-                                const SweepIO<R>& io, cudaStream_t st) {
-#define IXB_CASE_(TL_, G_) \
-  if (s.tl == TL_ && s.g == G_) return sweep_launch_one<R, EQ, SOLVER, TL_, G_>(s, Gd, Gf, io, st);
-  IXB_SWEEP_SHAPES(IXB_CASE_)
-#undef IXB_CASE_
-  return cudaErrorInvalidValue;
-}
-
-template <class R, int EQ, int SOLVER>
-cudaError_t sweep_smem_limit_solver(int bytes) {
-  cudaError_t e = cudaSuccess;
-  auto set = [&](auto k) {
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  };
-#define IXB_SET_(TL_, G_)                        \
-  if (SOLVER != IXB_SOLVER_EXACT)              \
-    set(sweep_kernel<R, EQ, SOLVER, TL_, G_, 3>); \
-  set(sweep_kernel<R, EQ, SOLVER, TL_, G_, 0>);
-  IXB_SWEEP_SHAPES(IXB_SET_)
-#undef IXB_SET_
-  return e;
-}
-
-// Resident CTAs per SM of the kernel a shape launches (0 if it cannot run).
-template <class R, int EQ, int SOLVER>
-int sweep_blocks_per_sm_solver(const SweepShape& s) {
-  int nb = 0;
-  cudaError_t e = cudaErrorInvalidValue;
-#define IXB_OCC_(TL_, G_)                                                                                    \
-  if (s.tl == TL_ && s.g == G_) {                                                                            \
-    if (SOLVER != IXB_SOLVER_EXACT && s.m == 3)                                                              \
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, SOLVER, TL_, G_, 3>,         \
-                                                        TL_ * G_, s.smem);                                   \
-    else                                                                                                     \
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<R, EQ, SOLVER, TL_, G_, 0>,         \
-                                                        TL_ * G_, s.smem);                                   \
-  }
-  IXB_SWEEP_SHAPES(IXB_OCC_)
-#undef IXB_OCC_
-  return e == cudaSuccess ? nb : 0;
 }
 
 }  // namespace ixb

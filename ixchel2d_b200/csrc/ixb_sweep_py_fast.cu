@@ -1,10 +1,7 @@
-// Sweep kernel EQ_PY with the fast assembly and the partitioned Thomas-PCR solve (built with FMA contraction).
+// Assembly of sweep EQ_PY in the fast binary64 form (reciprocal tables; built with FMA contraction).
 #include "ixb_sweep.cuh"
 
 namespace ixb {
-template cudaError_t sweep_launch_solver<double, EQ_PY, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&,
-                                                                     const Geo<float>&, const SweepIO<double>&,
-                                                                     cudaStream_t);
-template cudaError_t sweep_smem_limit_solver<double, EQ_PY, IXB_SOLVER_HYBRID>(int);
-template int sweep_blocks_per_sm_solver<double, EQ_PY, IXB_SOLVER_HYBRID>(const SweepShape&);
+template cudaError_t assemble_launch<EQ_PY, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&, const Geo<float>&,
+                                                               const SweepIO<double>&, const StageBuf&, cudaStream_t);
 }  // namespace ixb

@@ -1,10 +1,7 @@
-// Sweep kernel EQ_UY with the reference-order assembly and the sequential Thomas solve (bit-identical to the reference).
+// Assembly of sweep EQ_UY in the reference's operation order (built without FMA contraction: bit-identical rows).
 #include "ixb_sweep.cuh"
 
 namespace ixb {
-template cudaError_t sweep_launch_solver<double, EQ_UY, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&,
-                                                                     const Geo<float>&, const SweepIO<double>&,
-                                                                     cudaStream_t);
-template cudaError_t sweep_smem_limit_solver<double, EQ_UY, IXB_SOLVER_EXACT>(int);
-template int sweep_blocks_per_sm_solver<double, EQ_UY, IXB_SOLVER_EXACT>(const SweepShape&);
+template cudaError_t assemble_launch<EQ_UY, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&, const Geo<float>&,
+                                                              const SweepIO<double>&, const StageBuf&, cudaStream_t);
 }  // namespace ixb
