@@ -2,11 +2,16 @@
 
 Workload: the heated lid-driven cavity in mixed convection, Re=100, Ri=1,
 Pr=0.71, on a 701x301 staggered mesh (mi=701, nj=301: 702x302 = 212,004
-p-cells) with tanh wall clustering (parameter 1.2), binary64, synthetic
-inputs built in code (no dataset involved).  A step is ITERS outer SIMPLE
-iterations (one inner pass of each equation, as conv_u/p/t are set so each
-inner loop exits after its first pass).  Metric: Mcell-iter/s (p-cells x
-outer iterations per second), whole job over all ranks.
+p-cells) with tanh wall clustering (parameter 1.2), synthetic inputs built
+in code (no dataset involved).  A step is ITERS outer SIMPLE iterations (one
+inner pass of each equation, as conv_u/p/t are set so each inner loop exits
+after its first pass).  Metric: Mcell-iter/s (p-cells x outer iterations per
+second), whole job over all ranks, of the FP32+FP64-refined form
+(IXB_PREC_FP32_REFINED: binary32 line solves, binary64 defect correction);
+the plain binary64 form is timed beside it on the same box, and both forms
+are run to a converged answer (mass residual < 1e-8) on the 64x64
+natural-convection cavity, where their hot-wall Nusselt numbers are
+compared.
 
 The working set (~45 MB) fits the 126 MB L2, so L2 is flushed (a 256 MiB
 write) before every timed step and every timed kernel launch.
@@ -44,7 +49,10 @@ PHASES = ["u-y sweep", "u-x sweep", "v-y sweep", "v-x sweep", "p'-y sweep", "p'-
 BYTES_PER_CELL = [48, 56, 48, 64, 48, 64, 72, 40, 48, 48]
 MEMSET_BYTES_PER_CELL = 8
 SWEEPS = ["u-y", "u-x", "v-y", "v-x", "p'-y", "p'-x", "T-y", "T-x"]
-KERNELS_PER_ITER = 18      # 10 phase kernels + 4 gates/controls per inner loop set + outer control
+# per outer iteration: 8 sweeps x (assembly + line solve), correction, residual,
+# 3 loop gates, 3 inner-loop controls, 1 outer-loop control
+KERNELS_PER_ITER = 25
+METRIC = "Mcell-iter/s (SIMPLE outer iteration, p-cells): FP32+FP64-refined vs FP64"
 
 
 def workload_config():
@@ -169,7 +177,7 @@ def run_reference(args):
     tot = sum(times)
     value = case.cells * sample_iters * args.steps / tot / 1e6
     line = {
-        "impl": "reference", "metric": "Mcell-iter/s (SIMPLE outer iteration, p-cells)", "value": value,
+        "impl": "reference", "metric": METRIC, "value": value,
         "unit": "Mcell-iter/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "config": workload_config(),
@@ -183,56 +191,104 @@ def run_reference(args):
         pg.destroy_process_group()
 
 
+def time_steps(sim, stream, flush, steps, warmup):
+    """Device time (ms, CUDA events on the library's stream) of `steps` steps
+    of ITERS outer iterations, L2 flushed before each step; last report."""
+    import torch
+    for _ in range(warmup):
+        sim.iterations(ITERS)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    rep = None
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+        rep = sim.iterations(ITERS)
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev), rep
+
+
+def converge(sim, stream, chunk=200, cap=40000, tol=1e-8):
+    """Iterate until the mass residual maxbo < tol; device time in ms."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    it, rep = 0, None
+    while it < cap:
+        rep = sim.iterations(chunk)
+        it += chunk
+        if rep["maxbo"] < tol:
+            break
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return it, e0.elapsed_time(e1), rep
+
+
+def make_sim(case, prec, stream, shapes):
+    from ixchel2d_b200 import Simple2D
+    sim = Simple2D.from_case(case, prec=prec)
+    sim.set_stream(stream.cuda_stream)
+    if shapes is None:
+        # launch shapes of the eight sweeps picked by the library's autotuner (cold L2)
+        shapes = {k: tuple(v) for k, v in sim.autotune(reps=5, flush_bytes=FLUSH_BYTES).items()}
+    else:
+        for k, (tl, g, *_) in shapes.items():
+            sim.set_sweep_shape(int(k), tl, g)
+    return sim, shapes
+
+
 def run_ours(args):
     import torch
     world, rank, local, pg = dist_setup(args)
     torch.cuda.set_device(local)
-    from ixchel2d_b200 import Simple2D, lib
+    from ixchel2d_b200 import Simple2D, cases, lib
+    from ixchel2d_b200 import _ffi as F
     if lib.ixb_device_count() < 1:
         raise RuntimeError("no CUDA device visible")
     case = make_case()
     stream = torch.cuda.Stream()
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    loaded = json.loads(Path(args.shapes).read_text()) if args.shapes else {}
+    modes = {"refined": F.PREC_FP32_REFINED, "fp64": F.PREC_FP64}
 
-    sim = Simple2D.from_case(case)
-    sim.set_stream(stream.cuda_stream)
-    # launch shapes of the eight sweeps picked by the library's autotuner (cold L2)
-    shapes = sim.autotune(reps=5, flush_bytes=FLUSH_BYTES)
-    # warm-up (also builds the CUDA graph)
-    for _ in range(args.warmup):
-        sim.iterations(ITERS)
-    torch.cuda.synchronize()
+    sims, shapes = {}, {}
+    for name, prec in modes.items():
+        sims[name], shapes[name] = make_sim(case, prec, stream, loaded.get(name))
+    if args.save_shapes and rank == 0:
+        Path(args.save_shapes).write_text(json.dumps({n: {str(k): list(v) for k, v in sh.items()}
+                                                      for n, sh in shapes.items()}))
 
-    # ---- device-resident timed region ----
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # ---- device-resident timed regions: the refined path (headline), then binary64 ----
     sampler = ClockSampler(local)
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
     sampler.start()
     t_wall = time.perf_counter()
-    reports = []
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(k))
-            ev[k][0].record(stream)
-        reports.append(sim.iterations(ITERS))
-        with torch.cuda.stream(stream):
-            ev[k][1].record(stream)
-    torch.cuda.synchronize()
+    ms, reports = {}, {}
+    for name in modes:
+        ms[name], reports[name] = time_steps(sims[name], stream, flush, args.steps, args.warmup)
     wall = time.perf_counter() - t_wall
     clocks = sampler.stop()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
     if pg:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        t = torch.tensor([ms["refined"], ms["fp64"]], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = {"refined": float(t[0].item()), "fp64": float(t[1].item())}
         pg.barrier()
     torch.cuda.synchronize()
     cells_iters = case.cells * ITERS * args.steps * world
-    value = cells_iters / (ms / 1e3) / 1e6
+    rate = {n: cells_iters / (ms[n] / 1e3) / 1e6 for n in modes}
+    # the two forms after the same iterations from the same start (not converged at this size)
+    nu_big = {n: sims[n].nusselt_y(2, MI - 2) for n in modes}
 
-    # ---- end to end through the C ABI with host buffers ----
+    # ---- end to end through the C ABI with host buffers (refined path) ----
+    sim = sims["refined"]
     keys = ("u", "v", "p", "T", "u_ant", "v_ant", "T_ant")
     st0 = sim.download()
     host = {}
@@ -264,17 +320,25 @@ def run_ours(args):
         e2e_ms = float(t.item())
     e2e_value = cells_iters / (e2e_ms / 1e3) / 1e6
 
-    # ---- per-kernel times (cold L2) on a scratch handle ----
-    scratch = Simple2D.from_case(case)
-    scratch.set_stream(stream.cuda_stream)
-    for k, (tl, g, _) in shapes.items():
-        scratch.set_sweep_shape(k, tl, g)
+    # ---- converged answer: the plain 64x64 configuration to maxbo < 1e-8, both forms ----
+    small = cases.natural_cavity(64, 64, Ra=1e4, T0=0.5)
+    conv = {}
+    for name, prec in modes.items():
+        s2 = Simple2D.from_case(small, prec=prec)
+        s2.set_stream(stream.cuda_stream)
+        s2.iterations(10)
+        s2.upload(small.state)
+        it, cms, rep = converge(s2, stream)
+        conv[name] = {"iters": it, "ms": cms, "maxbo": rep["maxbo"], "nu_hot_wall": s2.nusselt_x(2, 62)[0]}
+        s2.close()
+
+    # ---- per-phase times (cold L2) of the refined path on a scratch handle ----
+    scratch, _ = make_sim(case, F.PREC_FP32_REFINED, stream, shapes["refined"])
     scratch.iterations(3)
     phase_ms = scratch.time_phases(reps=10, flush_bytes=FLUSH_BYTES)
     scratch.close()
     cells = case.cells
-    per_iter_ms = [m * (1 if k != 9 else 1) for k, m in enumerate(phase_ms)]
-    dom = int(np.argmax(per_iter_ms))
+    dom = int(np.argmax(phase_ms))
     peak, peak_kind = peaks()
     alg_bytes = BYTES_PER_CELL[dom] * cells
     achieved = alg_bytes / (phase_ms[dom] / 1e3) / 1e9
@@ -283,48 +347,54 @@ def run_ours(args):
     if tf.exists():
         traffic = json.loads(tf.read_text()).get(PHASES[dom])
 
-    line = None
     if rank == 0:
         cpu_val, cpu_iters, cpu_cores, cpu_s = cpu_oracle_rate(case) if world == 1 else (None, 0, 0, 0)
         iter_bytes = (sum(BYTES_PER_CELL) + MEMSET_BYTES_PER_CELL) * cells
         line = {
-            "metric": "Mcell-iter/s (SIMPLE outer iteration, p-cells)", "value": value, "unit": "Mcell-iter/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "metric": METRIC, "value": rate["refined"], "unit": "Mcell-iter/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["refined"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic", "config": {**workload_config(), "parallelism": f"replicas{world}"},
+            "fp64": {"value": rate["fp64"], "unit": "Mcell-iter/s", "ms_per_step": ms["fp64"] / args.steps,
+                     "dtype": "f64"},
+            "refined_over_fp64": rate["refined"] / rate["fp64"],
+            "dnu_bottom_wall_after_timed_iters": abs(nu_big["refined"][0] - nu_big["fp64"][0]),
+            "converged": {"case": "natural_cavity_64x64_Ra1e4_Pr0.71", "criterion": "maxbo < 1e-8", **conv,
+                          "dnu": abs(conv["refined"]["nu_hot_wall"] - conv["fp64"]["nu_hot_wall"]),
+                          "wall_speedup": conv["fp64"]["ms"] / conv["refined"]["ms"]},
             "e2e": {"value": e2e_value, "unit": "Mcell-iter/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": h2d,
-                    "note": "per step: 7 state arrays host->device, ITERS outer iterations, 7 arrays device->host"},
+                    "note": "refined path; per step: 7 state arrays host->device, ITERS outer iterations, "
+                            "7 arrays device->host"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": PHASES[dom],
                          "peak_kind": f"{peak_kind} (copy bandwidth)",
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": phase_ms[dom]},
             "phases_ms_cold_l2": dict(zip(PHASES, phase_ms)),
-            "sweep_shapes": {SWEEPS[k]: {"lines_per_cta": tl, "threads_per_line": g, "autotune_ms": ms_}
-                             for k, (tl, g, ms_) in shapes.items()},
+            "sweep_shapes": {n: {SWEEPS[int(k)]: list(v[:2]) for k, v in sh.items()} for n, sh in shapes.items()},
             "iteration_alg_bytes": iter_bytes,
-            "iteration_gbs": iter_bytes * ITERS * args.steps / (ms / 1e3) / 1e9 / world * world,
             "cpu_baseline": None if cpu_val is None else {
                 "value": cpu_val, "unit": "Mcell-iter/s", "cores": cpu_cores, "kind": "port",
                 "sample": f"{cpu_iters} outer iterations of the same 701x301 case ({cpu_s:.1f} s)"},
-            "gpu_launches": (KERNELS_PER_ITER * ITERS + 1) * args.steps,
+            "gpu_launches": 2 * (KERNELS_PER_ITER * ITERS + 1) * args.steps,
             "clocks": clocks,
-            "last_report": {k: reports[-1][k] for k in ("maxbo", "residuo", "n_simple", "n_momen")},
+            "last_report": {k: reports["refined"][k] for k in ("maxbo", "residuo", "n_simple", "n_momen")},
             "wall_s_timed_region": wall,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
+    for s_ in sims.values():
+        s_.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
 
 
-def run_profile_phases():
+def run_profile_phases(prec):
     """Profiling driver (no timing, no JSON): the benchmark case, three outer
     iterations, then one launch of each of the ten phases in order
     (u-y, u-x, v-y, v-x, p'-y, p'-x, correction, T-y, T-x, residual)."""
     from ixchel2d_b200 import Simple2D
-    sim = Simple2D.from_case(make_case())
+    sim = Simple2D.from_case(make_case(), prec=prec)
     sim.iterations(3)
     for k in range(10):
         sim.phase(k)
@@ -339,9 +409,12 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile-phases", action="store_true",
                     help="run the profiling driver instead of the benchmark")
+    ap.add_argument("--prec", type=int, default=1, help="precision mode of --profile-phases (0 fp64, 1 refined)")
+    ap.add_argument("--shapes", help="JSON of sweep launch shapes (from --save-shapes) instead of autotuning")
+    ap.add_argument("--save-shapes", help="write the autotuned sweep launch shapes to this JSON file")
     args = ap.parse_args()
     if args.profile_phases:
-        run_profile_phases()
+        run_profile_phases(args.prec)
         return
     if args.warmup < 3:
         args.warmup = 3
