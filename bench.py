@@ -230,6 +230,57 @@ def converge(sim, stream, chunk=200, cap=40000, tol=1e-8):
     return it, e0.elapsed_time(e1), rep
 
 
+def adi_microbench(stream, n=4096, nsys=4096, reps=5):
+    """Batched line-solve microbenchmark: nsys independent tridiagonal systems
+    of n unknowns, a,c ~ U(-1,0), b = |a|+|c|+U(0.1,1), rhs ~ U(-1,1) (Philox,
+    seed 1234), contiguous (x-sweep) and interleaved (y-sweep) layouts, binary64
+    and binary32, through ixb_tridiag_f64/_f32 (hybrid solver).  Algorithmic
+    bytes: a, b, c, d read and x written once (40 B per unknown binary64, 20 B
+    binary32).  Error: max |x - x_ref| / max |x_ref| against the sequential
+    binary64 Thomas (IXB_SOLVER_EXACT) on the same inputs."""
+    import torch
+    from ixchel2d_b200 import _ffi as F
+    gen = torch.Generator(device="cuda").manual_seed(1234)
+    u = lambda lo, hi: torch.rand((nsys, n), generator=gen, device="cuda", dtype=torch.float64) * (hi - lo) + lo
+    a, c = u(-1.0, 0.0), u(-1.0, 0.0)
+    b = a.abs() + c.abs() + u(0.1, 1.0)
+    d = u(-1.0, 1.0)
+    peak, peak_kind = peaks()
+    out = {"systems": nsys, "unknowns": n, "peak_gbs": peak, "peak_kind": peak_kind}
+    sh = stream.cuda_stream
+    for layout, lname in ((0, "contiguous"), (1, "strided")):
+        lay = (lambda t: t.contiguous()) if layout == 0 else (lambda t: t.t().contiguous())
+        A, B, C, D = map(lay, (a, b, c, d))
+        ref = torch.empty_like(D)
+        with torch.cuda.stream(stream):
+            F.check(F.lib.ixb_tridiag_f64(A.data_ptr(), B.data_ptr(), C.data_ptr(), D.data_ptr(), ref.data_ptr(),
+                                          n, nsys, layout, F.SOLVER_EXACT, sh), "ixb_tridiag_f64")
+        for dt, fn, eb in ((torch.float64, F.lib.ixb_tridiag_f64, 8), (torch.float32, F.lib.ixb_tridiag_f32, 4)):
+            Ai, Bi, Ci, Di = (t.to(dt) for t in (A, B, C, D))
+            X = torch.empty_like(Di)
+            args = (Ai.data_ptr(), Bi.data_ptr(), Ci.data_ptr(), Di.data_ptr(), X.data_ptr(), n, nsys, layout,
+                    F.SOLVER_HYBRID, sh)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(stream):
+                for _ in range(2):
+                    F.check(fn(*args), "ixb_tridiag")
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):  # inputs (5 x n x nsys) exceed L2: no flush needed
+                    F.check(fn(*args), "ixb_tridiag")
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            gbs = 5 * eb * n * nsys / (ms / 1e3) / 1e9
+            err = float((X.double() - ref).abs().max() / ref.abs().max())
+            out[f"{lname}_{'f64' if eb == 8 else 'f32'}"] = {"ms": ms, "gbs": gbs, "frac": gbs / peak,
+                                                             "max_err_vs_f64_thomas": err}
+            del Ai, Bi, Ci, Di, X
+        del A, B, C, D, ref
+    torch.cuda.empty_cache()
+    return out
+
+
 def make_sim(case, prec, stream, shapes):
     from ixchel2d_b200 import Simple2D
     sim = Simple2D.from_case(case, prec=prec)
@@ -332,6 +383,9 @@ def run_ours(args):
         conv[name] = {"iters": it, "ms": cms, "maxbo": rep["maxbo"], "nu_hot_wall": s2.nusselt_x(2, 62)[0]}
         s2.close()
 
+    # ---- batched line-solve microbenchmark (4096 systems x 4096 unknowns) ----
+    adi = adi_microbench(stream)
+
     # ---- per-phase times (cold L2) of the refined path on a scratch handle ----
     scratch, _ = make_sim(case, F.PREC_FP32_REFINED, stream, shapes["refined"])
     scratch.iterations(3)
@@ -371,6 +425,7 @@ def run_ours(args):
                          "peak_kind": f"{peak_kind} (copy bandwidth)",
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": phase_ms[dom]},
             "phases_ms_cold_l2": dict(zip(PHASES, phase_ms)),
+            "adi_line_solve": adi,
             "sweep_shapes": {n: {SWEEPS[int(k)]: list(v[:2]) for k, v in sh.items()} for n, sh in shapes.items()},
             "iteration_alg_bytes": iter_bytes,
             "cpu_baseline": None if cpu_val is None else {

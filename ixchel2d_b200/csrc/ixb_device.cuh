@@ -601,6 +601,48 @@ __device__ void thomas_pcr_warp(R* sa, R* sb, R* sc, R* sd, int m, int mp) {
 }
 
 
+// Reduced system of a partitioned line solve: the first and last rows of G
+// chunks, each with unit diagonal, coupled to the neighbouring chunks' end
+// rows (row 2k: eA x_{2k-1} + x_{2k} + eC x_{2k+1} = eD; row 2k+1 likewise
+// with oA, oC, oD).  Solved by parallel cyclic reduction over log2(2G) steps
+// in shared memory `red` (12 G elements, two buffers of a | c | d); thread
+// k supplies rows 2k, 2k+1 and receives their solutions x0, xl.  Called by
+// all threads of the CTA (it holds barriers); `active` false: barriers only.
+template <class R, int G>
+__device__ __forceinline__ void reduced_pcr(R* red, int k, bool active, R eA, R eC, R eD, R oA, R oC, R oD, R& x0,
+                                            R& xl) {
+  R* cur = red;
+  R* nxt = red + 6 * G;
+  if (active) {
+    cur[2 * k] = eA; cur[2 * G + 2 * k] = eC; cur[4 * G + 2 * k] = eD;
+    cur[2 * k + 1] = oA; cur[2 * G + 2 * k + 1] = oC; cur[4 * G + 2 * k + 1] = oD;
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 1; s < 2 * G; s <<= 1) {
+    if (active) {
+      const R* Ac = cur; const R* Cc = cur + 2 * G; const R* Dc = cur + 4 * G;
+      R* An = nxt; R* Cn = nxt + 2 * G; R* Dn = nxt + 4 * G;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int i = k + q * G;
+        const R ai = Ac[i], ci = Cc[i], di = Dc[i];
+        R alo = R(0), clo = R(0), dlo = R(0), ahi = R(0), chi = R(0), dhi = R(0);
+        if (i - s >= 0) { alo = Ac[i - s]; clo = Cc[i - s]; dlo = Dc[i - s]; }
+        if (i + s < 2 * G) { ahi = Ac[i + s]; chi = Cc[i + s]; dhi = Dc[i + s]; }
+        const R r = fast_rcp(fmaT(-ci, ahi, fmaT(-ai, clo, R(1))));
+        An[i] = -ai * alo * r;
+        Cn[i] = -ci * chi * r;
+        Dn[i] = fmaT(-ci, dhi, fmaT(-ai, dlo, di)) * r;
+      }
+    }
+    __syncthreads();
+    R* t = cur; cur = nxt; nxt = t;
+  }
+  x0 = cur[4 * G + 2 * k];
+  xl = cur[4 * G + 2 * k + 1];
+}
+
 // Partitioned line solve of the TL lines staged in shared memory, G threads
 // per line (thread t: line t / G, chunk k = t % G, rows k*m .. k*m+m-1 at
 // offset k*mp of the line's row arrays).  Every thread eliminates its chunk
@@ -655,37 +697,7 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
   }
   R x0, xl;
   if (rs == RS_PCR) {
-    // two buffers of the 2G rows (a | c | d), swapped every step
-    R* cur = red;
-    R* nxt = red + 6 * G;
-    if (active) {
-      cur[2 * k] = eA; cur[2 * G + 2 * k] = eC; cur[4 * G + 2 * k] = eD;
-      cur[2 * k + 1] = oA; cur[2 * G + 2 * k + 1] = oC; cur[4 * G + 2 * k + 1] = oD;
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int s = 1; s < 2 * G; s <<= 1) {
-      if (active) {
-        const R* Ac = cur; const R* Cc = cur + 2 * G; const R* Dc = cur + 4 * G;
-        R* An = nxt; R* Cn = nxt + 2 * G; R* Dn = nxt + 4 * G;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int i = k + q * G;
-          const R ai = Ac[i], ci = Cc[i], di = Dc[i];
-          R alo = R(0), clo = R(0), dlo = R(0), ahi = R(0), chi = R(0), dhi = R(0);
-          if (i - s >= 0) { alo = Ac[i - s]; clo = Cc[i - s]; dlo = Dc[i - s]; }
-          if (i + s < 2 * G) { ahi = Ac[i + s]; chi = Cc[i + s]; dhi = Dc[i + s]; }
-          const R r = fast_rcp(fmaT(-ci, ahi, fmaT(-ai, clo, R(1))));
-          An[i] = -ai * alo * r;
-          Cn[i] = -ci * chi * r;
-          Dn[i] = fmaT(-ci, dhi, fmaT(-ai, dlo, di)) * r;
-        }
-      }
-      __syncthreads();
-      R* t = cur; cur = nxt; nxt = t;
-    }
-    x0 = cur[4 * G + 2 * k];
-    xl = cur[4 * G + 2 * k + 1];
+    reduced_pcr<R, G>(red, k, active, eA, eC, eD, oA, oC, oD, x0, xl);
   } else {
     // reduced system in the warp solver's [32][M2P] chunk layout
     constexpr int ARR2 = 32 * M2P;

@@ -121,6 +121,216 @@ __global__ void __launch_bounds__(128) tri_inter_kernel(const R* __restrict__ a,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Streamed contiguous solve (hybrid solver): a persistent CTA of 256 threads
+// per SM slot walks its systems; while it solves system s from registers,
+// the bulk-copy engine is already loading system s+grid into shared memory,
+// and the solution leaves through a bulk shared->global copy.  Thread t owns
+// rows t*M .. t*M+M-1 (M odd, so the 32 threads of a warp reading their own
+// row j hit 32 different banks); it eliminates them in registers down to two
+// rows (modified Thomas), the 512 reduced rows are solved by PCR in shared
+// memory, and each thread back-substitutes its rows.  Every wait on the copy
+// engine is bounded: on a timeout the CTA records it in g_tri_timeout, waits
+// (bounded) for its copies still in flight and leaves without writing.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kStreamT = 256;       // threads per CTA (one system at a time)
+constexpr int kSpinLimit = 1 << 22;  // bounded mbarrier polls (a hang guard)
+__device__ int g_tri_timeout = 0;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_store_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_store_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  for (int i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Shared memory of the streamed kernel: 4 row arrays of NP = 256*M
+// elements (the copy target), the solution buffer (NP), the PCR buffers
+// (12*256) and the mbarrier.
+template <class R, int M>
+__host__ __device__ constexpr size_t stream_smem_bytes() {
+  return ((size_t)5 * kStreamT * M + 12 * kStreamT) * sizeof(R) + 16;
+}
+
+template <class R, int M>
+__global__ void __launch_bounds__(kStreamT, 1) tri_stream_kernel(const R* __restrict__ a, const R* __restrict__ b,
+                                                                 const R* __restrict__ c, const R* __restrict__ d,
+                                                                 R* __restrict__ x, int n, int nsys) {
+  constexpr int NP = kStreamT * M;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* buf = reinterpret_cast<R*>(smem_raw);  // a | b | c | d, NP each
+  R* xbuf = buf + 4 * NP;
+  R* red = xbuf + NP;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + 12 * kStreamT);
+  const int tid = threadIdx.x;
+  const unsigned bytes = (unsigned)n * sizeof(R);
+  // identity rows pad every system to NP rows; the copies never touch them
+  for (int r = n + tid; r < NP; r += kStreamT) {
+    buf[r] = R(0); buf[NP + r] = R(1); buf[2 * NP + r] = R(0); buf[3 * NP + r] = R(0);
+  }
+  if (tid == 0) mbar_init(bar);
+  __syncthreads();
+  auto issue = [&](int s) {
+    const size_t off = (size_t)s * n;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of buf precede the copies
+    mbar_expect_tx(bar, 4 * bytes);
+    bulk_load(buf, a + off, bytes, bar);
+    bulk_load(buf + NP, b + off, bytes, bar);
+    bulk_load(buf + 2 * NP, c + off, bytes, bar);
+    bulk_load(buf + 3 * NP, d + off, bytes, bar);
+  };
+  if (tid == 0 && blockIdx.x < nsys) issue(blockIdx.x);
+  unsigned parity = 0;
+  bool failed = false;
+  for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
+    const bool ok = mbar_wait_bounded(bar, parity);
+    if (__syncthreads_or(!ok)) { failed = true; break; }
+    parity ^= 1;
+    // own rows into registers (row 0 has no a, row n-1 no c)
+    R ra[M], rb[M], rc[M], rd[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = tid * M + j;
+      ra[j] = r == 0 ? R(0) : buf[r];
+      rb[j] = buf[NP + r];
+      rc[j] = r == n - 1 ? R(0) : buf[2 * NP + r];
+      rd[j] = buf[3 * NP + r];
+    }
+    __syncthreads();  // the row buffers are free: start loading the next system
+    if (tid == 0 && s + (int)gridDim.x < nsys) issue(s + gridDim.x);
+    // modified Thomas on the own rows: x_j + a'_j x_0 + c'_j x_{j+1} = d'_j ...
+    R inv = fast_rcp(rb[1]);
+    R ap = ra[1] * inv, cp = rc[1] * inv, dp = rd[1] * inv;
+    ra[1] = ap; rc[1] = cp; rd[1] = dp;
+#pragma unroll
+    for (int j = 2; j < M; ++j) {
+      const R aj = ra[j];
+      const R r = fast_rcp(fmaT(-aj, cp, rb[j]));
+      ap = -aj * ap * r;
+      dp = fmaT(-aj, dp, rd[j]) * r;
+      cp = rc[j] * r;
+      ra[j] = ap; rc[j] = cp; rd[j] = dp;
+    }
+    // ... then x_j + a''_j x_0 + c''_j x_{M-1} = d''_j for j = 1..M-2
+    R an = ra[M - 2], cn = rc[M - 2], dn = rd[M - 2];
+#pragma unroll
+    for (int j = M - 3; j >= 1; --j) {
+      const R cj = rc[j];
+      dn = fmaT(-cj, dn, rd[j]);
+      an = fmaT(-cj, an, ra[j]);
+      cn = -cj * cn;
+      ra[j] = an; rc[j] = cn; rd[j] = dn;
+    }
+    const R r0 = fast_rcp(fmaT(-rc[0], an, rb[0]));
+    const R eA = ra[0] * r0, eC = -rc[0] * cn * r0, eD = fmaT(-rc[0], dn, rd[0]) * r0;
+    R x0, xl;
+    reduced_pcr<R, kStreamT>(red, tid, true, eA, eC, eD, ap, cp, dp, x0, xl);
+    // the previous solution must have left xbuf before it is overwritten
+    if (tid == 0) bulk_store_wait_read();
+    __syncthreads();
+    xbuf[tid * M] = x0;
+#pragma unroll
+    for (int j = 1; j < M - 1; ++j) xbuf[tid * M + j] = fmaT(-rc[j], xl, fmaT(-ra[j], x0, rd[j]));
+    xbuf[tid * M + M - 1] = xl;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> copy engine
+    __syncthreads();
+    if (tid == 0) bulk_store(x + (size_t)s * n, xbuf, bytes);
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicExch(&g_tri_timeout, 1);
+      mbar_wait_bounded(bar, parity);  // copies still in flight land before the CTA leaves
+    }
+  }
+  if (tid == 0) bulk_store_wait_all();
+}
+
+template <class R, int M>
+cudaError_t stream_launch(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
+  auto k = tri_stream_kernel<R, M>;
+  const size_t smem = stream_smem_bytes<R, M>();
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, nsm = 0, per_sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kStreamT, smem)) != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidValue;
+  const int grid = std::min(nsys, nsm * per_sm);
+  k<<<grid, kStreamT, smem, st>>>(a, b, c, d, x, n, nsys);
+  return cudaGetLastError();
+}
+
+// The streamed kernel applies when the copies are legal (16-byte aligned
+// system starts and sizes) and the rows fit one CTA: n <= 256*M for an odd
+// M <= 19 whose buffers fit the shared memory.
+template <class R>
+bool stream_fits(const R* a, const R* b, const R* c, const R* d, const R* x, int n) {
+  const uintptr_t all = (uintptr_t)a | (uintptr_t)b | (uintptr_t)c | (uintptr_t)d | (uintptr_t)x;
+  if ((all & 15) != 0 || ((size_t)n * sizeof(R)) % 16 != 0) return false;
+  return n >= 3 * kStreamT / 2 && n <= kStreamT * 19;
+}
+
+template <class R>
+cudaError_t stream_solve(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
+  int m = (n + kStreamT - 1) / kStreamT;
+  m |= 1;
+  if (m < 3) m = 3;
+  switch (m) {
+    case 3: return stream_launch<R, 3>(a, b, c, d, x, n, nsys, st);
+    case 5: return stream_launch<R, 5>(a, b, c, d, x, n, nsys, st);
+    case 7: return stream_launch<R, 7>(a, b, c, d, x, n, nsys, st);
+    case 9: return stream_launch<R, 9>(a, b, c, d, x, n, nsys, st);
+    case 11: return stream_launch<R, 11>(a, b, c, d, x, n, nsys, st);
+    case 13: return stream_launch<R, 13>(a, b, c, d, x, n, nsys, st);
+    case 15: return stream_launch<R, 15>(a, b, c, d, x, n, nsys, st);
+    case 17: return stream_launch<R, 17>(a, b, c, d, x, n, nsys, st);
+    case 19: return stream_launch<R, 19>(a, b, c, d, x, n, nsys, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
 template <class R, int SOLVER, int TL>
 static cudaError_t contig_tl(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, int m, int mp,
                              size_t smem, cudaStream_t st) {
@@ -136,6 +346,10 @@ template <class R, int SOLVER>
 static cudaError_t tridiag_impl(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, int layout,
                                 cudaStream_t st) {
   if (layout == 0) {
+    if (SOLVER == IXB_SOLVER_HYBRID && stream_fits(a, b, c, d, x, n)) {
+      const cudaError_t e = stream_solve(a, b, c, d, x, n, nsys, st);
+      if (e != cudaErrorInvalidValue) return e;  // otherwise: does not fit this GPU, use the staged kernel
+    }
     int g = 32;
     while (g < 256 && 3 * g < n) g <<= 1;
     const int tl = 256 / g;
