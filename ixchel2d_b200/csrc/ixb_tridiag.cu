@@ -13,6 +13,7 @@
 // its modified diagonal (exact) or normalised super-diagonal (hybrid) in a
 // scratch array of n*nsys elements taken from the stream-ordered allocator,
 // and the modified right-hand side in x.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,7 +27,7 @@ template <class R, int SOLVER, int TL, int G>
 __global__ void __launch_bounds__(TL * G) tri_contig_kernel(const R* __restrict__ a, const R* __restrict__ b,
                                                             const R* __restrict__ c, const R* __restrict__ d,
                                                             R* x, int n, int nsys, int m, int mp) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
   const int npad = G * m;
   const size_t LS = line_smem_elems(G, mp), arr = (size_t)G * mp;
@@ -331,6 +332,181 @@ cudaError_t stream_solve(const R* a, const R* b, const R* c, const R* d, R* x, i
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Interleaved systems (row i of system s at i*nsys + s), hybrid solver: a
+// thread-block cluster of Q CTAs solves W adjacent systems at a time, CTA q
+// holding rows q*R .. q*R+R-1 (R = (T/W)*M) of all W systems.  Thread t owns
+// rows k*M .. k*M+M-1 (k = t / W) of system w = t % W, so a warp's loads and
+// stores cover 32/W rows of W adjacent systems: whole 32-byte sectors.  Each
+// thread eliminates its rows in registers (modified Thomas) to two rows; the
+// 2*Q*(T/W) reduced rows of system w are gathered in the shared memory of
+// cluster rank w (distributed shared memory) and solved there by PCR; every
+// thread reads its two solutions back and back-substitutes.  The reduced
+// rows are double-buffered across system groups, so a group costs two
+// cluster barriers.  No bulk copies: plain coalesced loads from registers of
+// several resident clusters per SM keep the memory system busy.
+// ---------------------------------------------------------------------------
+namespace {
+
+namespace cg = cooperative_groups;
+
+template <int W, int T, int M>
+struct StridedShape {
+  static constexpr int C = T / W;  // chunks per CTA per system
+  static constexpr int R = C * M;  // rows per CTA
+};
+
+// reduced-row buffers of one CTA: 2 sets x (a | c | d) x 2 PCR buffers x NR
+template <class R>
+__host__ __device__ constexpr size_t strided_smem_bytes(int nr) {
+  return (size_t)2 * 6 * nr * sizeof(R);
+}
+
+template <class R, int W, int T, int M>
+__global__ void __launch_bounds__(T) tri_strided_kernel(const R* __restrict__ a, const R* __restrict__ b,
+                                                        const R* __restrict__ c, const R* __restrict__ d,
+                                                        R* __restrict__ x, int n, int nsys) {
+  using SS = StridedShape<W, T, M>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* sm = reinterpret_cast<R*>(smem_raw);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int Q = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int NR = 2 * Q * SS::C;  // reduced rows per system
+  const int tid = threadIdx.x;
+  const int w = tid % W, k = tid / W;
+  const int row0 = rank * SS::R + k * M;
+  const int nclusters = gridDim.x / Q;
+  const int cl = blockIdx.x / Q;
+  const int ngroups = (nsys + W - 1) / W;
+  int steps = 0;
+  for (int s_ = 1; s_ < NR; s_ <<= 1) ++steps;
+  int set = 0;
+  for (int g = cl; g < ngroups; g += nclusters, set ^= 1) {
+    const int sys = g * W + w;
+    const bool live = sys < nsys;
+    R ra[M], rb[M], rc[M], rd[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = row0 + j;
+      const bool in = live && r < n;
+      const size_t o = (size_t)(in ? r : 0) * nsys + (live ? sys : 0);
+      ra[j] = (in && r > 0) ? __ldg(a + o) : R(0);
+      rb[j] = in ? __ldg(b + o) : R(1);
+      rc[j] = (in && r < n - 1) ? __ldg(c + o) : R(0);
+      rd[j] = in ? __ldg(d + o) : R(0);
+    }
+    // modified Thomas on the own rows (as in the contiguous kernels)
+    R inv = fast_rcp(rb[1]);
+    R ap = ra[1] * inv, cp = rc[1] * inv, dp = rd[1] * inv;
+    ra[1] = ap; rc[1] = cp; rd[1] = dp;
+#pragma unroll
+    for (int j = 2; j < M; ++j) {
+      const R aj = ra[j];
+      const R r = fast_rcp(fmaT(-aj, cp, rb[j]));
+      ap = -aj * ap * r;
+      dp = fmaT(-aj, dp, rd[j]) * r;
+      cp = rc[j] * r;
+      ra[j] = ap; rc[j] = cp; rd[j] = dp;
+    }
+    R an = ra[M - 2], cn = rc[M - 2], dn = rd[M - 2];
+#pragma unroll
+    for (int j = M - 3; j >= 1; --j) {
+      const R cj = rc[j];
+      dn = fmaT(-cj, dn, rd[j]);
+      an = fmaT(-cj, an, ra[j]);
+      cn = -cj * cn;
+      ra[j] = an; rc[j] = cn; rd[j] = dn;
+    }
+    const R r0 = fast_rcp(fmaT(-rc[0], an, rb[0]));
+    const R eA = ra[0] * r0, eC = -rc[0] * cn * r0, eD = fmaT(-rc[0], dn, rd[0]) * r0;
+    // reduced rows 2i, 2i+1 (i = rank*C + k) of system w -> shared memory of rank w
+    R* base = sm + (size_t)set * 6 * NR;  // this set: buffer 0 = a | c | d, buffer 1 = a | c | d
+    {
+      R* dst = cluster.map_shared_rank(base, w % Q);
+      const int i = 2 * (rank * SS::C + k);
+      dst[i] = eA; dst[NR + i] = eC; dst[2 * NR + i] = eD;
+      dst[i + 1] = ap; dst[NR + i + 1] = cp; dst[2 * NR + i + 1] = dp;
+    }
+    cluster.sync();
+    if (rank < W) {  // owner of system `rank` of this group: PCR on its NR rows
+      R* cur = base;
+      R* nxt = base + 3 * NR;
+      for (int s_ = 1; s_ < NR; s_ <<= 1) {
+        for (int i = tid; i < NR; i += T) {
+          const R ai = cur[i], ci = cur[NR + i], di = cur[2 * NR + i];
+          R alo = R(0), clo = R(0), dlo = R(0), ahi = R(0), chi = R(0), dhi = R(0);
+          if (i - s_ >= 0) { alo = cur[i - s_]; clo = cur[NR + i - s_]; dlo = cur[2 * NR + i - s_]; }
+          if (i + s_ < NR) { ahi = cur[i + s_]; chi = cur[NR + i + s_]; dhi = cur[2 * NR + i + s_]; }
+          const R rr = fast_rcp(fmaT(-ci, ahi, fmaT(-ai, clo, R(1))));
+          nxt[i] = -ai * alo * rr;
+          nxt[NR + i] = -ci * chi * rr;
+          nxt[2 * NR + i] = fmaT(-ci, dhi, fmaT(-ai, dlo, di)) * rr;
+        }
+        __syncthreads();
+        R* t = cur; cur = nxt; nxt = t;
+      }
+    }
+    cluster.sync();
+    // solutions of the own reduced rows, from rank w (final PCR buffer)
+    const R* sol = cluster.map_shared_rank(base + ((steps & 1) ? 3 * NR : 0) + 2 * NR, w % Q);
+    const int i = 2 * (rank * SS::C + k);
+    const R x0 = sol[i], xl = sol[i + 1];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = row0 + j;
+      if (live && r < n) {
+        const R xv = j == 0 ? x0 : (j == M - 1 ? xl : fmaT(-rc[j], xl, fmaT(-ra[j], x0, rd[j])));
+        x[(size_t)r * nsys + sys] = xv;
+      }
+    }
+  }
+  cluster.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+template <class R, int W, int T, int M>
+cudaError_t strided_launch(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
+  using SS = StridedShape<W, T, M>;
+  const int Q = (n + SS::R - 1) / SS::R;
+  if (Q < W || Q > 8) return cudaErrorInvalidValue;  // one owner CTA per system of a group
+  const int nr = 2 * Q * SS::C;
+  const size_t smem = strided_smem_bytes<R>(nr);
+  auto k = tri_strided_kernel<R, W, T, M>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = Q;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(Q);
+  int max_clusters = 0;
+  if ((e = cudaOccupancyMaxActiveClusters(&max_clusters, k, &cfg)) != cudaSuccess) return e;
+  if (max_clusters < 1) return cudaErrorInvalidValue;
+  const int ngroups = (nsys + W - 1) / W;
+  cfg.gridDim = dim3(Q * std::min(ngroups, max_clusters));
+  e = cudaLaunchKernelEx(&cfg, k, a, b, c, d, x, n, nsys);
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+// binary64: 4 systems (one 32-byte sector per row) x 32 chunks of 16 rows
+// per CTA of 128 threads; binary32: 8 systems x 32 chunks of 16 rows per
+// CTA of 256 threads.  Both cover up to 8 x 512 = 4096 rows per system.
+template <class R>
+cudaError_t strided_solve(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
+  if constexpr (sizeof(R) == 8) return strided_launch<R, 4, 128, 16>(a, b, c, d, x, n, nsys, st);
+  else return strided_launch<R, 8, 256, 16>(a, b, c, d, x, n, nsys, st);
+}
+
+}  // namespace
+
 template <class R, int SOLVER, int TL>
 static cudaError_t contig_tl(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, int m, int mp,
                              size_t smem, cudaStream_t st) {
@@ -366,6 +542,10 @@ static cudaError_t tridiag_impl(const R* a, const R* b, const R* c, const R* d, 
       case 4: return contig_tl<R, SOLVER, 4>(a, b, c, d, x, n, nsys, m, mp, smem, st);
       default: return contig_tl<R, SOLVER, 8>(a, b, c, d, x, n, nsys, m, mp, smem, st);
     }
+  }
+  if (SOLVER == IXB_SOLVER_HYBRID) {
+    const cudaError_t es = strided_solve(a, b, c, d, x, n, nsys, st);
+    if (es != cudaErrorInvalidValue) return es;  // otherwise: size outside the cluster kernel's range
   }
   R* work = nullptr;
   cudaError_t e = cudaMallocAsync((void**)&work, (size_t)n * nsys * sizeof(R), st);
