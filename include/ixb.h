@@ -226,6 +226,40 @@ int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float*
 int ixb_tridiag_f64_noalloc(const double* a, const double* b, const double* c, const double* d, double* x, int n,
                             int nsys, int layout, int solver, void* stream);
 
+/* ---- batched cavities: many instances, one launch per phase ----
+ * No counterpart in the reference, which runs one case per process.  A
+ * batch owns `count` instances of sizes mi[i] x nj[i] (4..1024 each), all in
+ * the same precision mode.  Each instance is an ordinary handle: set its
+ * mesh, parameters, boundary tables, sources and state, and read its state
+ * and Nusselt numbers, through the single-instance calls on the handle
+ * ixb_batch_instance returns (the batch owns it: do not destroy it).  One
+ * outer iteration of the batch runs every phase of the SIMPLE iteration as
+ * one launch over the work of all active instances, with one pass of each
+ * equation (the reference's loops with iter_ecuaci_max = 0); the loop is a
+ * single CUDA graph.  An instance stops when its outer test (main.f90:1202:
+ * maxbo < conv_paso and residuo < conv_resi) holds or a norm is not finite. */
+typedef struct ixb_batch ixb_batch;
+int ixb_batch_create(int count, const int* mi, const int* nj, int prec_mode, ixb_batch** out);
+int ixb_batch_destroy(ixb_batch* b);
+int ixb_batch_instance(ixb_batch* b, int i, ixb_handle** h);
+/* Launch shape of sweep `sweep` (IXB_SWEEP_* order) for every instance, as
+ * ixb_set_sweep_shape; 0, 0 restores the default. */
+int ixb_batch_set_sweep_shape(ixb_batch* b, int sweep, int lines_per_cta, int threads_per_line);
+/* Time the seven launch shapes of every sweep on the batch (reps batched
+ * iterations each) and keep the fastest; chosen[2*s], chosen[2*s+1] and
+ * ms[s] (may be null) receive the choice and its time per sweep.  The state
+ * of every instance is saved before and restored after. */
+int ixb_batch_autotune(ixb_batch* b, int reps, int* chosen, double* ms);
+/* Mark every instance active again with its counters cleared. */
+int ixb_batch_restart(ixb_batch* b);
+/* Run up to max_iters outer iterations of the active instances; *n_active
+ * receives how many are still active afterwards. */
+int ixb_batch_iterate(ixb_batch* b, int max_iters, int* n_active);
+/* Instance i after the last ixb_batch_iterate: norms, iterations done since
+ * the last restart (n_simple), exit_code 0 running, 1 converged, 2 stopped
+ * by the iteration budget, 3 non-finite norm (status IXB_ENONFINITE). */
+int ixb_batch_report(ixb_batch* b, int i, ixb_report* out);
+
 /* ---- host-side inputs (no GPU needed) ---- */
 /* lectura_cond_frontera index rule (source/mod_cond_frontera.f90:114-238):
  * for side 0/2 ('a'/'c') the divisions are located on `yy` (nn entries), for

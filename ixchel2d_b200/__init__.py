@@ -8,7 +8,7 @@ library raises ImportError (there is no CPU fallback).
 """
 import importlib
 
-__all__ = ["ffi", "lib", "IxbError", "Simple2D", "cases"]
+__all__ = ["ffi", "lib", "IxbError", "Simple2D", "Batch", "cases"]
 
 
 def __getattr__(name):
@@ -18,6 +18,8 @@ def __getattr__(name):
         return getattr(importlib.import_module("._ffi", __name__), name)
     if name == "Simple2D":
         return importlib.import_module(".simple", __name__).Simple2D
+    if name == "Batch":
+        return importlib.import_module(".batch", __name__).Batch
     if name == "cases":
         return importlib.import_module(".cases", __name__)
     raise AttributeError(name)

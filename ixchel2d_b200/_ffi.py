@@ -89,6 +89,14 @@ SIGNATURES = [
     ("ixb_tridiag_f64", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     ("ixb_tridiag_f32", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     ("ixb_tridiag_f64_noalloc", C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
+    ("ixb_batch_create", C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.POINTER(_vp)]),
+    ("ixb_batch_destroy", C.c_int, [_vp]),
+    ("ixb_batch_instance", C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    ("ixb_batch_set_sweep_shape", C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+    ("ixb_batch_autotune", C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("ixb_batch_restart", C.c_int, [_vp]),
+    ("ixb_batch_iterate", C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
+    ("ixb_batch_report", C.c_int, [_vp, C.c_int, C.POINTER(Report)]),
     ("ixb_bc_locate", C.c_int, [C.c_int, C.c_int, _dp, C.POINTER(C.c_int), _dp, _dp, C.c_int, _dp, C.c_int,
                                 C.POINTER(BCSide)]),
     ("ixb_read_bc_file", C.c_int, [C.c_char_p, _dp, C.c_int, _dp, C.c_int, C.POINTER(BCSide)]),

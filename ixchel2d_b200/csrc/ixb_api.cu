@@ -17,26 +17,11 @@
 #include <new>
 #include <vector>
 
-#include "ixb_internal.h"
+#include "ixb_handle.h"
 
 using namespace ixb;
 
 namespace {
-
-// device-side loop state for the graph-driven SIMPLE loop
-struct Ctl {
-  // inputs
-  double conv_u, conv_p, conv_t, conv_resi, conv_paso;
-  int iter_ecuaci_max, iter_simple_max;
-  int fixed_count;   // >0: run exactly this many outer passes, no outer test
-  // state
-  int iter_ecuaci, iter_simple;
-  int outer_done;    // passes done in this launch
-  int inner_done;    // passes of the current inner loop (hard cap: iter_ecuaci_max + 2)
-  int exit_code, status;
-  long long n_simple, n_momen, n_pres, n_ener;
-  double err_u, err_p, err_t, maxbo, residuo;
-};
 
 #define CK(x)                                    \
   do {                                           \
@@ -49,57 +34,6 @@ struct Ctl {
 
 }  // namespace
 
-struct ixb_handle {
-  int mi = 0, nj = 0, LD = 0, rows = 0, prec = 0;
-  size_t fsz = 0;  // elements per field buffer
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  cudaError_t last_cuda = cudaSuccess;
-  // fields (binary64)
-  double *u[2] = {}, *v[2] = {}, *T[2] = {}, *pc[2] = {};
-  double *p = nullptr, *u_ant = nullptr, *v_ant = nullptr, *T_ant = nullptr;
-  double *au = nullptr, *av = nullptr, *b_o = nullptr, *resu = nullptr;
-  double *fcon[3] = {}, *flin[3] = {};
-  double* zero = nullptr;  // a field of zeros: the sources of an equation without any
-  // rows of one sweep staged between its assembly and its line solve
-  void* stage = nullptr;
-  size_t stage_stride = 0;  // elements per row array
-  int stage_P = 0;          // row pitch of a line
-  int cu = 0, cv = 0, cT = 0, cpc = 0;
-  // mesh
-  double* metrics = nullptr;
-  int mstride = 0;
-  double* tables = nullptr;  // T_COUNT mesh-constant 2-D tables
-  float* metrics32 = nullptr;  // binary32 copies (IXB_PREC_FP32_REFINED)
-  float* tables32 = nullptr;
-  bool tables_dirty = true;
-  double *xp_d = nullptr, *yp_d = nullptr;
-  std::vector<double> xu, yv, xp, yp;
-  // boundary tables [var][side][line]
-  BCEntry* bc = nullptr;
-  int bcstride = 0;
-  // reductions
-  double* partials = nullptr;
-  unsigned int* counters = nullptr;
-  double* norms = nullptr;
-  int pstride = 0;
-  double* h_norms = nullptr;  // pinned
-  double* nu_d = nullptr;
-  // control for graphs
-  Ctl* ctl_d = nullptr;
-  Ctl* ctl_h = nullptr;  // pinned
-  cudaGraphExec_t graph_exec = nullptr;
-  cudaGraph_t graph = nullptr;
-  bool graph_dirty = true;
-  // params and flags
-  ixb_params prm{};
-  bool has_mesh = false, has_params = false, has_bc[3] = {false, false, false};
-  int iter_ecuaci = 0, iter_simple = 0;
-  int use_graph = 1;
-  int shape_tl[EQ_COUNT] = {};  // launch shape per sweep (0 = not chosen yet)
-  int shape_g[EQ_COUNT] = {};
-  int nsm = 148;
-};
 
 namespace {
 
@@ -184,11 +118,9 @@ void pick_shape(ixb_handle* h, int eq) {
   h->shape_g[eq] = kShapes[best][1];
 }
 
-// Launch one sweep reading field buffers `cur` and writing `cur^1`.
-int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
-  Geo<double> G = make_geo(h);
-  if (h->shape_tl[eq] == 0) pick_shape(h, eq);
-  SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), h->shape_tl[eq], h->shape_g[eq]);
+// Inputs and outputs of sweep `eq` at the handle's current buffer parity;
+// flips the parity of the swept field (its output becomes current).
+SweepIO<double> sweep_io(ixb_handle* h, int eq, const double* prev, bool with_norm) {
   SweepIO<double> io{};
   io.u = h->u[h->cu]; io.v = h->v[h->cv]; io.T = h->T[h->cT]; io.p = h->p; io.pc = h->pc[h->cpc];
   io.u_ant = h->u_ant; io.v_ant = h->v_ant; io.T_ant = h->T_ant;
@@ -222,10 +154,19 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
     if (eq == EQ_PX) { io.nrm0 = slot(h, N_DP); io.nrm1 = slot(h, N_BO); }
     if (eq == EQ_TX) io.nrm0 = slot(h, N_DT);
   }
+  *cur ^= 1;
+  return io;
+}
+
+// Launch one sweep reading field buffers `cur` and writing `cur^1`.
+int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
+  Geo<double> G = make_geo(h);
+  if (h->shape_tl[eq] == 0) pick_shape(h, eq);
+  SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), h->shape_tl[eq], h->shape_g[eq]);
+  const SweepIO<double> io = sweep_io(h, eq, prev, with_norm);
   const Geo<float> Gf = h->metrics32 ? make_geo32(h) : Geo<float>{};
   const StageBuf stage{h->stage, h->stage_stride, h->stage_P};
   CK(launch_sweep_f64(eq, solver_form(h), s, G, Gf, io, stage, h->stream));
-  *cur ^= 1;
   return IXB_OK;
 }
 
@@ -1088,3 +1029,12 @@ int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float*
 }
 
 }  // extern "C"
+
+namespace ixb {
+Geo<double> handle_geo(const ixb_handle* h) { return make_geo(h); }
+Geo<float> handle_geo32(const ixb_handle* h) { return h->metrics32 ? make_geo32(h) : Geo<float>{}; }
+int handle_solver_form(const ixb_handle* h) { return solver_form(h); }
+int handle_ready(ixb_handle* h) { return ready(h); }
+SweepIO<double> handle_sweep_io(ixb_handle* h, int eq, const double* prev) { return sweep_io(h, eq, prev, false); }
+int handle_real_bytes(const ixb_handle* h) { return real_bytes(h); }
+}  // namespace ixb

@@ -52,6 +52,12 @@ struct BCEntry {  // effective boundary row of one line (last covering segment w
   int pad;
 };
 
+struct BatchNorm {          // per-instance norms of a batched launch
+  double* partials;         // one per work item of the launch (null: no norm)
+  unsigned int* counter;    // one per instance
+  double* result;           // one per instance
+};
+
 struct NormSlot {        // deterministic two-level sum of squares
   double* partials;      // one per CTA
   unsigned int* counter; // CTAs finished (reset by the last one)

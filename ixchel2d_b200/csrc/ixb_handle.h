@@ -1,0 +1,91 @@
+// ixb_handle.h -- the handle behind the C ABI (one SIMPLE instance on one
+// CUDA stream), shared by the single-instance driver (ixb_api.cu) and the
+// batched driver (ixb_batch.cu).  Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "ixb_internal.h"
+
+namespace ixb {
+
+// device-side loop state for the graph-driven SIMPLE loop
+struct Ctl {
+  // inputs
+  double conv_u, conv_p, conv_t, conv_resi, conv_paso;
+  int iter_ecuaci_max, iter_simple_max;
+  int fixed_count;   // >0: run exactly this many outer passes, no outer test
+  // state
+  int iter_ecuaci, iter_simple;
+  int outer_done;    // passes done in this launch
+  int inner_done;    // passes of the current inner loop (hard cap: iter_ecuaci_max + 2)
+  int exit_code, status;
+  long long n_simple, n_momen, n_pres, n_ener;
+  double err_u, err_p, err_t, maxbo, residuo;
+};
+
+}  // namespace ixb
+
+struct ixb_handle {
+  int mi = 0, nj = 0, LD = 0, rows = 0, prec = 0;
+  size_t fsz = 0;  // elements per field buffer
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaError_t last_cuda = cudaSuccess;
+  // fields (binary64)
+  double *u[2] = {}, *v[2] = {}, *T[2] = {}, *pc[2] = {};
+  double *p = nullptr, *u_ant = nullptr, *v_ant = nullptr, *T_ant = nullptr;
+  double *au = nullptr, *av = nullptr, *b_o = nullptr, *resu = nullptr;
+  double *fcon[3] = {}, *flin[3] = {};
+  double* zero = nullptr;  // a field of zeros: the sources of an equation without any
+  // rows of one sweep staged between its assembly and its line solve
+  void* stage = nullptr;
+  size_t stage_stride = 0;  // elements per row array
+  int stage_P = 0;          // row pitch of a line
+  int cu = 0, cv = 0, cT = 0, cpc = 0;
+  // mesh
+  double* metrics = nullptr;
+  int mstride = 0;
+  double* tables = nullptr;  // T_COUNT mesh-constant 2-D tables
+  float* metrics32 = nullptr;  // binary32 copies (IXB_PREC_FP32_REFINED)
+  float* tables32 = nullptr;
+  bool tables_dirty = true;
+  double *xp_d = nullptr, *yp_d = nullptr;
+  std::vector<double> xu, yv, xp, yp;
+  // boundary tables [var][side][line]
+  ixb::BCEntry* bc = nullptr;
+  int bcstride = 0;
+  // reductions
+  double* partials = nullptr;
+  unsigned int* counters = nullptr;
+  double* norms = nullptr;
+  int pstride = 0;
+  double* h_norms = nullptr;  // pinned
+  double* nu_d = nullptr;
+  // control for graphs
+  ixb::Ctl* ctl_d = nullptr;
+  ixb::Ctl* ctl_h = nullptr;  // pinned
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  bool graph_dirty = true;
+  // params and flags
+  ixb_params prm{};
+  bool has_mesh = false, has_params = false, has_bc[3] = {false, false, false};
+  int iter_ecuaci = 0, iter_simple = 0;
+  int use_graph = 1;
+  int shape_tl[ixb::EQ_COUNT] = {};  // launch shape per sweep (0 = not chosen yet)
+  int shape_g[ixb::EQ_COUNT] = {};
+  int nsm = 148;
+};
+
+namespace ixb {
+// views and state of a handle used by the batched driver (defined in ixb_api.cu)
+Geo<double> handle_geo(const ixb_handle* h);
+Geo<float> handle_geo32(const ixb_handle* h);
+int handle_solver_form(const ixb_handle* h);
+int handle_ready(ixb_handle* h);  // mesh, params and boundary tables set; mesh tables built
+// inputs/outputs of sweep `eq` at the current buffer parity (flips it), no norms
+SweepIO<double> handle_sweep_io(ixb_handle* h, int eq, const double* prev);
+int handle_real_bytes(const ixb_handle* h);  // element size of the staged rows
+}  // namespace ixb

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/ixb.h"
 #include "ixb_device.cuh"
 
@@ -15,6 +17,38 @@ enum NormId { N_DV = 0, N_DP, N_BO, N_DT, N_RES, N_COUNT };
 // IXB_SOLVER_EXACT (1) of the public ABI, plus the mixed-precision form a
 // handle created with IXB_PREC_FP32_REFINED runs in place of the hybrid one.
 constexpr int SOLVER_MIXED = 2;
+
+template <int EQ>
+struct EqIsX { static constexpr bool value = (EQ & 1) != 0; };
+
+// Arithmetic types of one sweep.  The binary64 solvers use binary64
+// throughout.  The mixed solver (handle precision IXB_PREC_FP32_REFINED)
+// stages and solves every line in binary32.  The u, v and T rows are
+// assembled in binary64 and turned into a defect correction (DC): the
+// binary64 residual d - A x of the current values is solved for in binary32
+// and the correction added back in binary64, so the fixed point of these
+// equations is the binary64 one.  The p' rows are assembled and solved in
+// binary32 (p' only steers the iteration; it vanishes at convergence), with
+// their mass source b_o evaluated in binary64.
+template <int SOLVER, int EQ>
+struct SweepTypes {
+  static constexpr bool MIX = SOLVER == SOLVER_MIXED;
+  static constexpr bool DC = MIX && EQ != EQ_PY && EQ != EQ_PX;
+  using S = typename std::conditional<MIX, float, double>::type;        // staged rows, line solve
+  using A = typename std::conditional<MIX && !DC, float, double>::type;  // coefficient assembly
+};
+
+// x-sweep tiles: 64 consecutive rows of 4 lines, one cell per thread.
+// y-sweep tiles: 32 consecutive lines (adjacent ii) x 8 rows, one cell per
+// thread, written back through shared memory as 8-row runs of each line.
+constexpr int kAsmThreads = 256;
+constexpr int kAsmXR = 64, kAsmXL = 4;
+constexpr int kAsmYL = 32, kAsmYR = 8;
+
+__host__ __device__ constexpr int asm_tiles(bool x, int n, int nlines) {
+  return x ? ((n + kAsmXR - 1) / kAsmXR) * ((nlines + kAsmXL - 1) / kAsmXL)
+           : ((nlines + kAsmYL - 1) / kAsmYL) * ((n + kAsmYR - 1) / kAsmYR);
+}
 
 // launch shape of one sweep
 struct SweepShape {
@@ -53,11 +87,25 @@ struct StageBuf {
 // partials of a norm fit the handle's partials buffer.
 constexpr int kAsmGridCap = 148 * 8;
 
+// One instance of a batched launch (see ixb_batch.cu): its views, and its
+// work items first .. first+count-1 in the launch's item list.
+template <class A, class S>
+struct AsmInst {
+  Geo<A> G;
+  SweepIO<double> io;
+  Coef<S> co;
+  int n, line_lo, line_hi;
+  int first, count;
+};
+
 // per-equation assembly launchers (ixb_sweep_<eq>.cu: exact,
 // ixb_sweep_<eq>_fast.cu: hybrid, ixb_sweep_<eq>_mixed.cu: mixed precision)
 template <int EQ, int SOLVER>
 cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
                             const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st);
+template <int EQ, int SOLVER>
+cudaError_t assemble_batch_launch(const void* inst, const int2* items, int nitems, const int* active,
+                                  const BatchNorm& bn, cudaStream_t st);
 
 // line solve of a sweep (ixb_solve.cu): staged rows in, field out
 struct SolveIO {
@@ -71,14 +119,39 @@ struct SolveIO {
   int LD;
   int m, mp;            // chunk rows per thread, padded pitch
 };
+// one instance of a batched line solve
+struct SolveInst {
+  SolveIO io;
+  int n, line_lo, line_hi, nfull;
+  int first, count;  // its work items in the launch's item list
+};
 // form: IXB_SOLVER_HYBRID, IXB_SOLVER_EXACT or SOLVER_MIXED; x: line along
 // ii; dc: the staged right-hand sides are binary64 residuals whose solution
 // is added to `in`
 cudaError_t solve_launch(int form, bool x, bool dc, const SweepShape& s, const SolveIO& io, cudaStream_t st);
 int solve_blocks_per_sm(int form, bool x, bool dc, const SweepShape& s);
 cudaError_t solve_set_smem_limits(int bytes);
+// batched line solve with one launch shape (TL lines x G threads) for all
+// instances; smem: shared memory of the largest instance's lines
+cudaError_t solve_batch_launch(int form, bool x, bool dc, int tl, int g, size_t smem, const SolveInst* inst,
+                               const int2* items, int nitems, const int* active, const BatchNorm& bn,
+                               cudaStream_t st);
 int sweep_occupancy(int eq, int solver, const SweepShape& s);
 int max_sweep_lines(int mi, int nj);
+
+// one instance of a batched correction / residual launch; work items are
+// blocks of kCellChunk cells
+constexpr int kCellChunk = 256;
+struct CellInst {
+  Geo<double> G;
+  double *u, *v, *p, *resu;
+  const double *pc, *au, *av, *T, *u_ant, *fcon, *flin;
+  int first, count;  // its residual work items in the launch's item list
+};
+cudaError_t correct_batch_launch(const CellInst* inst, const int2* items, int nitems, const int* active, int fast,
+                                 cudaStream_t st);
+cudaError_t residual_batch_launch(const CellInst* inst, const int2* items, int nitems, const int* active,
+                                  const BatchNorm& bn, int fast, cudaStream_t st);
 
 // kernel launchers (ixb_kernels.cu); return cudaError_t
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,

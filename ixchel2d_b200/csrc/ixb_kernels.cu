@@ -87,18 +87,23 @@ cudaError_t launch_tables_f64(const Geo<double>& G, double* met, double* tab, cu
 // pressure and velocity correction, main.f90:931-962
 // ---------------------------------------------------------------------------
 template <class R, bool FAST>
-__global__ void correct_kernel(const Geo<R> G, R* __restrict__ u, R* __restrict__ v, R* __restrict__ p,
-                               const R* __restrict__ pc, const R* __restrict__ au, const R* __restrict__ av) {
+__device__ __forceinline__ void correct_cell(const Geo<R>& G, R* __restrict__ u, R* __restrict__ v, R* __restrict__ p,
+                                             const R* __restrict__ pc, const R* __restrict__ au,
+                                             const R* __restrict__ av, int idx) {
   const int ni = G.mi - 1;  // ii = 2..mi
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int total = ni * (G.nj - 1);
-  if (idx >= total) return;
   const int ii = 2 + idx % ni;
   const int jj = 2 + idx / ni;
   const size_t c0 = G.at(ii, jj);
   p[c0] = p[c0] + G.p_update * pc[c0];
   if (ii <= G.mi - 1) u[c0] = u[c0] + qdiv<FAST>(G.met(M_DYU, jj) * (pc[c0] - pc[G.at(ii + 1, jj)]), au[c0]);
   if (jj <= G.nj - 1) v[c0] = v[c0] + qdiv<FAST>(G.met(M_DXV, ii) * (pc[c0] - pc[G.at(ii, jj + 1)]), av[c0]);
+}
+
+template <class R, bool FAST>
+__global__ void correct_kernel(const Geo<R> G, R* __restrict__ u, R* __restrict__ v, R* __restrict__ p,
+                               const R* __restrict__ pc, const R* __restrict__ au, const R* __restrict__ av) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < (G.mi - 1) * (G.nj - 1)) correct_cell<R, FAST>(G, u, v, p, pc, au, av, idx);
 }
 
 // ---------------------------------------------------------------------------
@@ -122,6 +127,58 @@ __global__ void __launch_bounds__(256) residual_kernel(const Geo<R> G, const R* 
   }
   const double s = block_sum(acc);
   finish_norm(ns, s);
+}
+
+// batched forms: work item i = (instance, block of kCellChunk cells)
+template <bool FAST>
+__global__ void __launch_bounds__(kCellChunk) correct_batch_kernel(const CellInst* __restrict__ inst,
+                                                                   const int2* __restrict__ items, const int nitems,
+                                                                   const int* __restrict__ active) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 wi = items[it];
+    if (!active[wi.x]) continue;
+    const CellInst& d = inst[wi.x];
+    const int idx = wi.y * kCellChunk + threadIdx.x;
+    if (idx < (d.G.mi - 1) * (d.G.nj - 1)) correct_cell<double, FAST>(d.G, d.u, d.v, d.p, d.pc, d.au, d.av, idx);
+  }
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(kCellChunk) residual_batch_kernel(const CellInst* __restrict__ inst,
+                                                                    const int2* __restrict__ items, const int nitems,
+                                                                    const int* __restrict__ active,
+                                                                    const BatchNorm bn) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 wi = items[it];
+    if (!active[wi.x]) continue;
+    const CellInst& d = inst[wi.x];
+    const int ni = d.G.mi - 2;
+    const int idx = wi.y * kCellChunk + threadIdx.x;
+    double acc = 0.0;
+    if (idx < ni * (d.G.nj - 1)) {
+      const int ii = 2 + idx % ni, jj = 2 + idx / ni;
+      const double r = residual_u<FAST>(d.G, d.u, d.v, d.T, d.p, d.u_ant, d.fcon, d.flin, ii, jj);
+      d.resu[d.G.at(ii, jj)] = r;
+      acc = r * r;
+    }
+    finish_item_norm(bn, wi.x, d.first, d.count, it, block_sum(acc));
+  }
+}
+
+cudaError_t correct_batch_launch(const CellInst* inst, const int2* items, int nitems, const int* active, int fast,
+                                 cudaStream_t st) {
+  const int grid = std::max(1, std::min(nitems, 148 * 16));
+  if (fast) correct_batch_kernel<true><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active);
+  else correct_batch_kernel<false><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active);
+  return cudaGetLastError();
+}
+
+cudaError_t residual_batch_launch(const CellInst* inst, const int2* items, int nitems, const int* active,
+                                  const BatchNorm& bn, int fast, cudaStream_t st) {
+  const int grid = std::max(1, std::min(nitems, 148 * 8));
+  if (fast) residual_batch_kernel<true><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active, bn);
+  else residual_batch_kernel<false><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active, bn);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -55,4 +55,32 @@ static __device__ void finish_norm(const NormSlot& ns, double block_total) {
   }
 }
 
+// Per-instance norms of a batched launch.  Work item `item` (of instance
+// `inst`, whose items are first .. first+count-1) publishes its partial;
+// the last item of the instance to arrive sums the instance's partials in
+// item order and stores sqrt(sum).  Called by all threads of the CTA.
+
+static __device__ void finish_item_norm(const BatchNorm& bn, int inst, int first, int count, int item,
+                                        double block_total) {
+  __shared__ int is_last;
+  if (threadIdx.x == 0) {
+    bn.partials[item] = block_total;
+    __threadfence();
+    const unsigned prev = atomicAdd(bn.counter + inst, 1u);
+    is_last = (prev == (unsigned)count - 1);
+  }
+  __syncthreads();
+  if (is_last) {
+    __threadfence();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < count; i += blockDim.x) s += __ldcg(bn.partials + first + i);
+    s = block_sum(s);
+    if (threadIdx.x == 0) {
+      bn.result[inst] = sqrt(s);
+      bn.counter[inst] = 0u;
+    }
+  }
+  __syncthreads();
+}
+
 }  // namespace ixb

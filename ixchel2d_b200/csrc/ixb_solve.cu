@@ -20,18 +20,18 @@
 namespace ixb {
 namespace {
 
+// Lines L0 .. L0+TL-1 of one sweep: staged rows -> shared memory -> solve ->
+// field.  Returns this thread's share of ||new - prev||^2.  Called by all
+// threads of the CTA (it holds barriers).
 template <class S, bool X, bool DC, bool EXACT, int TL, int G, int M>
-__global__ void __launch_bounds__(TL * G) solve_kernel(const SolveIO io, const int n, const int line_lo,
-                                                       const int line_hi, const int nfull) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S* sm = reinterpret_cast<S*>(smem_raw);
+__device__ __forceinline__ double solve_group(S* sm, const SolveIO& io, const int n, const int line_lo,
+                                              const int line_hi, const int nfull, const int L0) {
   constexpr int NT = TL * G;
   const int m = M > 0 ? M : io.m;
   const int mp = M > 0 ? (M | 1) : io.mp;
   const int npad = G * m;
   const int LS = (int)line_smem_elems(G, mp);
   const int arr = G * mp;
-  const int L0 = 1 + blockIdx.x * TL;
   const S* ca = static_cast<const S*>(io.coef);
   const S* cb = ca + io.stride;
   const S* cc = cb + io.stride;
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(TL * G) solve_kernel(const SolveIO io, const i
       const S xs = sm[l * LS + 3 * arr + ch * mp + (r - ch * m)];
       if constexpr (DC) x = io.in[g] + double(xs);
       else x = double(xs);
-      if (io.nrm0.partials && r >= 1 && r <= n - 2) {
+      if (r >= 1 && r <= n - 2) {
         const double dv = x - (io.prev ? io.prev[g] : 0.0);
         acc += dv * dv;
       }
@@ -99,9 +99,37 @@ __global__ void __launch_bounds__(TL * G) solve_kernel(const SolveIO io, const i
     }
     io.out[g] = x;
   }
+  return acc;
+}
+
+template <class S, bool X, bool DC, bool EXACT, int TL, int G, int M>
+__global__ void __launch_bounds__(TL * G) solve_kernel(const SolveIO io, const int n, const int line_lo,
+                                                       const int line_hi, const int nfull) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const double acc = solve_group<S, X, DC, EXACT, TL, G, M>(reinterpret_cast<S*>(smem_raw), io, n, line_lo, line_hi,
+                                                            nfull, 1 + blockIdx.x * TL);
   if (io.nrm0.partials) {
     const double s = block_sum(acc);
     finish_norm(io.nrm0, s);
+  }
+}
+
+// Batched line solve: work item i = (instance, line group) of items[i];
+// a CTA walks the items grid-stride, skipping instances that no longer
+// iterate; the pass norm is reduced per instance.
+template <class S, bool X, bool DC, bool EXACT, int TL, int G>
+__global__ void __launch_bounds__(TL * G) solve_batch_kernel(const SolveInst* __restrict__ inst,
+                                                             const int2* __restrict__ items, const int nitems,
+                                                             const int* __restrict__ active, const BatchNorm bn) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 wi = items[it];
+    if (!active[wi.x]) continue;  // uniform across the CTA
+    const SolveInst& d = inst[wi.x];
+    const double acc = solve_group<S, X, DC, EXACT, TL, G, 0>(reinterpret_cast<S*>(smem_raw), d.io, d.n, d.line_lo,
+                                                              d.line_hi, d.nfull, 1 + wi.y * TL);
+    if (bn.partials) finish_item_norm(bn, wi.x, d.first, d.count, it, block_sum(acc));
+    __syncthreads();  // the next item reuses the shared memory
   }
 }
 
@@ -141,6 +169,27 @@ struct SolveSet {
 #undef IXB_OCC_
     return e == cudaSuccess ? nb : 0;
   }
+  static cudaError_t launch_batch(int tl, int g, size_t smem, const SolveInst* inst, const int2* items, int nitems,
+                                  const int* active, const BatchNorm& bn, cudaStream_t st) {
+#define IXB_BCASE_(TL_, G_)                                                                                \
+  if (tl == TL_ && g == G_) {                                                                              \
+    auto k = solve_batch_kernel<S, X, DC, EXACT, TL_, G_>;                                                 \
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
+    if (e != cudaSuccess) return e;                                                                        \
+    int per_sm = 0, dev = 0, nsm = 0;                                                                      \
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TL_ * G_, smem)) != cudaSuccess)    \
+      return e;                                                                                            \
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;                                                \
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;  \
+    if (per_sm < 1) return cudaErrorInvalidValue;                                                          \
+    const int grid = std::max(1, std::min(nitems, per_sm * nsm));                                          \
+    k<<<grid, TL_ * G_, smem, st>>>(inst, items, nitems, active, bn);                                      \
+    return cudaGetLastError();                                                                             \
+  }
+    IXB_SWEEP_SHAPES(IXB_BCASE_)
+#undef IXB_BCASE_
+    return cudaErrorInvalidValue;
+  }
   static cudaError_t limits(int bytes) {
     cudaError_t e = cudaSuccess;
     auto set = [&](auto k) {
@@ -175,6 +224,14 @@ cudaError_t solve_launch(int form, bool x, bool dc, const SweepShape& s, const S
 
 int solve_blocks_per_sm(int form, bool x, bool dc, const SweepShape& s) {
   return with_set(form, x, dc, [&](auto set) { return decltype(set)::occupancy(s); });
+}
+
+cudaError_t solve_batch_launch(int form, bool x, bool dc, int tl, int g, size_t smem, const SolveInst* inst,
+                               const int2* items, int nitems, const int* active, const BatchNorm& bn,
+                               cudaStream_t st) {
+  return with_set(form, x, dc, [&](auto set) {
+    return decltype(set)::launch_batch(tl, g, smem, inst, items, nitems, active, bn, st);
+  });
 }
 
 cudaError_t solve_set_smem_limits(int bytes) {

@@ -26,8 +26,6 @@ namespace ixb {
 // ---------------------------------------------------------------------------
 // per-equation assembly dispatch
 // ---------------------------------------------------------------------------
-template <int EQ>
-struct EqIsX { static constexpr bool value = (EQ & 1) != 0; };
 
 // Row of cell (ii,jj); the side outputs (au, av, b_o and the b_o norm) are
 // written only when `keep` is set.
@@ -64,23 +62,6 @@ __device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<F
     return assemble_tx<FAST>(G, io, ii, jj);
   }
 }
-
-// Arithmetic types of one sweep.  The binary64 solvers use binary64
-// throughout.  The mixed solver (handle precision IXB_PREC_FP32_REFINED)
-// stages and solves every line in binary32.  The u, v and T rows are
-// assembled in binary64 and turned into a defect correction (DC): the
-// binary64 residual d - A x of the current values is solved for in binary32
-// and the correction added back in binary64, so the fixed point of these
-// equations is the binary64 one.  The p' rows are assembled and solved in
-// binary32 (p' only steers the iteration; it vanishes at convergence), with
-// their mass source b_o evaluated in binary64.
-template <int SOLVER, int EQ>
-struct SweepTypes {
-  static constexpr bool MIX = SOLVER == SOLVER_MIXED;
-  static constexpr bool DC = MIX && EQ != EQ_PY && EQ != EQ_PX;
-  using S = typename std::conditional<MIX, float, double>::type;        // staged rows, line solve
-  using A = typename std::conditional<MIX && !DC, float, double>::type;  // coefficient assembly
-};
 
 template <class A>
 __host__ __device__ inline const Geo<A>& pick_geo(const Geo<double>& d, const Geo<float>& f) {
@@ -145,71 +126,99 @@ __device__ __forceinline__ Row<typename SweepTypes<SOLVER, EQ>::A> staged_row(
   return row;
 }
 
-// x-sweep tiles: 64 consecutive rows of 4 lines, one cell per thread.
-// y-sweep tiles: 32 consecutive lines (adjacent ii) x 8 rows, one cell per
-// thread, written back through shared memory as 8-row runs of each line.
-constexpr int kAsmThreads = 256;
-constexpr int kAsmXR = 64, kAsmXL = 4;
-constexpr int kAsmYL = 32, kAsmYR = 8;
-
-__host__ __device__ constexpr int asm_tiles(bool x, int n, int nlines) {
-  return x ? ((n + kAsmXR - 1) / kAsmXR) * ((nlines + kAsmXL - 1) / kAsmXL)
-           : ((nlines + kAsmYL - 1) / kAsmYL) * ((n + kAsmYR - 1) / kAsmYR);
+// One tile of the assembly of sweep EQ: rows of lines line_lo..line_hi
+// written to `co` (line L at (L - line_lo) * P).  Called by all threads of
+// the CTA (a y tile holds barriers around its shared-memory transpose).
+template <int EQ, int SOLVER>
+__device__ __forceinline__ void assemble_tile(const Geo<typename SweepTypes<SOLVER, EQ>::A>& G_,
+                                              const SweepIO<double>& io,
+                                              const Coef<typename SweepTypes<SOLVER, EQ>::S>& co, const int n,
+                                              const int line_lo, const int line_hi, const int tile, double& acc_bo,
+                                              typename SweepTypes<SOLVER, EQ>::S (*tile_s)[kAsmYR][kAsmYL + 1]) {
+  using S = typename SweepTypes<SOLVER, EQ>::S;
+  constexpr bool X = EqIsX<EQ>::value;
+  if constexpr (X) {
+    const int tr_n = (n + kAsmXR - 1) / kAsmXR;
+    const int tl = tile / tr_n, tr = tile - tl * tr_n;
+    const int r = tr * kAsmXR + (threadIdx.x % kAsmXR);
+    const int L = line_lo + tl * kAsmXL + threadIdx.x / kAsmXR;
+    const bool valid = r < n && L <= line_hi;
+    const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
+    if (valid) {
+      const size_t o = (size_t)(L - line_lo) * co.P + r;
+      co.a[o] = S(row.a); co.b[o] = S(row.b); co.c[o] = S(row.c); co.d[o] = S(row.d);
+    }
+  } else {
+    const int nl = line_hi - line_lo + 1;
+    const int tl_n = (nl + kAsmYL - 1) / kAsmYL;
+    const int tr = tile / tl_n, tl = tile - tr * tl_n;
+    const int lo = threadIdx.x % kAsmYL, ro = threadIdx.x / kAsmYL;
+    const int L = line_lo + tl * kAsmYL + lo;  // adjacent ii in a warp: coalesced field reads
+    const int r = tr * kAsmYR + ro;
+    const bool valid = r < n && L <= line_hi;
+    const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
+    tile_s[0][ro][lo] = S(row.a); tile_s[1][ro][lo] = S(row.b);
+    tile_s[2][ro][lo] = S(row.c); tile_s[3][ro][lo] = S(row.d);
+    __syncthreads();
+    const int wl = threadIdx.x / kAsmYR, wr = threadIdx.x % kAsmYR;  // 8-row runs of one line
+    const int Lw = line_lo + tl * kAsmYL + wl, rw = tr * kAsmYR + wr;
+    if (Lw <= line_hi && rw < n) {
+      const size_t o = (size_t)(Lw - line_lo) * co.P + rw;
+      co.a[o] = tile_s[0][wr][wl]; co.b[o] = tile_s[1][wr][wl];
+      co.c[o] = tile_s[2][wr][wl]; co.d[o] = tile_s[3][wr][wl];
+    }
+    __syncthreads();
+  }
 }
 
-// Assemble the rows of lines line_lo..line_hi of sweep EQ into `co`
-// (line L at (L - line_lo) * P).  Grid-stride over tiles; the b_o norm
-// (p'-x) is reduced over the grid.
+// Assemble the rows of lines line_lo..line_hi of sweep EQ into `co`.
+// Grid-stride over tiles; the b_o norm (p'-x) is reduced over the grid.
 template <int EQ, int SOLVER>
 __global__ void __launch_bounds__(kAsmThreads)
     assemble_kernel(const Geo<typename SweepTypes<SOLVER, EQ>::A> G_, const SweepIO<double> io,
                     const Coef<typename SweepTypes<SOLVER, EQ>::S> co, const int n, const int line_lo,
                     const int line_hi) {
   using S = typename SweepTypes<SOLVER, EQ>::S;
-  constexpr bool X = EqIsX<EQ>::value;
-  const int nl = line_hi - line_lo + 1;
-  const int ntiles = asm_tiles(X, n, nl);
+  __shared__ S tile_s[4][kAsmYR][kAsmYL + 1];
+  const int ntiles = asm_tiles(EqIsX<EQ>::value, n, line_hi - line_lo + 1);
   double acc_bo = 0.0;
-  if constexpr (X) {
-    const int tr_n = (n + kAsmXR - 1) / kAsmXR;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-      const int tl = tile / tr_n, tr = tile - tl * tr_n;
-      const int r = tr * kAsmXR + (threadIdx.x % kAsmXR);
-      const int L = line_lo + tl * kAsmXL + threadIdx.x / kAsmXR;
-      const bool valid = r < n && L <= line_hi;
-      const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
-      if (valid) {
-        const size_t o = (size_t)(L - line_lo) * co.P + r;
-        co.a[o] = S(row.a); co.b[o] = S(row.b); co.c[o] = S(row.c); co.d[o] = S(row.d);
-      }
-    }
-  } else {
-    __shared__ S tile_s[4][kAsmYR][kAsmYL + 1];
-    const int tl_n = (nl + kAsmYL - 1) / kAsmYL;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-      const int tr = tile / tl_n, tl = tile - tr * tl_n;
-      const int lo = threadIdx.x % kAsmYL, ro = threadIdx.x / kAsmYL;
-      const int L = line_lo + tl * kAsmYL + lo;  // adjacent ii in a warp: coalesced field reads
-      const int r = tr * kAsmYR + ro;
-      const bool valid = r < n && L <= line_hi;
-      const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
-      tile_s[0][ro][lo] = S(row.a); tile_s[1][ro][lo] = S(row.b);
-      tile_s[2][ro][lo] = S(row.c); tile_s[3][ro][lo] = S(row.d);
-      __syncthreads();
-      const int wl = threadIdx.x / kAsmYR, wr = threadIdx.x % kAsmYR;  // 8-row runs of one line
-      const int Lw = line_lo + tl * kAsmYL + wl, rw = tr * kAsmYR + wr;
-      if (Lw <= line_hi && rw < n) {
-        const size_t o = (size_t)(Lw - line_lo) * co.P + rw;
-        co.a[o] = tile_s[0][wr][wl]; co.b[o] = tile_s[1][wr][wl];
-        co.c[o] = tile_s[2][wr][wl]; co.d[o] = tile_s[3][wr][wl];
-      }
-      __syncthreads();
-    }
-  }
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    assemble_tile<EQ, SOLVER>(G_, io, co, n, line_lo, line_hi, tile, acc_bo, tile_s);
   if (io.nrm1.partials) {
     const double s = block_sum(acc_bo);
     finish_norm(io.nrm1, s);
   }
+}
+
+// Batched assembly: work item i = (instance, tile) of items[i]; a CTA walks
+// the items grid-stride, skipping instances that no longer iterate.  The
+// b_o norm is reduced per instance over its items (finish_item_norm).
+template <int EQ, int SOLVER>
+__global__ void __launch_bounds__(kAsmThreads)
+    assemble_batch_kernel(const AsmInst<typename SweepTypes<SOLVER, EQ>::A, typename SweepTypes<SOLVER, EQ>::S>*
+                              __restrict__ inst,
+                          const int2* __restrict__ items, const int nitems, const int* __restrict__ active,
+                          const BatchNorm bn) {
+  using S = typename SweepTypes<SOLVER, EQ>::S;
+  __shared__ S tile_s[4][kAsmYR][kAsmYL + 1];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 wi = items[it];
+    if (!active[wi.x]) continue;  // uniform across the CTA
+    const auto& d = inst[wi.x];
+    double acc_bo = 0.0;
+    assemble_tile<EQ, SOLVER>(d.G, d.io, d.co, d.n, d.line_lo, d.line_hi, wi.y, acc_bo, tile_s);
+    if (bn.partials) finish_item_norm(bn, wi.x, d.first, d.count, it, block_sum(acc_bo));
+  }
+}
+
+template <int EQ, int SOLVER>
+cudaError_t assemble_batch_launch(const void* inst, const int2* items, int nitems, const int* active,
+                                  const BatchNorm& bn, cudaStream_t st) {
+  using ST = SweepTypes<SOLVER, EQ>;
+  const int grid = std::max(1, std::min(nitems, kAsmGridCap * 4));
+  assemble_batch_kernel<EQ, SOLVER><<<grid, kAsmThreads, 0, st>>>(
+      static_cast<const AsmInst<typename ST::A, typename ST::S>*>(inst), items, nitems, active, bn);
+  return cudaGetLastError();
 }
 
 template <int EQ, int SOLVER>

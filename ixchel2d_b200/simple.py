@@ -17,12 +17,30 @@ def _f64(a) -> np.ndarray:
 class Simple2D:
     """Owns an ixb handle (device memory + stream) for an (mi, nj) grid."""
 
-    def __init__(self, mi: int, nj: int, prec: int = F.PREC_FP64):
+    def __init__(self, mi: int, nj: int, prec: int = F.PREC_FP64, handle=None):
         self.mi, self.nj = mi, nj
-        h = C.c_void_p()
-        F.check(F.lib.ixb_create(mi, nj, prec, C.byref(h)), "ixb_create")
+        if handle is None:
+            h = C.c_void_p()
+            F.check(F.lib.ixb_create(mi, nj, prec, C.byref(h)), "ixb_create")
+            self._owned = True
+        else:  # a handle owned elsewhere (an instance of a batch)
+            h = handle
+            self._owned = False
         self.h = h
         self._shapes = shapes(mi, nj)
+
+    def setup(self, case: Case, **param_over) -> "Simple2D":
+        """Mesh, parameters, boundary tables, sources and state of `case`."""
+        self.set_mesh(case.xu, case.yv, case.xp, case.yp)
+        prm = dict(case.params)
+        prm.update(param_over)
+        self.set_params(**prm)
+        for var, sides in case.bc.items():
+            self.set_bc(var, sides)
+        for var, (fc, fl) in case.sources.items():
+            self.set_sources(var, fc, fl)
+        self.upload(case.state)
+        return self
 
     # ---- setup ----
     def set_mesh(self, xu, yv, xp, yp):
@@ -73,17 +91,7 @@ class Simple2D:
 
     @classmethod
     def from_case(cls, case: Case, prec: int = F.PREC_FP64, **param_over) -> "Simple2D":
-        s = cls(case.mi, case.nj, prec)
-        s.set_mesh(case.xu, case.yv, case.xp, case.yp)
-        prm = dict(case.params)
-        prm.update(param_over)
-        s.set_params(**prm)
-        for var, sides in case.bc.items():
-            s.set_bc(var, sides)
-        for var, (fc, fl) in case.sources.items():
-            s.set_sources(var, fc, fl)
-        s.upload(case.state)
-        return s
+        return cls(case.mi, case.nj, prec).setup(case, **param_over)
 
     # ---- hot path ----
     def iterations(self, n: int) -> dict:
@@ -142,7 +150,8 @@ class Simple2D:
 
     def close(self):
         if getattr(self, "h", None):
-            F.lib.ixb_destroy(self.h)
+            if self._owned:
+                F.lib.ixb_destroy(self.h)
             self.h = None
 
     def __del__(self):
