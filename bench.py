@@ -281,6 +281,88 @@ def adi_microbench(stream, n=4096, nsys=4096, reps=5):
     return out
 
 
+def batched_bench(stream, n_inst=256, iters=30, n_conv=16, conv_cap=20000):
+    """Batched cavities (ixb_batch_*): natural-convection cavities, square
+    side uniform in {64..512} and Ra log-uniform in [1e3, 1e6] (Pr 0.71,
+    seed 1234).  Throughput: `iters` outer iterations of all n_inst
+    instances (every instance kept active), batched in both precision
+    forms, against the single-instance binary64 path looped over the first
+    16 instances.  Convergence: n_conv smaller cavities (side 64..128, Ra
+    1e3..1e5) each iterated to maxbo < 1e-8 (cap conv_cap iterations),
+    batched refined vs the single-instance binary64 path one after the
+    other; instances per second of each."""
+    import torch
+    from ixchel2d_b200 import Batch, Simple2D, cases
+    from ixchel2d_b200 import _ffi as F
+    rng = np.random.default_rng(1234)
+    sides = rng.integers(64, 513, n_inst)
+    ras = 10.0 ** rng.uniform(3.0, 6.0, n_inst)
+    cs = [cases.natural_cavity(int(a), int(a), Ra=float(r), T0=0.5) for a, r in zip(sides, ras)]
+    cells = sum(c.cells for c in cs)
+    out = {"instances": n_inst, "cells": cells, "iters": iters}
+
+    def timed(fn):  # host wall time of calls that synchronise before returning
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    for name, prec in (("refined", F.PREC_FP32_REFINED), ("fp64", F.PREC_FP64)):
+        bt = Batch.from_cases(cs, prec=prec, conv_paso=0.0)
+        bt.autotune(reps=2)
+        bt.iterate(3)
+        dt = timed(lambda: bt.iterate(iters))
+        out[f"batched_{name}"] = {"ms_per_iter": dt / iters * 1e3, "mcell_iter_s": cells * iters / dt / 1e6}
+        bt.close()
+    sims = [Simple2D.from_case(c) for c in cs[:16]]
+    for sm in sims:
+        sm.iterations(3)
+    dt = timed(lambda: [sm.iterations(iters) for sm in sims])
+    c16 = sum(c.cells for c in cs[:16])
+    out["looped_single_fp64"] = {"instances": 16, "mcell_iter_s": c16 * iters / dt / 1e6,
+                                 "ms_per_instance_iter": dt / 16 / iters * 1e3}
+    for sm in sims:
+        sm.close()
+    out["batched_refined_over_looped_fp64"] = (out["batched_refined"]["mcell_iter_s"] /
+                                               out["looped_single_fp64"]["mcell_iter_s"])
+    # convergence of smaller cavities
+    sides = rng.integers(64, 129, n_conv)
+    ras = 10.0 ** rng.uniform(3.0, 5.0, n_conv)
+    cc = [cases.natural_cavity(int(a), int(a), Ra=float(r), T0=0.5) for a, r in zip(sides, ras)]
+    bt = Batch.from_cases(cc, prec=F.PREC_FP32_REFINED, conv_paso=1e-8, conv_resi=1e30)
+    bt.autotune(reps=2)
+    bt.restart()
+    left = [n_conv]
+    dt_b = timed(lambda: left.__setitem__(0, bt.iterate(conv_cap)))
+    reps = [bt.report(i) for i in range(n_conv)]
+    bt.close()
+    conv_b = sum(1 for r in reps if r["exit_code"] == 1)
+
+    def single_all():
+        n = 0
+        for c in cc:
+            sm = Simple2D.from_case(c, conv_paso=1e-8, conv_resi=1e30)
+            it = 0
+            while it < conv_cap:
+                r = sm.iterations(500)
+                it += 500
+                if r["maxbo"] < 1e-8:
+                    n += 1
+                    break
+            sm.close()
+        return n
+    conv_s = [0]
+    dt_s = timed(lambda: conv_s.__setitem__(0, single_all()))
+    out["converge_small"] = {
+        "instances": n_conv, "criterion": "maxbo < 1e-8", "cap_iters": conv_cap,
+        "batched_refined": {"converged": conv_b, "seconds": dt_b, "instances_per_s": conv_b / dt_b,
+                            "iters": [r["n_simple"] for r in reps]},
+        "looped_single_fp64": {"converged": conv_s[0], "seconds": dt_s, "instances_per_s": conv_s[0] / dt_s},
+    }
+    return out
+
+
 def make_sim(case, prec, stream, shapes):
     from ixchel2d_b200 import Simple2D
     sim = Simple2D.from_case(case, prec=prec)
@@ -385,6 +467,8 @@ def run_ours(args):
 
     # ---- batched line-solve microbenchmark (4096 systems x 4096 unknowns) ----
     adi = adi_microbench(stream)
+    # ---- batched cavities ----
+    batched = batched_bench(stream)
 
     # ---- per-phase times (cold L2) of the refined path on a scratch handle ----
     scratch, _ = make_sim(case, F.PREC_FP32_REFINED, stream, shapes["refined"])
@@ -426,6 +510,7 @@ def run_ours(args):
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": phase_ms[dom]},
             "phases_ms_cold_l2": dict(zip(PHASES, phase_ms)),
             "adi_line_solve": adi,
+            "batched_cavities": batched,
             "sweep_shapes": {n: {SWEEPS[int(k)]: list(v[:2]) for k, v in sh.items()} for n, sh in shapes.items()},
             "iteration_alg_bytes": iter_bytes,
             "cpu_baseline": None if cpu_val is None else {
