@@ -267,6 +267,7 @@ int body_host(ixb_handle* h, bool outer_test, ixb_report* rep, int* exit_code) {
 __device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
 
 __global__ void ctl_begin_kernel(Ctl* c, cudaGraphConditionalHandle outer) {
+  IXB_PDL_ENTRY();
   cudaGraphSetConditional(outer, 1u);
   c->outer_done = 0;
   c->exit_code = 0;
@@ -275,6 +276,7 @@ __global__ void ctl_begin_kernel(Ctl* c, cudaGraphConditionalHandle outer) {
 }
 
 __global__ void ctl_inner_kernel(Ctl* c, const double* norms, int which, cudaGraphConditionalHandle inner) {
+  IXB_PDL_ENTRY();
   // which: 0 momentum (N_DV vs conv_u), 1 pressure (N_DP vs conv_p), 2 energy (N_DT vs conv_t)
   double err, conv;
   if (which == 0) { err = norms[N_DV]; conv = c->conv_u; c->err_u = err; c->n_momen++; }
@@ -297,11 +299,13 @@ __global__ void ctl_inner_kernel(Ctl* c, const double* norms, int which, cudaGra
 // Gate: after a non-finite stop, later inner loops of the same pass must not
 // start.  Sets the inner loop's initial condition.
 __global__ void ctl_gate_kernel(Ctl* c, cudaGraphConditionalHandle inner) {
+  IXB_PDL_ENTRY();
   c->inner_done = 0;
   cudaGraphSetConditional(inner, c->status == 0 ? 1u : 0u);
 }
 
 __global__ void ctl_outer_kernel(Ctl* c, const double* norms, cudaGraphConditionalHandle outer) {
+  IXB_PDL_ENTRY();
   if (c->status != 0) { cudaGraphSetConditional(outer, 0); return; }
   c->residuo = norms[N_RES];
   c->n_simple++;
@@ -371,8 +375,7 @@ int build_graph(ixb_handle* h) {
   CK(cudaGraphConditionalHandleCreate(&c_outer, g, 1, cudaGraphCondAssignDefault));
   cudaGraphNode_t n_begin, n_outer;
   TRY(capture_into(h, g, nullptr, [&]() {
-    ctl_begin_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_outer);
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+    return launch_k(ctl_begin_kernel, 1, 1, 0, h->stream, h->ctl_d, c_outer) == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &n_begin));
   cudaGraph_t outer_body;
   TRY(add_while(h, g, &n_begin, c_outer, &outer_body, &n_outer));
@@ -384,7 +387,7 @@ int build_graph(ixb_handle* h) {
   cudaGraphNode_t last, wn;
   cudaGraph_t b;
   TRY(capture_into(h, outer_body, nullptr, [&]() {
-    ctl_gate_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_mom);
+    if (launch_k(ctl_gate_kernel, 1, 1, 0, h->stream, h->ctl_d, c_mom) != cudaSuccess) return IXB_ECUDA;
     return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &last));
   TRY(add_while(h, outer_body, &last, c_mom, &b, &wn));
@@ -394,12 +397,12 @@ int build_graph(ixb_handle* h) {
     const double* v_start = h->v[h->cv];
     TRY(sweep(h, EQ_VY, nullptr, false));
     TRY(sweep(h, EQ_VX, v_start, true));
-    ctl_inner_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, 0, c_mom);
+    if (launch_k(ctl_inner_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, 0, c_mom) != cudaSuccess) return IXB_ECUDA;
     return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &last));
   TRY(capture_into(h, outer_body, &wn, [&]() {
     if (cudaMemsetAsync(h->pc[h->cpc], 0, h->fsz * sizeof(double), h->stream) != cudaSuccess) return IXB_ECUDA;
-    ctl_gate_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_pres);
+    if (launch_k(ctl_gate_kernel, 1, 1, 0, h->stream, h->ctl_d, c_pres) != cudaSuccess) return IXB_ECUDA;
     return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &last));
   TRY(add_while(h, outer_body, &last, c_pres, &b, &wn));
@@ -407,12 +410,12 @@ int build_graph(ixb_handle* h) {
     const double* pc_start = h->pc[h->cpc];
     TRY(sweep(h, EQ_PY, nullptr, false));
     TRY(sweep(h, EQ_PX, pc_start, true));
-    ctl_inner_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, 1, c_pres);
+    if (launch_k(ctl_inner_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, 1, c_pres) != cudaSuccess) return IXB_ECUDA;
     return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &last));
   TRY(capture_into(h, outer_body, &wn, [&]() {
     TRY(correct(h));
-    ctl_gate_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, c_ener);
+    if (launch_k(ctl_gate_kernel, 1, 1, 0, h->stream, h->ctl_d, c_ener) != cudaSuccess) return IXB_ECUDA;
     return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &last));
   TRY(add_while(h, outer_body, &last, c_ener, &b, &wn));
@@ -420,12 +423,12 @@ int build_graph(ixb_handle* h) {
     const double* t_start = h->T[h->cT];
     TRY(sweep(h, EQ_TY, nullptr, false));
     TRY(sweep(h, EQ_TX, t_start, true));
-    ctl_inner_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, 2, c_ener);
+    if (launch_k(ctl_inner_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, 2, c_ener) != cudaSuccess) return IXB_ECUDA;
     return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &last));
   TRY(capture_into(h, outer_body, &wn, [&]() {
     TRY(residual(h));
-    ctl_outer_kernel<<<1, 1, 0, h->stream>>>(h->ctl_d, h->norms, c_outer);
+    if (launch_k(ctl_outer_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, c_outer) != cudaSuccess) return IXB_ECUDA;
     return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
   }, &last));
   CK(cudaGraphInstantiate(&h->graph_exec, g, 0));

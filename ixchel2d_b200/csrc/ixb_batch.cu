@@ -306,6 +306,7 @@ __device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
 // budget left.
 __global__ void batch_ctl_kernel(BInst* inst, int* active, const double* results, int count, BCtl* ctl,
                                  cudaGraphConditionalHandle cond) {
+  IXB_PDL_ENTRY();
   int any = 0;
   for (int i = threadIdx.x; i < count; i += blockDim.x) {
     if (!active[i]) continue;
@@ -340,6 +341,7 @@ __global__ void batch_ctl_kernel(BInst* inst, int* active, const double* results
 }
 
 __global__ void batch_begin_kernel(const int* active, int count, BCtl* ctl, cudaGraphConditionalHandle cond) {
+  IXB_PDL_ENTRY();
   int any = 0;
   for (int i = threadIdx.x; i < count; i += blockDim.x) any |= active[i];
   any = __syncthreads_or(any);
@@ -356,8 +358,7 @@ int build_graph(ixb_batch* b) {
   cudaGraphNode_t n_begin, n_while;
   {
     BCK(cudaStreamBeginCaptureToGraph(b->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    batch_begin_kernel<<<1, 256, 0, b->stream>>>(b->active, b->count, b->ctl_d, cond);
-    const cudaError_t le = cudaGetLastError();
+    const cudaError_t le = launch_k(batch_begin_kernel, 1, 256, 0, b->stream, (const int*)b->active, b->count, b->ctl_d, cond);
     cudaGraph_t out = nullptr;
     BCK(cudaStreamEndCapture(b->stream, &out));
     BCK(le);
@@ -375,8 +376,9 @@ int build_graph(ixb_batch* b) {
   BCK(cudaStreamBeginCaptureToGraph(b->stream, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   int st = body(b);
   if (st == IXB_OK) {
-    batch_ctl_kernel<<<1, 256, 0, b->stream>>>(b->inst_d, b->active, b->results, b->count, b->ctl_d, cond);
-    if (cudaGetLastError() != cudaSuccess) st = IXB_ECUDA;
+    if (launch_k(batch_ctl_kernel, 1, 256, 0, b->stream, b->inst_d, b->active, (const double*)b->results, b->count,
+                 b->ctl_d, cond) != cudaSuccess)
+      st = IXB_ECUDA;
   }
   cudaGraph_t captured;
   const cudaError_t ce = cudaStreamEndCapture(b->stream, &captured);

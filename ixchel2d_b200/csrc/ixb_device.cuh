@@ -17,6 +17,15 @@
 
 namespace ixb {
 
+// First statement of every kernel of the SIMPLE loop: wait for the previous
+// kernel of the stream (programmatic dependent launch) and let the next one
+// be placed.
+#define IXB_PDL_ENTRY()                        \
+  do {                                         \
+    cudaGridDependencySynchronize();           \
+    cudaTriggerProgrammaticLaunchCompletion(); \
+  } while (0)
+
 // metric arrays inside one device buffer, each `mstride` long, 1-based.
 // M_HXU/M_HYV are the energy equation's face diffusivities
 // hmean(ge,ge,fexu(k)) / hmean(ge,ge,feyv(k)), M_RHXU/M_RHYV their

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "ixb_internal.h"
 #include "ixb_reduce.cuh"
@@ -102,6 +103,7 @@ __device__ __forceinline__ void correct_cell(const Geo<R>& G, R* __restrict__ u,
 template <class R, bool FAST>
 __global__ void correct_kernel(const Geo<R> G, R* __restrict__ u, R* __restrict__ v, R* __restrict__ p,
                                const R* __restrict__ pc, const R* __restrict__ au, const R* __restrict__ av) {
+  IXB_PDL_ENTRY();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx < (G.mi - 1) * (G.nj - 1)) correct_cell<R, FAST>(G, u, v, p, pc, au, av, idx);
 }
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(256) residual_kernel(const Geo<R> G, const R* 
                                                        const R* __restrict__ p, const R* __restrict__ u_ant,
                                                        const R* __restrict__ fcon, const R* __restrict__ flin,
                                                        R* __restrict__ resu, NormSlot ns) {
+  IXB_PDL_ENTRY();
   const int ni = G.mi - 2;  // ii = 2..mi-1
   const int total = ni * (G.nj - 1);
   double acc = 0.0;
@@ -134,6 +137,7 @@ template <bool FAST>
 __global__ void __launch_bounds__(kCellChunk) correct_batch_kernel(const CellInst* __restrict__ inst,
                                                                    const int2* __restrict__ items, const int nitems,
                                                                    const int* __restrict__ active) {
+  IXB_PDL_ENTRY();
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 wi = items[it];
     if (!active[wi.x]) continue;
@@ -148,6 +152,7 @@ __global__ void __launch_bounds__(kCellChunk) residual_batch_kernel(const CellIn
                                                                     const int2* __restrict__ items, const int nitems,
                                                                     const int* __restrict__ active,
                                                                     const BatchNorm bn) {
+  IXB_PDL_ENTRY();
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 wi = items[it];
     if (!active[wi.x]) continue;
@@ -168,17 +173,15 @@ __global__ void __launch_bounds__(kCellChunk) residual_batch_kernel(const CellIn
 cudaError_t correct_batch_launch(const CellInst* inst, const int2* items, int nitems, const int* active, int fast,
                                  cudaStream_t st) {
   const int grid = std::max(1, std::min(nitems, 148 * 16));
-  if (fast) correct_batch_kernel<true><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active);
-  else correct_batch_kernel<false><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active);
-  return cudaGetLastError();
+  if (fast) return launch_k(correct_batch_kernel<true>, grid, kCellChunk, 0, st, inst, items, nitems, active);
+  return launch_k(correct_batch_kernel<false>, grid, kCellChunk, 0, st, inst, items, nitems, active);
 }
 
 cudaError_t residual_batch_launch(const CellInst* inst, const int2* items, int nitems, const int* active,
                                   const BatchNorm& bn, int fast, cudaStream_t st) {
   const int grid = std::max(1, std::min(nitems, 148 * 8));
-  if (fast) residual_batch_kernel<true><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active, bn);
-  else residual_batch_kernel<false><<<grid, kCellChunk, 0, st>>>(inst, items, nitems, active, bn);
-  return cudaGetLastError();
+  if (fast) return launch_k(residual_batch_kernel<true>, grid, kCellChunk, 0, st, inst, items, nitems, active, bn);
+  return launch_k(residual_batch_kernel<false>, grid, kCellChunk, 0, st, inst, items, nitems, active, bn);
 }
 
 // ---------------------------------------------------------------------------
@@ -271,6 +274,14 @@ int sweep_occupancy(int eq, int solver, const SweepShape& s) {
   return solve_blocks_per_sm(solver, eq_is_x(eq), eq_dc(eq, solver), s);
 }
 
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("IXB_PDL");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 cudaError_t sweep_set_smem_limits() {
   static int done = 0;
   if (done) return cudaSuccess;
@@ -323,9 +334,9 @@ cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, doubl
                                const double* au, const double* av, int fast, cudaStream_t st) {
   const int total = (G.mi - 1) * (G.nj - 1);
   const int bs = 256;
-  if (fast) correct_kernel<double, true><<<(total + bs - 1) / bs, bs, 0, st>>>(G, u, v, p, pc, au, av);
-  else correct_kernel<double, false><<<(total + bs - 1) / bs, bs, 0, st>>>(G, u, v, p, pc, au, av);
-  return cudaGetLastError();
+  const int grid = (total + bs - 1) / bs;
+  if (fast) return launch_k(correct_kernel<double, true>, grid, bs, 0, st, G, u, v, p, pc, au, av);
+  return launch_k(correct_kernel<double, false>, grid, bs, 0, st, G, u, v, p, pc, au, av);
 }
 
 int residual_grid(int mi, int nj) {
@@ -336,11 +347,9 @@ int residual_grid(int mi, int nj) {
 cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const double* v, const double* T,
                                 const double* p, const double* u_ant, const double* fcon, const double* flin,
                                 double* resu, NormSlot ns, int fast, cudaStream_t st) {
-  if (fast)
-    residual_kernel<double, true><<<residual_grid(G.mi, G.nj), 256, 0, st>>>(G, u, v, T, p, u_ant, fcon, flin, resu, ns);
-  else
-    residual_kernel<double, false><<<residual_grid(G.mi, G.nj), 256, 0, st>>>(G, u, v, T, p, u_ant, fcon, flin, resu, ns);
-  return cudaGetLastError();
+  const int grid = residual_grid(G.mi, G.nj);
+  if (fast) return launch_k(residual_kernel<double, true>, grid, 256, 0, st, G, u, v, T, p, u_ant, fcon, flin, resu, ns);
+  return launch_k(residual_kernel<double, false>, grid, 256, 0, st, G, u, v, T, p, u_ant, fcon, flin, resu, ns);
 }
 
 cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,

@@ -105,6 +105,7 @@ __device__ __forceinline__ double solve_group(S* sm, const SolveIO& io, const in
 template <class S, bool X, bool DC, bool EXACT, int TL, int G, int M>
 __global__ void __launch_bounds__(TL * G) solve_kernel(const SolveIO io, const int n, const int line_lo,
                                                        const int line_hi, const int nfull) {
+  IXB_PDL_ENTRY();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const double acc = solve_group<S, X, DC, EXACT, TL, G, M>(reinterpret_cast<S*>(smem_raw), io, n, line_lo, line_hi,
                                                             nfull, 1 + blockIdx.x * TL);
@@ -121,6 +122,7 @@ template <class S, bool X, bool DC, bool EXACT, int TL, int G>
 __global__ void __launch_bounds__(TL * G) solve_batch_kernel(const SolveInst* __restrict__ inst,
                                                              const int2* __restrict__ items, const int nitems,
                                                              const int* __restrict__ active, const BatchNorm bn) {
+  IXB_PDL_ENTRY();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 wi = items[it];
@@ -142,12 +144,10 @@ struct SolveSet {
 #define IXB_CASE_(TL_, G_)                                                                                    \
   if (s.tl == TL_ && s.g == G_) {                                                                             \
     if (!EXACT && s.m == 3)                                                                                   \
-      solve_kernel<S, X, DC, EXACT, TL_, G_, 3><<<s.grid, TL_ * G_, s.smem, st>>>(io, s.n, s.line_lo,         \
-                                                                                  s.line_hi, s.nfull);        \
-    else                                                                                                      \
-      solve_kernel<S, X, DC, EXACT, TL_, G_, 0><<<s.grid, TL_ * G_, s.smem, st>>>(io, s.n, s.line_lo,         \
-                                                                                  s.line_hi, s.nfull);        \
-    return cudaGetLastError();                                                                                \
+      return launch_k(solve_kernel<S, X, DC, EXACT, TL_, G_, 3>, s.grid, TL_ * G_, s.smem, st, io, s.n,       \
+                      s.line_lo, s.line_hi, s.nfull);                                                         \
+    return launch_k(solve_kernel<S, X, DC, EXACT, TL_, G_, 0>, s.grid, TL_ * G_, s.smem, st, io, s.n,         \
+                    s.line_lo, s.line_hi, s.nfull);                                                           \
   }
     IXB_SWEEP_SHAPES(IXB_CASE_)
 #undef IXB_CASE_
@@ -183,8 +183,7 @@ struct SolveSet {
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;  \
     if (per_sm < 1) return cudaErrorInvalidValue;                                                          \
     const int grid = std::max(1, std::min(nitems, per_sm * nsm));                                          \
-    k<<<grid, TL_ * G_, smem, st>>>(inst, items, nitems, active, bn);                                      \
-    return cudaGetLastError();                                                                             \
+    return launch_k(k, grid, TL_ * G_, smem, st, inst, items, nitems, active, bn);                         \
   }
     IXB_SWEEP_SHAPES(IXB_BCASE_)
 #undef IXB_BCASE_

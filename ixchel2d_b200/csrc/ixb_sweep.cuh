@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(kAsmThreads)
     assemble_kernel(const Geo<typename SweepTypes<SOLVER, EQ>::A> G_, const SweepIO<double> io,
                     const Coef<typename SweepTypes<SOLVER, EQ>::S> co, const int n, const int line_lo,
                     const int line_hi) {
+  IXB_PDL_ENTRY();
   using S = typename SweepTypes<SOLVER, EQ>::S;
   __shared__ S tile_s[4][kAsmYR][kAsmYL + 1];
   const int ntiles = asm_tiles(EqIsX<EQ>::value, n, line_hi - line_lo + 1);
@@ -199,6 +200,7 @@ __global__ void __launch_bounds__(kAsmThreads)
                               __restrict__ inst,
                           const int2* __restrict__ items, const int nitems, const int* __restrict__ active,
                           const BatchNorm bn) {
+  IXB_PDL_ENTRY();
   using S = typename SweepTypes<SOLVER, EQ>::S;
   __shared__ S tile_s[4][kAsmYR][kAsmYL + 1];
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -216,9 +218,8 @@ cudaError_t assemble_batch_launch(const void* inst, const int2* items, int nitem
                                   const BatchNorm& bn, cudaStream_t st) {
   using ST = SweepTypes<SOLVER, EQ>;
   const int grid = std::max(1, std::min(nitems, kAsmGridCap * 4));
-  assemble_batch_kernel<EQ, SOLVER><<<grid, kAsmThreads, 0, st>>>(
-      static_cast<const AsmInst<typename ST::A, typename ST::S>*>(inst), items, nitems, active, bn);
-  return cudaGetLastError();
+  return launch_k(assemble_batch_kernel<EQ, SOLVER>, grid, kAsmThreads, 0, st,
+                  static_cast<const AsmInst<typename ST::A, typename ST::S>*>(inst), items, nitems, active, bn);
 }
 
 template <int EQ, int SOLVER>
@@ -233,8 +234,7 @@ cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& Gd, const Ge
   co.P = buf.P;
   const int tiles = asm_tiles(EqIsX<EQ>::value, s.n, s.line_hi - s.line_lo + 1);
   const int grid = std::max(1, std::min(tiles, kAsmGridCap));
-  assemble_kernel<EQ, SOLVER><<<grid, kAsmThreads, 0, st>>>(Gm, io, co, s.n, s.line_lo, s.line_hi);
-  return cudaGetLastError();
+  return launch_k(assemble_kernel<EQ, SOLVER>, grid, kAsmThreads, 0, st, Gm, io, co, s.n, s.line_lo, s.line_hi);
 }
 
 }  // namespace ixb
