@@ -541,6 +541,41 @@ def run_profile_phases(prec):
     sim.close()
 
 
+def run_profile_adi():
+    """Profiling driver: one launch of each batched line solve of the
+    microbenchmark (contiguous f64, contiguous f32, interleaved f64,
+    interleaved f32; 4096 systems x 4096 unknowns)."""
+    import torch
+    from ixchel2d_b200 import _ffi as F
+    n = nsys = 4096
+    gen = torch.Generator(device="cuda").manual_seed(1234)
+    for layout in (0, 1):
+        for dt, fn in ((torch.float64, F.lib.ixb_tridiag_f64), (torch.float32, F.lib.ixb_tridiag_f32)):
+            a = -torch.rand((nsys, n), generator=gen, device="cuda", dtype=dt)
+            c = -torch.rand((nsys, n), generator=gen, device="cuda", dtype=dt)
+            b = a.abs() + c.abs() + 0.1 + 0.9 * torch.rand((nsys, n), generator=gen, device="cuda", dtype=dt)
+            d = 2 * torch.rand((nsys, n), generator=gen, device="cuda", dtype=dt) - 1
+            x = torch.empty_like(d)
+            F.check(fn(a.data_ptr(), b.data_ptr(), c.data_ptr(), d.data_ptr(), x.data_ptr(), n, nsys, layout,
+                       F.SOLVER_HYBRID, torch.cuda.current_stream().cuda_stream), "ixb_tridiag")
+            torch.cuda.synchronize()
+            del a, b, c, d, x
+
+
+def run_profile_batch():
+    """Profiling driver: 64 natural-convection cavities (side 64..512, Ra
+    1e3..1e6, seed 1234), refined form, default shapes, two batched outer
+    iterations (run with IXB_NO_GRAPH=1 so that ncu sees the kernels)."""
+    from ixchel2d_b200 import Batch, cases
+    rng = np.random.default_rng(1234)
+    sides = rng.integers(64, 513, 64)
+    ras = 10.0 ** rng.uniform(3.0, 6.0, 64)
+    bt = Batch.from_cases([cases.natural_cavity(int(a), int(a), Ra=float(r), T0=0.5) for a, r in zip(sides, ras)],
+                          conv_paso=0.0)
+    bt.iterate(2)
+    bt.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -552,9 +587,17 @@ def main():
     ap.add_argument("--prec", type=int, default=1, help="precision mode of --profile-phases (0 fp64, 1 refined)")
     ap.add_argument("--shapes", help="JSON of sweep launch shapes (from --save-shapes) instead of autotuning")
     ap.add_argument("--save-shapes", help="write the autotuned sweep launch shapes to this JSON file")
+    ap.add_argument("--profile-adi", action="store_true", help="run the line-solve profiling driver")
+    ap.add_argument("--profile-batch", action="store_true", help="run the batched-cavities profiling driver")
     args = ap.parse_args()
     if args.profile_phases:
         run_profile_phases(args.prec)
+        return
+    if args.profile_adi:
+        run_profile_adi()
+        return
+    if args.profile_batch:
+        run_profile_batch()
         return
     if args.warmup < 3:
         args.warmup = 3

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <type_traits>
@@ -80,6 +81,7 @@ struct ixb_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool dirty = true;
+  bool use_graph = true;  // IXB_NO_GRAPH=1: host-driven loop (one sync per iteration)
 };
 
 namespace {
@@ -305,7 +307,7 @@ __device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
 // (main.f90:1202-1215), then the loop condition = any instance active and
 // budget left.
 __global__ void batch_ctl_kernel(BInst* inst, int* active, const double* results, int count, BCtl* ctl,
-                                 cudaGraphConditionalHandle cond) {
+                                 cudaGraphConditionalHandle cond, int in_graph) {
   IXB_PDL_ENTRY();
   int any = 0;
   for (int i = threadIdx.x; i < count; i += blockDim.x) {
@@ -335,8 +337,8 @@ __global__ void batch_ctl_kernel(BInst* inst, int* active, const double* results
     if (!go)
       for (int i = 0; i < count; ++i)
         if (active[i] && inst[i].exit_code == 0) inst[i].exit_code = 2;
-    ctl->any_active = any;
-    cudaGraphSetConditional(cond, go ? 1u : 0u);
+    ctl->any_active = go;
+    if (in_graph) cudaGraphSetConditional(cond, go ? 1u : 0u);
   }
 }
 
@@ -377,7 +379,7 @@ int build_graph(ixb_batch* b) {
   int st = body(b);
   if (st == IXB_OK) {
     if (launch_k(batch_ctl_kernel, 1, 256, 0, b->stream, b->inst_d, b->active, (const double*)b->results, b->count,
-                 b->ctl_d, cond) != cudaSuccess)
+                 b->ctl_d, cond, 1) != cudaSuccess)
       st = IXB_ECUDA;
   }
   cudaGraph_t captured;
@@ -389,9 +391,9 @@ int build_graph(ixb_batch* b) {
 }
 
 int ensure_ready(ixb_batch* b) {
-  if (!b->dirty && b->exec) return IXB_OK;
+  if (!b->dirty && (b->exec || !b->use_graph)) return IXB_OK;
   BTRY(build_tables(b));
-  BTRY(build_graph(b));
+  if (b->use_graph) BTRY(build_graph(b));
   b->dirty = false;
   return IXB_OK;
 }
@@ -436,6 +438,8 @@ int ixb_batch_create(int count, const int* mi, const int* nj, int prec_mode, ixb
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return fail(IXB_ECUDA);
+  const char* env = std::getenv("IXB_NO_GRAPH");
+  if (env && env[0] == '1') b->use_graph = false;
   *out = b;
   return IXB_OK;
 }
@@ -576,7 +580,17 @@ int ixb_batch_iterate(ixb_batch* b, int max_iters, int* n_active) {
   b->ctl_h->budget = max_iters;
   b->ctl_h->any_active = 0;
   BCK(cudaMemcpyAsync(b->ctl_d, b->ctl_h, sizeof(BCtl), cudaMemcpyHostToDevice, b->stream));
-  if (max_iters > 0) BCK(cudaGraphLaunch(b->exec, b->stream));
+  if (max_iters > 0 && b->use_graph) BCK(cudaGraphLaunch(b->exec, b->stream));
+  if (max_iters > 0 && !b->use_graph) {  // the same kernels driven from the host
+    for (;;) {
+      BTRY(body(b));
+      BCK(launch_k(batch_ctl_kernel, 1, 256, 0, b->stream, b->inst_d, b->active, (const double*)b->results, b->count,
+                   b->ctl_d, cudaGraphConditionalHandle{}, 0));
+      BCK(cudaMemcpyAsync(b->ctl_h, b->ctl_d, sizeof(BCtl), cudaMemcpyDeviceToHost, b->stream));
+      BCK(cudaStreamSynchronize(b->stream));
+      if (!b->ctl_h->any_active) break;
+    }
+  }
   BCK(cudaMemcpyAsync(b->inst_h, b->inst_d, b->count * sizeof(BInst), cudaMemcpyDeviceToHost, b->stream));
   std::vector<int> act(b->count);
   BCK(cudaMemcpyAsync(act.data(), b->active, b->count * sizeof(int), cudaMemcpyDeviceToHost, b->stream));

@@ -106,3 +106,16 @@ def test_batch_rejects_bad_sizes():
     nj = (C.c_int * 2)(64, 64)
     b = C.c_void_p()
     assert F.lib.ixb_batch_create(2, mi, nj, F.PREC_FP64, C.byref(b)) == F.EINVAL
+
+
+def test_batch_host_driven_loop_matches_graph(monkeypatch):
+    cs = _mixed_cases()[:3]
+    g = Batch.from_cases(cs, prec=F.PREC_FP32_REFINED, conv_paso=0.0)
+    monkeypatch.setenv("IXB_NO_GRAPH", "1")
+    h = Batch.from_cases(cs, prec=F.PREC_FP32_REFINED, conv_paso=0.0)
+    assert g.iterate(12) == 3 and h.iterate(12) == 3
+    for i in range(3):
+        a, b = g[i].download(), h[i].download()
+        for k in STATE:
+            assert np.array_equal(a[k], b[k]), (i, k)
+        assert h.report(i)["n_simple"] == 12
