@@ -260,6 +260,34 @@ int ixb_batch_iterate(ixb_batch* b, int max_iters, int* n_active);
  * by the iteration budget, 3 non-finite norm (status IXB_ENONFINITE). */
 int ixb_batch_report(ixb_batch* b, int i, ixb_report* out);
 
+/* ---- mesh generation and mesh/state files (host only, no GPU needed) ---- */
+#define IXB_MESH_UNIF 0 /* malla/malla_irr.f90:97-100 */
+#define IXB_MESH_TUBO 1 /* erf clustering at both walls, malla_irr.f90:81-89 */
+#define IXB_MESH_CENT 2 /* sinh clustering around `centre` (tau = param), malla_irr.f90:54-64 */
+#define IXB_MESH_TANH 3 /* two-sided tanh wall clustering, parameter = stretching; no counterpart
+                           in malla_irr.f90 */
+/* n u- (or v-) node coordinates of one axis on [0, length]. */
+int ixb_mesh_axis(int kind, int n, double length, double param, double centre, double* nodes);
+/* Staggered mesh of malla_irr.f90: xu (mi), yv (nj) from ixb_mesh_axis (the
+ * cent kind centred on the middle of the axis), p nodes xp (mi+1), yp (nj+1)
+ * at the midpoints plus one node half a cell outside each wall (:66-77,
+ * :101-106); every coordinate rounded to 15 significant digits, as the
+ * D23.15 mesh files hold them. */
+int ixb_staggered_mesh(int mi, int nj, int xkind, double xparam, int ykind, double yparam, double ao, double bo,
+                       double* xu, double* yv, double* xp, double* yp);
+/* The three mesh/state files (written by malla_irr.f90:176-203, read by
+ * lectura_mallas_escalonadas, source/mod_malla.f90:137-162): header
+ * "i_0 i_1 iter a", then per node (DO jj, DO ii) "x y u" (u file), "x y v"
+ * (v file), "x y T p" (p file) in D23.15.  Arrays in the Fortran shapes
+ * u(mi,nj+1), v(mi+1,nj), T/p(mi+1,nj+1), column-major.  Returns IXB_EIO when a
+ * file cannot be opened, written or parsed. */
+int ixb_write_state_files(const char* ufile, const char* vfile, const char* pfile, int mi, int nj, const double* xu,
+                          const double* yv, const double* xp, const double* yp, const double* u, const double* v,
+                          const double* T, const double* p, int i0, int i1, int iter, double a);
+int ixb_read_state_files(const char* ufile, const char* vfile, const char* pfile, int mi, int nj, double* xu,
+                         double* yv, double* xp, double* yp, double* u, double* v, double* T, double* p, int* i0,
+                         int* i1, int* iter, double* a);
+
 /* ---- host-side inputs (no GPU needed) ---- */
 /* lectura_cond_frontera index rule (source/mod_cond_frontera.f90:114-238):
  * for side 0/2 ('a'/'c') the divisions are located on `yy` (nn entries), for

@@ -20,6 +20,7 @@ PREC_FP64, PREC_FP32_REFINED = 0, 1
 SOLVER_HYBRID, SOLVER_EXACT = 0, 1
 VAR_U, VAR_V, VAR_T = 0, 1, 2
 BC_OTHER, BC_DIRI, BC_NEUM = 0, 1, 2
+MESH_UNIF, MESH_TUBO, MESH_CENT, MESH_TANH = 0, 1, 2, 3
 
 
 class Params(C.Structure):
@@ -97,6 +98,13 @@ SIGNATURES = [
     ("ixb_batch_restart", C.c_int, [_vp]),
     ("ixb_batch_iterate", C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
     ("ixb_batch_report", C.c_int, [_vp, C.c_int, C.POINTER(Report)]),
+    ("ixb_mesh_axis", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _vp]),
+    ("ixb_staggered_mesh", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,
+                                     C.c_double, _vp, _vp, _vp, _vp]),
+    ("ixb_write_state_files", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_int] + [_vp] * 8 +
+     [C.c_int, C.c_int, C.c_int, C.c_double]),
+    ("ixb_read_state_files", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_int] + [_vp] * 8 +
+     [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     ("ixb_bc_locate", C.c_int, [C.c_int, C.c_int, _dp, C.POINTER(C.c_int), _dp, _dp, C.c_int, _dp, C.c_int,
                                 C.POINTER(BCSide)]),
     ("ixb_read_bc_file", C.c_int, [C.c_char_p, _dp, C.c_int, _dp, C.c_int, C.POINTER(BCSide)]),

@@ -79,11 +79,17 @@ bool ListReader::read(std::vector<std::string>& items, int count) {
   return true;
 }
 
+// A Fortran real: D or E exponents, and the exponent-letter-free form that
+// Dw.d / Ew.d output takes for |exponent| > 99 ("0.25-120").
 bool parse_real(const std::string& t, double* out) {
   std::string s = t;
   for (auto& ch : s)
     if (ch == 'd' || ch == 'D') ch = 'e';
   if (s.empty()) return false;
+  if (s.find_first_of("eE") == std::string::npos) {
+    const size_t k = s.find_first_of("+-", 1);
+    if (k != std::string::npos && (std::isdigit((unsigned char)s[k - 1]) || s[k - 1] == '.')) s.insert(k, 1, 'e');
+  }
   char* end = nullptr;
   const double v = std::strtod(s.c_str(), &end);
   if (end == s.c_str() || *end != '\0') return false;
