@@ -19,6 +19,7 @@ module ixb
   integer(c_int), parameter :: IXB_SOLVER_HYBRID = 0, IXB_SOLVER_EXACT = 1
   integer(c_int), parameter :: IXB_VAR_U = 0, IXB_VAR_V = 1, IXB_VAR_T = 2
   integer(c_int), parameter :: IXB_BC_OTHER = 0, IXB_BC_DIRI = 1, IXB_BC_NEUM = 2
+  integer(c_int), parameter :: IXB_MESH_UNIF = 0, IXB_MESH_TUBO = 1, IXB_MESH_CENT = 2, IXB_MESH_TANH = 3
 
   type, bind(C) :: ixb_params
      real(c_double) :: gamma_momen, gamma_energ, Ri, Riy, dt
@@ -120,6 +121,84 @@ module ixb
        integer(c_int), value :: mm, nn
        type(ixb_bc_side), intent(out) :: sides(4)
      end function ixb_read_bc_file
+     integer(c_int) function ixb_simple_iterations(h, n, rep) bind(C, name="ixb_simple_iterations")
+       import :: c_int, c_ptr, ixb_report
+       type(c_ptr), value :: h
+       integer(c_int), value :: n
+       type(ixb_report), intent(out) :: rep
+     end function ixb_simple_iterations
+
+     integer(c_int) function ixb_nusselt_x(h, j0, j1, nu0, nu1) bind(C, name="ixb_nusselt_x")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: j0, j1
+       real(c_double), intent(out) :: nu0, nu1
+     end function ixb_nusselt_x
+
+     integer(c_int) function ixb_staggered_mesh(mi, nj, xkind, xparam, ykind, yparam, ao, bo, xu, yv, xp, yp) &
+          bind(C, name="ixb_staggered_mesh")
+       import :: c_int, c_double
+       integer(c_int), value :: mi, nj, xkind, ykind
+       real(c_double), value :: xparam, yparam, ao, bo
+       real(c_double), intent(out) :: xu(*), yv(*), xp(*), yp(*)
+     end function ixb_staggered_mesh
+
+     integer(c_int) function ixb_read_state_files(ufile, vfile, pfile, mi, nj, xu, yv, xp, yp, u, v, T, p, &
+          i0, i1, iter, a) bind(C, name="ixb_read_state_files")
+       import :: c_int, c_char, c_double
+       character(kind=c_char), intent(in) :: ufile(*), vfile(*), pfile(*)
+       integer(c_int), value :: mi, nj
+       real(c_double), intent(out) :: xu(*), yv(*), xp(*), yp(*), u(*), v(*), T(*), p(*)
+       integer(c_int), intent(out) :: i0, i1, iter
+       real(c_double), intent(out) :: a
+     end function ixb_read_state_files
+
+     integer(c_int) function ixb_write_state_files(ufile, vfile, pfile, mi, nj, xu, yv, xp, yp, u, v, T, p, &
+          i0, i1, iter, a) bind(C, name="ixb_write_state_files")
+       import :: c_int, c_char, c_double
+       character(kind=c_char), intent(in) :: ufile(*), vfile(*), pfile(*)
+       integer(c_int), value :: mi, nj, i0, i1, iter
+       real(c_double), intent(in) :: xu(*), yv(*), xp(*), yp(*), u(*), v(*), T(*), p(*)
+       real(c_double), value :: a
+     end function ixb_write_state_files
+
+     integer(c_int) function ixb_batch_create(count, mi, nj, prec_mode, b) bind(C, name="ixb_batch_create")
+       import :: c_int, c_ptr
+       integer(c_int), value :: count, prec_mode
+       integer(c_int), intent(in) :: mi(*), nj(*)
+       type(c_ptr) :: b
+     end function ixb_batch_create
+
+     integer(c_int) function ixb_batch_destroy(b) bind(C, name="ixb_batch_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: b
+     end function ixb_batch_destroy
+
+     integer(c_int) function ixb_batch_instance(b, i, h) bind(C, name="ixb_batch_instance")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: b
+       integer(c_int), value :: i
+       type(c_ptr) :: h
+     end function ixb_batch_instance
+
+     integer(c_int) function ixb_batch_restart(b) bind(C, name="ixb_batch_restart")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: b
+     end function ixb_batch_restart
+
+     integer(c_int) function ixb_batch_iterate(b, max_iters, n_active) bind(C, name="ixb_batch_iterate")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: b
+       integer(c_int), value :: max_iters
+       integer(c_int), intent(out) :: n_active
+     end function ixb_batch_iterate
+
+     integer(c_int) function ixb_batch_report(b, i, rep) bind(C, name="ixb_batch_report")
+       import :: c_int, c_ptr, ixb_report
+       type(c_ptr), value :: b
+       integer(c_int), value :: i
+       type(ixb_report), intent(out) :: rep
+     end function ixb_batch_report
   end interface
 
 end module ixb
