@@ -17,6 +17,7 @@
 #include <new>
 #include <vector>
 
+#include "ixb_ctl.cuh"
 #include "ixb_handle.h"
 
 using namespace ixb;
@@ -159,28 +160,28 @@ SweepIO<double> sweep_io(ixb_handle* h, int eq, const double* prev, bool with_no
 }
 
 // Launch one sweep reading field buffers `cur` and writing `cur^1`.
-int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm) {
+int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm, const CtlRef& ctl = CtlRef{}) {
   Geo<double> G = make_geo(h);
   if (h->shape_tl[eq] == 0) pick_shape(h, eq);
   SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), h->shape_tl[eq], h->shape_g[eq]);
   const SweepIO<double> io = sweep_io(h, eq, prev, with_norm);
   const Geo<float> Gf = h->metrics32 ? make_geo32(h) : Geo<float>{};
   const StageBuf stage{h->stage, h->stage_stride, h->stage_P};
-  CK(launch_sweep_f64(eq, solver_form(h), s, G, Gf, io, stage, h->stream));
+  CK(launch_sweep_f64(eq, solver_form(h), s, G, Gf, io, stage, h->stream, ctl));
   return IXB_OK;
 }
 
-int correct(ixb_handle* h) {
+int correct(ixb_handle* h, const CtlRef& gate = CtlRef{}) {
   Geo<double> G = make_geo(h);
   CK(launch_correct_f64(G, h->u[h->cu], h->v[h->cv], h->p, h->pc[h->cpc], h->au, h->av,
-                         h->prm.solver == IXB_SOLVER_HYBRID, h->stream));
+                         h->prm.solver == IXB_SOLVER_HYBRID, h->stream, gate));
   return IXB_OK;
 }
 
-int residual(ixb_handle* h) {
+int residual(ixb_handle* h, const CtlRef& outer = CtlRef{}) {
   Geo<double> G = make_geo(h);
   CK(launch_residual_f64(G, h->u[h->cu], h->v[h->cv], h->T[h->cT], h->p, h->u_ant, h->fcon[0], h->flin[0],
-                         h->resu, slot(h, N_RES), h->prm.solver == IXB_SOLVER_HYBRID, h->stream));
+                         h->resu, slot(h, N_RES), h->prm.solver == IXB_SOLVER_HYBRID, h->stream, outer));
   return IXB_OK;
 }
 
@@ -264,63 +265,14 @@ int body_host(ixb_handle* h, bool outer_test, ixb_report* rep, int* exit_code) {
 // ---------------------------------------------------------------------------
 // graph-driven loop: control kernels set the WHILE conditions
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
-
 __global__ void ctl_begin_kernel(Ctl* c, cudaGraphConditionalHandle outer) {
   IXB_PDL_ENTRY();
   cudaGraphSetConditional(outer, 1u);
   c->outer_done = 0;
+  c->inner_done = 0;
   c->exit_code = 0;
   c->status = 0;
   c->n_simple = c->n_momen = c->n_pres = c->n_ener = 0;
-}
-
-__global__ void ctl_inner_kernel(Ctl* c, const double* norms, int which, cudaGraphConditionalHandle inner) {
-  IXB_PDL_ENTRY();
-  // which: 0 momentum (N_DV vs conv_u), 1 pressure (N_DP vs conv_p), 2 energy (N_DT vs conv_t)
-  double err, conv;
-  if (which == 0) { err = norms[N_DV]; conv = c->conv_u; c->err_u = err; c->n_momen++; }
-  else if (which == 1) { err = norms[N_DP]; conv = c->conv_p; c->err_p = err; c->maxbo = norms[N_BO]; c->n_pres++; }
-  else { err = norms[N_DT]; conv = c->conv_t; c->err_t = err; c->n_ener++; }
-  bool again;
-  c->inner_done++;
-  if (!finite_d(err) || (which == 1 && !finite_d(norms[N_BO]))) {
-    c->status = IXB_ENONFINITE;  // the outer control kernel ends the loop
-    again = false;
-  } else if (err < conv) { c->iter_ecuaci = 0; again = false; }
-  else if (c->iter_ecuaci > c->iter_ecuaci_max) { c->iter_ecuaci = 0; again = false; }
-  else { c->iter_ecuaci++; again = true; }
-  // the reference's counter logic bounds a loop by iter_ecuaci_max + 2
-  // passes; enforce it independently so no WHILE node can run away
-  if (again && (long long)c->inner_done >= (long long)c->iter_ecuaci_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
-  cudaGraphSetConditional(inner, again ? 1u : 0u);
-}
-
-// Gate: after a non-finite stop, later inner loops of the same pass must not
-// start.  Sets the inner loop's initial condition.
-__global__ void ctl_gate_kernel(Ctl* c, cudaGraphConditionalHandle inner) {
-  IXB_PDL_ENTRY();
-  c->inner_done = 0;
-  cudaGraphSetConditional(inner, c->status == 0 ? 1u : 0u);
-}
-
-__global__ void ctl_outer_kernel(Ctl* c, const double* norms, cudaGraphConditionalHandle outer) {
-  IXB_PDL_ENTRY();
-  if (c->status != 0) { cudaGraphSetConditional(outer, 0); return; }
-  c->residuo = norms[N_RES];
-  c->n_simple++;
-  c->outer_done++;
-  if (!finite_d(c->residuo)) { c->status = IXB_ENONFINITE; cudaGraphSetConditional(outer, 0); return; }
-  if (c->fixed_count > 0) {
-    cudaGraphSetConditional(outer, c->outer_done < c->fixed_count ? 1u : 0u);
-    return;
-  }
-  bool again;
-  if (c->maxbo < c->conv_paso && c->residuo < c->conv_resi) { c->iter_simple = 0; c->exit_code = 1; again = false; }
-  else if (c->iter_simple > c->iter_simple_max) { c->iter_simple = 0; c->exit_code = 2; again = false; }
-  else { c->iter_simple++; again = true; }
-  if (again && (long long)c->outer_done >= (long long)c->iter_simple_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
-  cudaGraphSetConditional(outer, again ? 1u : 0u);
 }
 
 // Add a WHILE node to `g` after `dep` and return its body graph.
@@ -379,58 +331,46 @@ int build_graph(ixb_handle* h) {
   }, &n_begin));
   cudaGraph_t outer_body;
   TRY(add_while(h, g, &n_begin, c_outer, &outer_body, &n_outer));
-  CK(cudaGraphConditionalHandleCreate(&c_mom, outer_body, 1, 0));
+  CK(cudaGraphConditionalHandleCreate(&c_mom, outer_body, 1, cudaGraphCondAssignDefault));
   CK(cudaGraphConditionalHandleCreate(&c_pres, outer_body, 1, 0));
   CK(cudaGraphConditionalHandleCreate(&c_ener, outer_body, 1, 0));
-  // outer body: gate(mom) -> WHILE(mom) -> memset p' + gate(pres) -> WHILE(pres)
-  //             -> correct + gate(ener) -> WHILE(ener) -> residual + ctl_outer
-  cudaGraphNode_t last, wn;
+  // outer body: WHILE(mom) -> p' reset + gate(pres) -> WHILE(pres) -> correct + gate(ener)
+  //             -> WHILE(ener) -> residual + outer test.  The kernel that finishes a loop's norm
+  //             applies its exit test (ixb_ctl.cuh); the momentum loop is opened by the outer
+  //             test of the previous pass and, for the first pass, by the handle's default.
+  cudaGraphNode_t last = nullptr, wn;
   cudaGraph_t b;
-  TRY(capture_into(h, outer_body, nullptr, [&]() {
-    if (launch_k(ctl_gate_kernel, 1, 1, 0, h->stream, h->ctl_d, c_mom) != cudaSuccess) return IXB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
-  }, &last));
-  TRY(add_while(h, outer_body, &last, c_mom, &b, &wn));
+  const double* nrm = h->norms;
+  TRY(add_while(h, outer_body, nullptr, c_mom, &b, &wn));
   TRY(capture_into(h, b, nullptr, [&]() {
     TRY(sweep(h, EQ_UY, nullptr, false));
     TRY(sweep(h, EQ_UX, nullptr, false));
     const double* v_start = h->v[h->cv];
     TRY(sweep(h, EQ_VY, nullptr, false));
-    TRY(sweep(h, EQ_VX, v_start, true));
-    if (launch_k(ctl_inner_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, 0, c_mom) != cudaSuccess) return IXB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+    TRY(sweep(h, EQ_VX, v_start, true, CtlRef{h->ctl_d, nrm, c_mom, 0, 0}));
+    return IXB_OK;
   }, &last));
   TRY(capture_into(h, outer_body, &wn, [&]() {
-    if (cudaMemsetAsync(h->pc[h->cpc], 0, h->fsz * sizeof(double), h->stream) != cudaSuccess) return IXB_ECUDA;
-    if (launch_k(ctl_gate_kernel, 1, 1, 0, h->stream, h->ctl_d, c_pres) != cudaSuccess) return IXB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+    return launch_preset_f64(h->pc[h->cpc], h->fsz, CtlRef{h->ctl_d, nrm, c_pres, 0, 0}, h->stream) == cudaSuccess
+               ? IXB_OK : IXB_ECUDA;
   }, &last));
   TRY(add_while(h, outer_body, &last, c_pres, &b, &wn));
   TRY(capture_into(h, b, nullptr, [&]() {
     const double* pc_start = h->pc[h->cpc];
     TRY(sweep(h, EQ_PY, nullptr, false));
-    TRY(sweep(h, EQ_PX, pc_start, true));
-    if (launch_k(ctl_inner_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, 1, c_pres) != cudaSuccess) return IXB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+    TRY(sweep(h, EQ_PX, pc_start, true, CtlRef{h->ctl_d, nrm, c_pres, 0, 1}));
+    return IXB_OK;
   }, &last));
-  TRY(capture_into(h, outer_body, &wn, [&]() {
-    TRY(correct(h));
-    if (launch_k(ctl_gate_kernel, 1, 1, 0, h->stream, h->ctl_d, c_ener) != cudaSuccess) return IXB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
-  }, &last));
+  TRY(capture_into(h, outer_body, &wn, [&]() { return correct(h, CtlRef{h->ctl_d, nrm, c_ener, 0, 0}); }, &last));
   TRY(add_while(h, outer_body, &last, c_ener, &b, &wn));
   TRY(capture_into(h, b, nullptr, [&]() {
     const double* t_start = h->T[h->cT];
     TRY(sweep(h, EQ_TY, nullptr, false));
-    TRY(sweep(h, EQ_TX, t_start, true));
-    if (launch_k(ctl_inner_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, 2, c_ener) != cudaSuccess) return IXB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+    TRY(sweep(h, EQ_TX, t_start, true, CtlRef{h->ctl_d, nrm, c_ener, 0, 2}));
+    return IXB_OK;
   }, &last));
-  TRY(capture_into(h, outer_body, &wn, [&]() {
-    TRY(residual(h));
-    if (launch_k(ctl_outer_kernel, 1, 1, 0, h->stream, h->ctl_d, (const double*)h->norms, c_outer) != cudaSuccess) return IXB_ECUDA;
-    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
-  }, &last));
+  TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
+                   &last));
   CK(cudaGraphInstantiate(&h->graph_exec, g, 0));
   h->cu = cu; h->cv = cv; h->cT = cT; h->cpc = cpc;
   h->graph_dirty = false;

@@ -37,6 +37,19 @@ inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t s
 
 enum NormId { N_DV = 0, N_DP, N_BO, N_DT, N_RES, N_COUNT };
 
+// Loop control carried by a kernel of the graph-driven SIMPLE loop (ctl
+// null: none, as in the host-driven loop): the kernel that finishes a norm
+// applies the exit test that reads it and sets the loop's conditional node
+// (ixb_ctl.cuh).
+struct Ctl;
+struct CtlRef {
+  Ctl* ctl;
+  const double* norms;
+  cudaGraphConditionalHandle cond;   // the loop this kernel ends or opens
+  cudaGraphConditionalHandle cond2;  // outer step: the momentum loop to reopen
+  int which;                         // inner step: 0 momentum, 1 pressure, 2 energy
+};
+
 // Line-solve forms of the sweep kernels: IXB_SOLVER_HYBRID (0) and
 // IXB_SOLVER_EXACT (1) of the public ABI, plus the mixed-precision form a
 // handle created with IXB_PREC_FP32_REFINED runs in place of the hybrid one.
@@ -140,6 +153,7 @@ struct SolveIO {
   double* out;          // swept field, new values
   const double* prev;   // field at the start of the inner pass (null: zero)
   NormSlot nrm0;        // ||out - prev|| over interior rows of solved lines
+  CtlRef ctl;           // inner-loop test after nrm0 (graph only)
   int LD;
   int m, mp;            // chunk rows per thread, padded pitch
 };
@@ -180,12 +194,16 @@ cudaError_t residual_batch_launch(const CellInst* inst, const int2* items, int n
 // kernel launchers (ixb_kernels.cu); return cudaError_t
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
                              const Geo<float>& Gf, const SweepIO<double>& io, const StageBuf& buf,
-                             cudaStream_t st);
+                             cudaStream_t st, const CtlRef& ctl = CtlRef{});
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
-                               const double* au, const double* av, int fast, cudaStream_t st);
+                               const double* au, const double* av, int fast, cudaStream_t st,
+                               const CtlRef& gate = CtlRef{});
 cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const double* v, const double* T,
                                 const double* p, const double* u_ant, const double* fcon, const double* flin,
-                                double* resu, NormSlot ns, int fast, cudaStream_t st);
+                                double* resu, NormSlot ns, int fast, cudaStream_t st,
+                                const CtlRef& outer = CtlRef{});
+// p' = 0 over a whole field, opening the pressure loop (graph only)
+cudaError_t launch_preset_f64(double* pc, size_t n, const CtlRef& gate, cudaStream_t st);
 int residual_grid(int mi, int nj);
 cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,
                                int vertical, int k0, int k1, double* out2, cudaStream_t st);

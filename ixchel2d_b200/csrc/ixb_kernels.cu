@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdlib>
 
+#include "ixb_ctl.cuh"
 #include "ixb_internal.h"
 #include "ixb_reduce.cuh"
 
@@ -102,10 +103,20 @@ __device__ __forceinline__ void correct_cell(const Geo<R>& G, R* __restrict__ u,
 
 template <class R, bool FAST>
 __global__ void correct_kernel(const Geo<R> G, R* __restrict__ u, R* __restrict__ v, R* __restrict__ p,
-                               const R* __restrict__ pc, const R* __restrict__ au, const R* __restrict__ av) {
+                               const R* __restrict__ pc, const R* __restrict__ au, const R* __restrict__ av,
+                               const CtlRef gate) {
   IXB_PDL_ENTRY();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx < (G.mi - 1) * (G.nj - 1)) correct_cell<R, FAST>(G, u, v, p, pc, au, av, idx);
+  if (gate.ctl && idx == 0) ctl_gate_step(gate.ctl, gate.cond);  // opens the energy loop
+}
+
+// p' reset at the start of the pressure loop (main.f90:752-758), opening it
+__global__ void preset_kernel(double* __restrict__ pc, size_t n, const CtlRef gate) {
+  IXB_PDL_ENTRY();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    pc[i] = 0.0;
+  if (gate.ctl && blockIdx.x == 0 && threadIdx.x == 0) ctl_gate_step(gate.ctl, gate.cond);
 }
 
 // ---------------------------------------------------------------------------
@@ -116,7 +127,7 @@ __global__ void __launch_bounds__(256) residual_kernel(const Geo<R> G, const R* 
                                                        const R* __restrict__ v, const R* __restrict__ T,
                                                        const R* __restrict__ p, const R* __restrict__ u_ant,
                                                        const R* __restrict__ fcon, const R* __restrict__ flin,
-                                                       R* __restrict__ resu, NormSlot ns) {
+                                                       R* __restrict__ resu, NormSlot ns, const CtlRef outer) {
   IXB_PDL_ENTRY();
   const int ni = G.mi - 2;  // ii = 2..mi-1
   const int total = ni * (G.nj - 1);
@@ -129,7 +140,8 @@ __global__ void __launch_bounds__(256) residual_kernel(const Geo<R> G, const R* 
     acc += (double)r * (double)r;
   }
   const double s = block_sum(acc);
-  finish_norm(ns, s);
+  const bool last = finish_norm(ns, s);
+  if (last && outer.ctl && threadIdx.x == 0) ctl_outer_step(outer.ctl, outer.norms, outer.cond, outer.cond2);
 }
 
 // batched forms: work item i = (instance, block of kCellChunk cells)
@@ -299,7 +311,7 @@ cudaError_t sweep_set_smem_limits() {
 // line in `buf`, then the line solve writes the field.
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
                              const Geo<float>& Gf, const SweepIO<double>& io, const StageBuf& buf,
-                             cudaStream_t st) {
+                             cudaStream_t st, const CtlRef& ctl) {
   cudaError_t e;
   if (solver == IXB_SOLVER_EXACT) {
     auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, IXB_SOLVER_EXACT>(s, G, Gf, io, buf, st)) };
@@ -314,7 +326,7 @@ cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<
   if (e != cudaSuccess) return e;
   SolveIO so{};
   so.coef = buf.base; so.stride = buf.stride; so.P = buf.P;
-  so.in = io.in; so.out = io.out; so.prev = io.prev; so.nrm0 = io.nrm0;
+  so.in = io.in; so.out = io.out; so.prev = io.prev; so.nrm0 = io.nrm0; so.ctl = ctl;
   so.LD = G.LD; so.m = s.m; so.mp = s.mp;
   return solve_launch(solver, eq_is_x(eq), eq_dc(eq, solver), s, so, st);
 }
@@ -330,13 +342,18 @@ cudaError_t launch_narrow_f32(const double* src, float* dst, size_t n, cudaStrea
   return cudaGetLastError();
 }
 
+cudaError_t launch_preset_f64(double* pc, size_t n, const CtlRef& gate, cudaStream_t st) {
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 4);
+  return launch_k(preset_kernel, grid, 256, 0, st, pc, n, gate);
+}
+
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
-                               const double* au, const double* av, int fast, cudaStream_t st) {
+                               const double* au, const double* av, int fast, cudaStream_t st, const CtlRef& gate) {
   const int total = (G.mi - 1) * (G.nj - 1);
   const int bs = 256;
   const int grid = (total + bs - 1) / bs;
-  if (fast) return launch_k(correct_kernel<double, true>, grid, bs, 0, st, G, u, v, p, pc, au, av);
-  return launch_k(correct_kernel<double, false>, grid, bs, 0, st, G, u, v, p, pc, au, av);
+  if (fast) return launch_k(correct_kernel<double, true>, grid, bs, 0, st, G, u, v, p, pc, au, av, gate);
+  return launch_k(correct_kernel<double, false>, grid, bs, 0, st, G, u, v, p, pc, au, av, gate);
 }
 
 int residual_grid(int mi, int nj) {
@@ -346,10 +363,13 @@ int residual_grid(int mi, int nj) {
 
 cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const double* v, const double* T,
                                 const double* p, const double* u_ant, const double* fcon, const double* flin,
-                                double* resu, NormSlot ns, int fast, cudaStream_t st) {
+                                double* resu, NormSlot ns, int fast, cudaStream_t st, const CtlRef& outer) {
   const int grid = residual_grid(G.mi, G.nj);
-  if (fast) return launch_k(residual_kernel<double, true>, grid, 256, 0, st, G, u, v, T, p, u_ant, fcon, flin, resu, ns);
-  return launch_k(residual_kernel<double, false>, grid, 256, 0, st, G, u, v, T, p, u_ant, fcon, flin, resu, ns);
+  if (fast)
+    return launch_k(residual_kernel<double, true>, grid, 256, 0, st, G, u, v, T, p, u_ant, fcon, flin, resu, ns,
+                    outer);
+  return launch_k(residual_kernel<double, false>, grid, 256, 0, st, G, u, v, T, p, u_ant, fcon, flin, resu, ns,
+                  outer);
 }
 
 cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,

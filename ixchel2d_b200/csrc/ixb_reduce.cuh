@@ -33,8 +33,8 @@ static __device__ double block_sum(double v) {
 
 // Publish this CTA's partial; the last CTA to arrive sums all partials in
 // CTA order (every thread of that CTA loads its share in one round trip)
-// and stores sqrt(sum).
-static __device__ void finish_norm(const NormSlot& ns, double block_total) {
+// and stores sqrt(sum).  Returns true in every thread of that last CTA.
+static __device__ bool finish_norm(const NormSlot& ns, double block_total) {
   __shared__ int is_last;
   if (threadIdx.x == 0) {
     ns.partials[blockIdx.x] = block_total;
@@ -53,6 +53,7 @@ static __device__ void finish_norm(const NormSlot& ns, double block_total) {
       *ns.counter = 0u;
     }
   }
+  return is_last != 0;
 }
 
 // Per-instance norms of a batched launch.  Work item `item` (of instance

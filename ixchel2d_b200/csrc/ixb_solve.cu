@@ -14,6 +14,7 @@
 
 #include <algorithm>
 
+#include "ixb_ctl.cuh"
 #include "ixb_internal.h"
 #include "ixb_reduce.cuh"
 
@@ -111,7 +112,8 @@ __global__ void __launch_bounds__(TL * G) solve_kernel(const SolveIO io, const i
                                                             nfull, 1 + blockIdx.x * TL);
   if (io.nrm0.partials) {
     const double s = block_sum(acc);
-    finish_norm(io.nrm0, s);
+    const bool last = finish_norm(io.nrm0, s);
+    if (last && io.ctl.ctl && threadIdx.x == 0) ctl_inner_step(io.ctl.ctl, io.ctl.norms, io.ctl.which, io.ctl.cond);
   }
 }
 
