@@ -226,6 +226,22 @@ int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float*
 int ixb_tridiag_f64_noalloc(const double* a, const double* b, const double* c, const double* d, double* x, int n,
                             int nsys, int layout, int solver, void* stream);
 
+/* ---- energy equation with the flow held fixed, and its discrete adjoint ----
+ * No counterpart in the reference.  ixb_energy_iterations runs n passes of
+ * the two T sweeps (T-y then T-x, main.f90:985-1136) at the current u, v.
+ * ixb_adjoint_energy returns, for the same K passes from the current state,
+ * the gradient of the hot-wall Nusselt number nu0 of ixb_nusselt_x(h, j0, j1)
+ * with respect to the boundary value of every T x-line on side a (x = 0):
+ * grad[jj-1] = d nu0 / d value(jj), jj = 1..nj+1 (zero where the line is not
+ * solved).  The map is affine in T with u, v fixed, so the gradient is exact
+ * (transposed line solves, no stored forward states); the state is left
+ * unchanged.  ixb_set_bc_values sets the per-line values of one side of a
+ * boundary table (a per-node profile, beyond the reference's 15 segments),
+ * keeping each line's type. */
+int ixb_energy_iterations(ixb_handle* h, int n);
+int ixb_adjoint_energy(ixb_handle* h, int K, int j0, int j1, double* grad);
+int ixb_set_bc_values(ixb_handle* h, int var, int side, const double* values);
+
 /* ---- batched cavities: many instances, one launch per phase ----
  * No counterpart in the reference, which runs one case per process.  A
  * batch owns `count` instances of sizes mi[i] x nj[i] (4..1024 each), all in

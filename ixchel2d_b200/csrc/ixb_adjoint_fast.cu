@@ -1,0 +1,224 @@
+// ixb_adjoint_fast.cu -- discrete adjoint of the energy iteration with the
+// flow held fixed: the gradient of the hot-wall Nusselt number after K
+// passes of the T sweeps (T-y then T-x, source/main.f90:985-1136) with
+// respect to the Dirichlet value of every x-line on side a (the hot wall,
+// x = 0).  The reference has no counterpart.
+//
+// With u, v frozen, every T sweep is affine in the temperatures: a line solve
+// x = A^-1 (R T_in + f) with coefficients (AI, AD, BS, BN and the relaxed
+// diagonal) that depend on the mesh and the velocities only, and f holding
+// the boundary values.  The adjoint therefore needs no stored forward states:
+// starting from the Nusselt number's weights, each sweep is reversed as
+// mu = A^-T lambda (a transposed batched line solve) followed by
+// lambda_in = R^T mu plus the lines the sweep copies, and the side-a
+// boundary rows of the x-sweeps collect d Nu / d value += mu[row 0].
+// Built with FMA contraction, like the fast forward assembly, whose
+// coefficients it re-evaluates.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "ixb_handle.h"
+#include "ixb_nusselt.h"
+
+namespace ixb {
+namespace {
+
+// coefficient arrays (field layout) of the energy rows: AI, AD, BS, BN, diag
+enum { C_AI = 0, C_AD, C_BS, C_BN, C_DG, C_COUNT };
+
+__global__ void adj_coef_kernel(const Geo<double> G, const SweepIO<double> io, double* __restrict__ coef,
+                                size_t fsz) {
+  const int ni = G.mi - 1;  // ii = 2..mi, jj = 2..nj
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ni * (G.nj - 1)) return;
+  const int ii = 2 + idx % ni, jj = 2 + idx / ni;
+  const Row<double> rx = assemble_tx<true>(G, io, ii, jj);  // a = AI, c = AD, b = diagonal
+  const Row<double> ry = assemble_ty<true>(G, io, ii, jj);  // a = BS, c = BN
+  const int c0 = G.at(ii, jj);
+  coef[C_AI * fsz + c0] = rx.a;
+  coef[C_AD * fsz + c0] = rx.c;
+  coef[C_BS * fsz + c0] = ry.a;
+  coef[C_BN * fsz + c0] = ry.c;
+  coef[C_DG * fsz + c0] = rx.b;
+}
+
+struct Sweep {
+  bool x;               // x-lines (fixed jj) or y-lines (fixed ii)
+  int n;                // rows per line
+  int nl;               // solved lines 2 .. nl+1
+  const BCEntry* first;
+  const BCEntry* last;
+};
+
+// Forward row r of solved line L: (a, b, c) of impone_cond_frontera's boundary
+// rows or of the energy assembly.
+__device__ __forceinline__ void fwd_row(const Geo<double>& G, const Sweep& s, const double* coef, size_t fsz, int L,
+                                        int r, double& a, double& b, double& c) {
+  if (r == 0) {
+    const BCEntry e = s.first[L];
+    a = 0.0; b = e.type == 2 ? -1.0 : 1.0; c = e.type == 2 ? 1.0 : 0.0;
+  } else if (r == s.n - 1) {
+    const BCEntry e = s.last[L];
+    a = e.type == 2 ? -1.0 : 0.0; b = 1.0; c = 0.0;
+  } else {
+    const int c0 = s.x ? G.at(r + 1, L) : G.at(L, r + 1);
+    a = coef[(s.x ? C_AI : C_BS) * fsz + c0];
+    c = coef[(s.x ? C_AD : C_BN) * fsz + c0];
+    b = coef[C_DG * fsz + c0];
+  }
+}
+
+// Transposed rows (a'_r = c_{r-1}, b'_r = b_r, c'_r = a_{r+1}) and right-hand
+// side lambda of every solved line, contiguous per line.
+__global__ void adj_stage_kernel(const Geo<double> G, const Sweep s, const double* __restrict__ coef, size_t fsz,
+                                 const double* __restrict__ lam, double* __restrict__ ta, double* __restrict__ tb,
+                                 double* __restrict__ tc, double* __restrict__ td) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= s.nl * s.n) return;
+  const int li = idx / s.n, r = idx - li * s.n, L = li + 2;
+  double a, b, c, t;
+  fwd_row(G, s, coef, fsz, L, r, a, b, c);
+  ta[idx] = 0.0;
+  tc[idx] = 0.0;
+  if (r > 0) { fwd_row(G, s, coef, fsz, L, r - 1, t, t, c); ta[idx] = c; }
+  if (r < s.n - 1) { fwd_row(G, s, coef, fsz, L, r + 1, a, t, t); tc[idx] = a; }
+  fwd_row(G, s, coef, fsz, L, r, a, b, c);
+  tb[idx] = b;
+  td[idx] = lam[s.x ? G.at(r + 1, L) : G.at(L, r + 1)];
+}
+
+// lambda_in = R^T mu + copies of the unsolved lines; x-sweeps also add the
+// side-a boundary rows' sensitivities to grad (indexed by line).
+__global__ void adj_scatter_kernel(const Geo<double> G, const Sweep s, const double* __restrict__ coef, size_t fsz,
+                                   double rel, const double* __restrict__ mu, const double* __restrict__ lam_out,
+                                   double* __restrict__ lam_in, double* __restrict__ grad) {
+  const int nx = G.mi + 1, ny = G.nj + 1;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nx * ny) return;
+  const int ii = 1 + idx % nx, jj = 1 + idx / nx;
+  const int L = s.x ? jj : ii;  // line of this cell
+  const int r = s.x ? ii - 1 : jj - 1;
+  const int nfull = s.nl + 2;
+  auto solved = [&](int l) { return l >= 2 && l <= s.nl + 1; };
+  auto mu_at = [&](int l, int rr) { return mu[(size_t)(l - 2) * s.n + rr]; };
+  const bool interior = r >= 1 && r <= s.n - 2;
+  double v = 0.0;
+  if (L >= 1 && L <= nfull) {
+    if (solved(L)) {
+      if (interior) v += coef[C_DG * fsz + G.at(ii, jj)] * (1.0 - rel) * mu_at(L, r);
+      if (s.x && r == 0) grad[L] += mu_at(L, 0);
+    } else {
+      v += lam_out[G.at(ii, jj)];
+    }
+    // rows of the neighbouring lines that read this cell through d
+    if (interior) {
+      if (solved(L + 1)) {
+        const int cn = s.x ? G.at(ii, jj + 1) : G.at(ii + 1, jj);
+        v -= coef[(s.x ? C_BS : C_AI) * fsz + cn] * mu_at(L + 1, r);
+      }
+      if (solved(L - 1)) {
+        const int cp = s.x ? G.at(ii, jj - 1) : G.at(ii - 1, jj);
+        v -= coef[(s.x ? C_BN : C_AD) * fsz + cp] * mu_at(L - 1, r);
+      }
+    }
+  }
+  lam_in[G.at(ii, jj)] = v;
+}
+
+}  // namespace
+}  // namespace ixb
+
+using namespace ixb;
+
+#define ACK(x)                   \
+  do {                           \
+    cudaError_t e_ = (x);        \
+    if (e_ != cudaSuccess) {     \
+      h->last_cuda = e_;         \
+      return IXB_ECUDA;          \
+    }                            \
+  } while (0)
+
+extern "C" int ixb_adjoint_energy(ixb_handle* h, int K, int j0, int j1, double* grad) {
+  if (!h || K < 0 || !grad) return IXB_EINVAL;
+  const int st0 = handle_ready(h);
+  if (st0 != IXB_OK) return st0;
+  const int mi = h->mi, nj = h->nj;
+  if (j0 < 1 || j1 < j0) return IXB_EINVAL;
+  for (int k = j0; k <= j1; k += 2)
+    if (k + 2 > nj + 1) return IXB_EINVAL;
+  // workspace
+  const size_t fsz = h->fsz;
+  const size_t nst = (size_t)std::max((nj - 1) * (mi + 1), (mi - 1) * (nj + 1));
+  const size_t need = (C_COUNT + 2) * fsz + 5 * nst + (size_t)(nj + 2);
+  if (h->adj_size < need) {
+    if (h->adj_pool) cudaFree(h->adj_pool);
+    h->adj_pool = nullptr;
+    h->adj_size = 0;
+    ACK(cudaMalloc(&h->adj_pool, need * sizeof(double)));
+    h->adj_size = need;
+  }
+  double* coef = h->adj_pool;
+  double* lam = coef + C_COUNT * fsz;
+  double* lam2 = lam + fsz;
+  double* ta = lam2 + fsz;
+  double* tb = ta + nst;
+  double* tc = tb + nst;
+  double* td = tc + nst;
+  double* mu = td + nst;
+  double* gd = mu + nst;
+  cudaStream_t st = h->stream;
+  // coefficients of the energy rows at the current (frozen) velocities
+  const int cT = h->cT;
+  SweepIO<double> io = handle_sweep_io(h, EQ_TX, nullptr);
+  h->cT = cT;
+  const Geo<double> G = handle_geo(h);
+  ACK(cudaMemsetAsync(coef, 0, C_COUNT * fsz * sizeof(double), st));
+  {
+    const int cells = (mi - 1) * (nj - 1);
+    adj_coef_kernel<<<(cells + 255) / 256, 256, 0, st>>>(G, io, coef, fsz);
+    ACK(cudaGetLastError());
+  }
+  // the objective's weights: Nu is linear in T (the wall-normal 3-point
+  // derivative integrated panel by panel), evaluated here on unit fields
+  std::vector<double> along(nj + 2, 0.0), across(mi + 2, 0.0);
+  for (int j = 1; j <= nj + 1; ++j) along[j] = h->yp[j - 1];
+  for (int i = 1; i <= mi + 1; ++i) across[i] = h->xp[i - 1];
+  std::vector<double> w((size_t)fsz, 0.0);
+  for (int k = j0; k <= j1 + 2; ++k)
+    for (int l = 1; l <= 3; ++l) {
+      auto f = [&](int kk, int ll) { return (kk == k && ll == l) ? 1.0 : 0.0; };
+      w[(size_t)(k - 1) * h->LD + (l - 1)] = nusselt_wall(f, along.data(), across.data(), mi + 1, 0, 0, j0, j1);
+    }
+  ACK(cudaMemcpyAsync(lam, w.data(), fsz * sizeof(double), cudaMemcpyHostToDevice, st));
+  ACK(cudaMemsetAsync(gd, 0, (nj + 2) * sizeof(double), st));
+  const BCEntry* base = h->bc + (size_t)2 * 4 * h->bcstride;  // T tables, sides a b c d
+  const Sweep sx{true, mi + 1, nj - 1, base + 0 * (size_t)h->bcstride, base + 2 * (size_t)h->bcstride};
+  const Sweep sy{false, nj + 1, mi - 1, base + 1 * (size_t)h->bcstride, base + 3 * (size_t)h->bcstride};
+  const double rel = h->prm.rel_ener;
+  const int cells = (mi + 1) * (nj + 1);
+  auto reverse = [&](const Sweep& s, const double* lam_out, double* lam_in) -> int {
+    const int rows = s.nl * s.n;
+    adj_stage_kernel<<<(rows + 255) / 256, 256, 0, st>>>(G, s, coef, fsz, lam_out, ta, tb, tc, td);
+    ACK(cudaGetLastError());
+    ACK(tridiag_f64(ta, tb, tc, td, mu, s.n, s.nl, 0, IXB_SOLVER_HYBRID, st));
+    adj_scatter_kernel<<<(cells + 255) / 256, 256, 0, st>>>(G, s, coef, fsz, rel, mu, lam_out, lam_in, gd);
+    ACK(cudaGetLastError());
+    return IXB_OK;
+  };
+  // K passes of (T-y, T-x), reversed: T-x first
+  for (int k = 0; k < K; ++k) {
+    int r = reverse(sx, lam, lam2);
+    if (r != IXB_OK) return r;
+    r = reverse(sy, lam2, lam);
+    if (r != IXB_OK) return r;
+  }
+  std::vector<double> g(nj + 2);
+  ACK(cudaMemcpyAsync(g.data(), gd, (nj + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
+  ACK(cudaStreamSynchronize(st));
+  for (int jj = 1; jj <= nj + 1; ++jj) grad[jj - 1] = g[jj];
+  return IXB_OK;
+}

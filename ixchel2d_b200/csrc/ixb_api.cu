@@ -421,6 +421,7 @@ void free_all(ixb_handle* h) {
   for (auto b : bufs) if (*b) cudaFree(*b);
   if (h->metrics32) cudaFree(h->metrics32);
   if (h->stage) cudaFree(h->stage);
+  if (h->adj_pool) cudaFree(h->adj_pool);
   if (h->tables32) cudaFree(h->tables32);
   if (h->bc) cudaFree(h->bc);
   if (h->counters) cudaFree(h->counters);
@@ -947,6 +948,31 @@ static int nusselt(ixb_handle* h, int vertical, int k0, int k1, double* nu0, dou
   CK(cudaStreamSynchronize(h->stream));
   if (nu0) *nu0 = out[0];
   if (nu1) *nu1 = out[1];
+  return IXB_OK;
+}
+
+int ixb_energy_iterations(ixb_handle* h, int n) {
+  if (!h || n < 0) return IXB_EINVAL;
+  TRY(ready(h));
+  for (int k = 0; k < n; ++k) {
+    TRY(sweep(h, EQ_TY, nullptr, false));
+    TRY(sweep(h, EQ_TX, nullptr, false));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return IXB_OK;
+}
+
+int ixb_set_bc_values(ixb_handle* h, int var, int side, const double* values) {
+  if (!h || !values || var < 0 || var > 2 || side < 0 || side > 3) return IXB_EINVAL;
+  if (!h->has_bc[var]) return IXB_ESTATE;
+  const int nl = (side == 0 || side == 2) ? (var == 1 ? h->nj : h->nj + 1) : (var == 0 ? h->mi : h->mi + 1);
+  std::vector<BCEntry> e(nl + 1);
+  BCEntry* d = h->bc + ((size_t)var * 4 + side) * h->bcstride;
+  CK(cudaMemcpyAsync(e.data(), d, e.size() * sizeof(BCEntry), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int l = 1; l <= nl; ++l) e[l].val = values[l - 1];
+  CK(cudaMemcpyAsync(d, e.data(), e.size() * sizeof(BCEntry), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return IXB_OK;
 }
 

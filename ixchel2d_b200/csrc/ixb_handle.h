@@ -77,6 +77,9 @@ struct ixb_handle {
   int shape_tl[ixb::EQ_COUNT] = {};  // launch shape per sweep (0 = not chosen yet)
   int shape_g[ixb::EQ_COUNT] = {};
   int nsm = 148;
+  // adjoint workspace (ixb_adjoint_energy), allocated on first use
+  double* adj_pool = nullptr;
+  size_t adj_size = 0;
 };
 
 namespace ixb {

@@ -8,6 +8,7 @@
 #include <cstdlib>
 
 #include "ixb_ctl.cuh"
+#include "ixb_nusselt.h"
 #include "ixb_internal.h"
 #include "ixb_reduce.cuh"
 
@@ -212,30 +213,7 @@ __global__ void nusselt_kernel(const Geo<double> G, const double* __restrict__ T
   const double* across = vertical ? xp : yp;
   const int n_across = vertical ? G.mi + 1 : G.nj + 1;
   auto f = [&](int k, int l) { return vertical ? T[G.at(l, k)] : T[G.at(k, l)]; };
-  for (int wall = 0; wall < 2; ++wall) {
-    const int jj = wall == 0 ? 1 : n_across - 2;
-    double nu = 0.0;
-    for (int ii = k0; ii <= k1; ii += 2) {
-      double der[3];
-      for (int q = 0; q < 3; ++q) {
-        const int k = ii + q;
-        if (quirk && k > k1) { der[q] = 0.0; continue; }  // derivada beyond i_1o stays 0
-        const double dy1 = f(k, jj + 1) - f(k, jj), dy2 = f(k, jj + 2) - f(k, jj + 1);
-        const double dx1 = across[jj + 1] - across[jj], dx2 = across[jj + 2] - across[jj + 1];
-        const double a = (dy2 / dx2 - dy1 / dx1) / (dx1 + dx2);
-        const double b = dy2 / dx2 - a * (across[jj + 1] + across[jj + 2]);
-        der[q] = 2.0 * a * (wall == 0 ? across[jj] : across[jj + 2]) + b;
-      }
-      const double x_o = along[ii], x_1 = along[ii + 1], x_2 = along[ii + 2];
-      const double y_o = der[0], y_1 = der[1], y_2 = der[2];
-      const double alpha = ((y_2 - y_1) / (x_2 - x_1) - (y_1 - y_o) / (x_1 - x_o)) / (x_2 - x_o);
-      const double beta = (y_2 - y_1) / (x_2 - x_1) - alpha * (x_1 + x_2);
-      const double gamma = y_o - alpha * x_o * x_o - beta * x_o;
-      nu = nu + alpha / 3.0 * (x_2 * x_2 * x_2 - x_o * x_o * x_o) + beta / 2.0 * (x_2 * x_2 - x_o * x_o) +
-           gamma * (x_2 - x_o);
-    }
-    out2[wall] = -nu;
-  }
+  for (int wall = 0; wall < 2; ++wall) out2[wall] = nusselt_wall(f, along, across, n_across, wall, quirk, k0, k1);
 }
 
 // ---------------------------------------------------------------------------

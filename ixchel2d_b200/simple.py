@@ -144,6 +144,20 @@ class Simple2D:
         F.check(F.lib.ixb_autotune(self.h, reps, flush_bytes, chosen, F.dptr(ms)), "ixb_autotune")
         return {k: (chosen[2 * k], chosen[2 * k + 1], float(ms[k])) for k in range(8)}
 
+    # ---- energy equation with the flow fixed, and its adjoint ----
+    def energy_iterations(self, n: int):
+        F.check(F.lib.ixb_energy_iterations(self.h, n), "ixb_energy_iterations")
+
+    def adjoint_energy(self, K: int, j0: int, j1: int) -> np.ndarray:
+        """d nu0(ixb_nusselt_x(j0, j1)) / d (side-a value of T x-line jj), jj = 1..nj+1, after K passes."""
+        g = np.zeros(self.nj + 1)
+        F.check(F.lib.ixb_adjoint_energy(self.h, K, j0, j1, F.dptr(g)), "ixb_adjoint_energy")
+        return g
+
+    def set_bc_values(self, var: int, side: int, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        F.check(F.lib.ixb_set_bc_values(self.h, var, side, F.dptr(v)), "ixb_set_bc_values")
+
     def set_stream(self, stream_handle: int):
         """Launch on an external cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
         F.check(F.lib.ixb_set_stream(self.h, C.c_void_p(stream_handle)), "ixb_set_stream")
