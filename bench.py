@@ -363,6 +363,45 @@ def batched_bench(stream, n_inst=256, iters=30, n_conv=16, conv_cap=20000):
     return out
 
 
+def adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, warm=500, fd_nodes=8):
+    """Energy-equation adjoint with the flow held fixed: natural-convection
+    cavity n x n, Ra, after `warm` SIMPLE iterations; hot-wall profile of
+    `nodes` piecewise-linear nodes, value 1 + U(-0.05, 0.05) (seed 1234);
+    objective the hot-wall Nusselt number after K passes of the T sweeps.
+    Gradient by the adjoint against central differences (h = 1e-6) of the
+    same GPU forward on fd_nodes of the nodes."""
+    from ixchel2d_b200 import Simple2D, cases
+    from ixchel2d_b200.adjoint import HotWallNusselt
+    case = cases.natural_cavity(n, n, Ra=Ra, T0=0.5)
+    sim = Simple2D.from_case(case)
+    sim.iterations(warm)
+    state = sim.download()
+    J = HotWallNusselt(sim, state, case.yp, nodes, K, 2, n - 2)
+    rng = np.random.default_rng(1234)
+    theta = 1.0 + rng.uniform(-0.05, 0.05, nodes)
+    J.gradient(theta)  # warm
+    t0 = time.perf_counter()
+    g = J.gradient(theta)
+    t_adj = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    nu = J.value(theta)
+    t_fwd = time.perf_counter() - t0
+    pick = np.linspace(0, nodes - 1, fd_nodes).astype(int)
+    h = 1e-6
+    fd = np.zeros(fd_nodes)
+    for q, k in enumerate(pick):
+        e = np.zeros(nodes)
+        e[k] = h
+        fd[q] = (J.value(theta + e) - J.value(theta - e)) / (2 * h)
+    sim.close()
+    return {"case": f"natural_cavity_{n}x{n}_Ra{Ra:g}", "flow": f"held fixed after {warm} SIMPLE iterations",
+            "nodes": nodes, "K": K, "nu_hot_wall": nu,
+            "adjoint_s": t_adj, "forward_s": t_fwd, "fd_all_nodes_s_estimate": 2 * nodes * t_fwd,
+            "fd_nodes_checked": fd_nodes,
+            "max_rel_err_vs_fd": float(np.max(np.abs(g[pick] - fd) / np.maximum(np.abs(fd), 1e-300))),
+            "normwise_rel_err_vs_fd": float(np.linalg.norm(g[pick] - fd) / np.linalg.norm(fd))}
+
+
 def make_sim(case, prec, stream, shapes):
     from ixchel2d_b200 import Simple2D
     sim = Simple2D.from_case(case, prec=prec)
@@ -469,6 +508,8 @@ def run_ours(args):
     adi = adi_microbench(stream)
     # ---- batched cavities ----
     batched = batched_bench(stream)
+    # ---- energy adjoint (flow held fixed) ----
+    adjoint = adjoint_bench()
 
     # ---- per-phase times (cold L2) of the refined path on a scratch handle ----
     scratch, _ = make_sim(case, F.PREC_FP32_REFINED, stream, shapes["refined"])
@@ -511,6 +552,7 @@ def run_ours(args):
             "phases_ms_cold_l2": dict(zip(PHASES, phase_ms)),
             "adi_line_solve": adi,
             "batched_cavities": batched,
+            "energy_adjoint": adjoint,
             "sweep_shapes": {n: {SWEEPS[int(k)]: list(v[:2]) for k, v in sh.items()} for n, sh in shapes.items()},
             "iteration_alg_bytes": iter_bytes,
             "cpu_baseline": None if cpu_val is None else {
