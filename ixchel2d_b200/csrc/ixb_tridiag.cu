@@ -356,10 +356,15 @@ struct StridedShape {
   static constexpr int R = C * M;  // rows per CTA
 };
 
-// reduced-row buffers of one CTA: 2 sets x (a | c | d) x 2 PCR buffers x NR
+// reduced-row buffers of one CTA: 2 sets x ((a | c | d) x NR gathered rows
+// + the PCR buffers of T threads)
 template <class R>
-__host__ __device__ constexpr size_t strided_smem_bytes(int nr) {
-  return (size_t)2 * 6 * nr * sizeof(R);
+__host__ __device__ constexpr size_t strided_set_elems(int nr, int t) {
+  return (size_t)3 * nr + (size_t)12 * t;
+}
+template <class R>
+__host__ __device__ constexpr size_t strided_smem_bytes(int nr, int t) {
+  return 2 * strided_set_elems<R>(nr, t) * sizeof(R);
 }
 
 template <class R, int W, int T, int M>
@@ -379,8 +384,6 @@ __global__ void __launch_bounds__(T) tri_strided_kernel(const R* __restrict__ a,
   const int nclusters = gridDim.x / Q;
   const int cl = blockIdx.x / Q;
   const int ngroups = (nsys + W - 1) / W;
-  int steps = 0;
-  for (int s_ = 1; s_ < NR; s_ <<= 1) ++steps;
   int set = 0;
   for (int g = cl; g < ngroups; g += nclusters, set ^= 1) {
     const int sys = g * W + w;
@@ -421,7 +424,7 @@ __global__ void __launch_bounds__(T) tri_strided_kernel(const R* __restrict__ a,
     const R r0 = fast_rcp(fmaT(-rc[0], an, rb[0]));
     const R eA = ra[0] * r0, eC = -rc[0] * cn * r0, eD = fmaT(-rc[0], dn, rd[0]) * r0;
     // reduced rows 2i, 2i+1 (i = rank*C + k) of system w -> shared memory of rank w
-    R* base = sm + (size_t)set * 6 * NR;  // this set: buffer 0 = a | c | d, buffer 1 = a | c | d
+    R* base = sm + (size_t)set * strided_set_elems<R>(NR, T);  // this set: a | c | d, then PCR buffers
     {
       R* dst = cluster.map_shared_rank(base, w % Q);
       const int i = 2 * (rank * SS::C + k);
@@ -429,27 +432,55 @@ __global__ void __launch_bounds__(T) tri_strided_kernel(const R* __restrict__ a,
       dst[i + 1] = ap; dst[NR + i + 1] = cp; dst[2 * NR + i + 1] = dp;
     }
     cluster.sync();
-    if (rank < W) {  // owner of system `rank` of this group: PCR on its NR rows
-      R* cur = base;
-      R* nxt = base + 3 * NR;
-      for (int s_ = 1; s_ < NR; s_ <<= 1) {
-        for (int i = tid; i < NR; i += T) {
-          const R ai = cur[i], ci = cur[NR + i], di = cur[2 * NR + i];
-          R alo = R(0), clo = R(0), dlo = R(0), ahi = R(0), chi = R(0), dhi = R(0);
-          if (i - s_ >= 0) { alo = cur[i - s_]; clo = cur[NR + i - s_]; dlo = cur[2 * NR + i - s_]; }
-          if (i + s_ < NR) { ahi = cur[i + s_]; chi = cur[NR + i + s_]; dhi = cur[2 * NR + i + s_]; }
-          const R rr = fast_rcp(fmaT(-ci, ahi, fmaT(-ai, clo, R(1))));
-          nxt[i] = -ai * alo * rr;
-          nxt[NR + i] = -ci * chi * rr;
-          nxt[2 * NR + i] = fmaT(-ci, dhi, fmaT(-ai, dlo, di)) * rr;
+    if (rank < W) {  // owner of system `rank` of this group: solve its NR reduced rows
+      // every thread takes RPT consecutive rows (padding rows beyond NR are
+      // identity rows, decoupled); with 4 rows it first eliminates its two
+      // middle rows (modified Thomas on 4 rows), so the PCR runs on 2 rows
+      // per thread
+      constexpr int RPT = 16 / W;  // NR / T: 4 (binary64, W = 4) or 2 (binary32, W = 8)
+      R ea[RPT], ec[RPT], ed[RPT];
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const int i = RPT * tid + q;
+        const bool in = i < NR;
+        ea[q] = in ? base[i] : R(0);
+        ec[q] = in ? base[NR + i] : R(0);
+        ed[q] = in ? base[2 * NR + i] : R(0);
+      }
+      R eA, eC, eD, oA, oC, oD, x0, xl;
+      R m1a = R(0), m1c = R(0), m1d = R(0), m2a = R(0), m2c = R(0), m2d = R(0);
+      if constexpr (RPT == 4) {
+        // forward: rows 1..3 -> x_k + a'_k x_0 + c'_k x_{k+1} = d'_k (unit diagonals)
+        R ap = ea[1], cp = ec[1], dp = ed[1];
+        m1a = ap; m1c = cp; m1d = dp;
+        R r = fast_rcp(fmaT(-ea[2], cp, R(1)));
+        ap = -ea[2] * ap * r; dp = fmaT(-ea[2], dp, ed[2]) * r; cp = ec[2] * r;
+        m2a = ap; m2c = cp; m2d = dp;
+        r = fast_rcp(fmaT(-ea[3], cp, R(1)));
+        oA = -ea[3] * ap * r; oD = fmaT(-ea[3], dp, ed[3]) * r; oC = ec[3] * r;
+        // backward: row 1 -> x_1 + a''_1 x_0 + c''_1 x_3 = d''_1
+        const R dn = fmaT(-m1c, m2d, m1d), an = fmaT(-m1c, m2a, m1a), cn = -m1c * m2c;
+        m1a = an; m1c = cn; m1d = dn;
+        const R r0 = fast_rcp(fmaT(-ec[0], an, R(1)));
+        eA = ea[0] * r0; eC = -ec[0] * cn * r0; eD = fmaT(-ec[0], dn, ed[0]) * r0;
+      } else {
+        eA = ea[0]; eC = ec[0]; eD = ed[0];
+        oA = ea[RPT - 1]; oC = ec[RPT - 1]; oD = ed[RPT - 1];
+      }
+      reduced_pcr<R, T>(base + 3 * NR, tid, true, eA, eC, eD, oA, oC, oD, x0, xl);
+      // solutions of the owned rows -> base[2*NR + i], where the other CTAs read them
+      if (RPT * tid < NR) {
+        base[2 * NR + RPT * tid] = x0;
+        if constexpr (RPT == 4) {
+          base[2 * NR + 4 * tid + 1] = fmaT(-m1c, xl, fmaT(-m1a, x0, m1d));
+          base[2 * NR + 4 * tid + 2] = fmaT(-m2c, xl, fmaT(-m2a, x0, m2d));
         }
-        __syncthreads();
-        R* t = cur; cur = nxt; nxt = t;
+        base[2 * NR + RPT * tid + RPT - 1] = xl;
       }
     }
     cluster.sync();
-    // solutions of the own reduced rows, from rank w (final PCR buffer)
-    const R* sol = cluster.map_shared_rank(base + ((steps & 1) ? 3 * NR : 0) + 2 * NR, w % Q);
+    // solutions of the own reduced rows, from rank w
+    const R* sol = cluster.map_shared_rank(base + 2 * NR, w % Q);
     const int i = 2 * (rank * SS::C + k);
     const R x0 = sol[i], xl = sol[i + 1];
 #pragma unroll
@@ -470,7 +501,7 @@ cudaError_t strided_launch(const R* a, const R* b, const R* c, const R* d, R* x,
   const int Q = (n + SS::R - 1) / SS::R;
   if (Q < W || Q > 8) return cudaErrorInvalidValue;  // one owner CTA per system of a group
   const int nr = 2 * Q * SS::C;
-  const size_t smem = strided_smem_bytes<R>(nr);
+  const size_t smem = strided_smem_bytes<R>(nr, T);
   auto k = tri_strided_kernel<R, W, T, M>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
