@@ -75,12 +75,13 @@ struct SweepTypes {
   using A = typename std::conditional<MIX && !DC, float, double>::type;  // coefficient assembly
 };
 
-// x-sweep tiles: 64 consecutive rows of 4 lines, one cell per thread.
-// y-sweep tiles: 32 consecutive lines (adjacent ii) x 8 rows, one cell per
-// thread, written back through shared memory as 8-row runs of each line.
+// x-sweep tiles: 64 consecutive rows of 8 lines; y-sweep tiles: 32 lines
+// (adjacent ii) x 16 rows, written back through shared memory as 16-row
+// runs of each line.  Each of the 256 threads assembles kAsmCPT cells.
 constexpr int kAsmThreads = 256;
-constexpr int kAsmXR = 64, kAsmXL = 4;
-constexpr int kAsmYL = 32, kAsmYR = 8;
+constexpr int kAsmCPT = 2;  // cells per thread (their loads in flight together)
+constexpr int kAsmXR = 64, kAsmXL = 4 * kAsmCPT;
+constexpr int kAsmYL = 32, kAsmYR = 8 * kAsmCPT;
 
 __host__ __device__ constexpr int asm_tiles(bool x, int n, int nlines) {
   return x ? ((n + kAsmXR - 1) / kAsmXR) * ((nlines + kAsmXL - 1) / kAsmXL)

@@ -141,31 +141,42 @@ __device__ __forceinline__ void assemble_tile(const Geo<typename SweepTypes<SOLV
     const int tr_n = (n + kAsmXR - 1) / kAsmXR;
     const int tl = tile / tr_n, tr = tile - tl * tr_n;
     const int r = tr * kAsmXR + (threadIdx.x % kAsmXR);
-    const int L = line_lo + tl * kAsmXL + threadIdx.x / kAsmXR;
-    const bool valid = r < n && L <= line_hi;
-    const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
-    if (valid) {
-      const size_t o = (size_t)(L - line_lo) * co.P + r;
-      co.a[o] = S(row.a); co.b[o] = S(row.b); co.c[o] = S(row.c); co.d[o] = S(row.d);
+#pragma unroll
+    for (int u = 0; u < kAsmCPT; ++u) {
+      const int L = line_lo + tl * kAsmXL + threadIdx.x / kAsmXR + u * (kAsmThreads / kAsmXR);
+      const bool valid = r < n && L <= line_hi;
+      const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
+      if (valid) {
+        const size_t o = (size_t)(L - line_lo) * co.P + r;
+        co.a[o] = S(row.a); co.b[o] = S(row.b); co.c[o] = S(row.c); co.d[o] = S(row.d);
+      }
     }
   } else {
     const int nl = line_hi - line_lo + 1;
     const int tl_n = (nl + kAsmYL - 1) / kAsmYL;
     const int tr = tile / tl_n, tl = tile - tr * tl_n;
-    const int lo = threadIdx.x % kAsmYL, ro = threadIdx.x / kAsmYL;
+    const int lo = threadIdx.x % kAsmYL;
     const int L = line_lo + tl * kAsmYL + lo;  // adjacent ii in a warp: coalesced field reads
-    const int r = tr * kAsmYR + ro;
-    const bool valid = r < n && L <= line_hi;
-    const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
-    tile_s[0][ro][lo] = S(row.a); tile_s[1][ro][lo] = S(row.b);
-    tile_s[2][ro][lo] = S(row.c); tile_s[3][ro][lo] = S(row.d);
+#pragma unroll
+    for (int u = 0; u < kAsmCPT; ++u) {
+      const int ro = threadIdx.x / kAsmYL + u * (kAsmThreads / kAsmYL);
+      const int r = tr * kAsmYR + ro;
+      const bool valid = r < n && L <= line_hi;
+      const auto row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
+      tile_s[0][ro][lo] = S(row.a); tile_s[1][ro][lo] = S(row.b);
+      tile_s[2][ro][lo] = S(row.c); tile_s[3][ro][lo] = S(row.d);
+    }
     __syncthreads();
-    const int wl = threadIdx.x / kAsmYR, wr = threadIdx.x % kAsmYR;  // 8-row runs of one line
-    const int Lw = line_lo + tl * kAsmYL + wl, rw = tr * kAsmYR + wr;
-    if (Lw <= line_hi && rw < n) {
-      const size_t o = (size_t)(Lw - line_lo) * co.P + rw;
-      co.a[o] = tile_s[0][wr][wl]; co.b[o] = tile_s[1][wr][wl];
-      co.c[o] = tile_s[2][wr][wl]; co.d[o] = tile_s[3][wr][wl];
+#pragma unroll
+    for (int u = 0; u < kAsmCPT; ++u) {  // kAsmYR-row runs of one line
+      const int q = threadIdx.x + u * kAsmThreads;
+      const int wl = q / kAsmYR, wr = q % kAsmYR;
+      const int Lw = line_lo + tl * kAsmYL + wl, rw = tr * kAsmYR + wr;
+      if (Lw <= line_hi && rw < n) {
+        const size_t o = (size_t)(Lw - line_lo) * co.P + rw;
+        co.a[o] = tile_s[0][wr][wl]; co.b[o] = tile_s[1][wr][wl];
+        co.c[o] = tile_s[2][wr][wl]; co.d[o] = tile_s[3][wr][wl];
+      }
     }
     __syncthreads();
   }
