@@ -504,6 +504,11 @@ def run_ours(args):
         conv[name] = {"iters": it, "ms": cms, "maxbo": rep["maxbo"], "nu_hot_wall": s2.nusselt_x(2, 62)[0]}
         s2.close()
 
+    # ---- per-phase times (cold L2) of the refined path on a scratch handle ----
+    scratch, _ = make_sim(case, F.PREC_FP32_REFINED, stream, shapes["refined"])
+    scratch.iterations(3)
+    phase_ms = scratch.time_phases(reps=10, flush_bytes=FLUSH_BYTES)
+    scratch.close()
     # ---- batched line-solve microbenchmark (4096 systems x 4096 unknowns) ----
     adi = adi_microbench(stream)
     # ---- batched cavities ----
@@ -511,11 +516,6 @@ def run_ours(args):
     # ---- energy adjoint (flow held fixed) ----
     adjoint = adjoint_bench()
 
-    # ---- per-phase times (cold L2) of the refined path on a scratch handle ----
-    scratch, _ = make_sim(case, F.PREC_FP32_REFINED, stream, shapes["refined"])
-    scratch.iterations(3)
-    phase_ms = scratch.time_phases(reps=10, flush_bytes=FLUSH_BYTES)
-    scratch.close()
     cells = case.cells
     dom = int(np.argmax(phase_ms))
     peak, peak_kind = peaks()
