@@ -38,13 +38,14 @@ extern "C" {
 #define IXB_ENOMEM 8     /* device or host allocation failed */
 
 /* precision modes for ixb_create.  Fields are held in binary64 in both.
- * IXB_PREC_FP32_REFINED (with IXB_SOLVER_HYBRID): every line is staged and
- * solved in binary32.  The u, v and T sweeps are defect corrections: their
- * rows and the residual d - A x of the current values are evaluated in
- * binary64, the correction is solved for in binary32 and added back in
- * binary64, so the converged fields are the binary64 ones.  The p' rows are
- * assembled and solved in binary32 around a binary64 mass source b_o; the
- * p update and the convergence norms stay in binary64.
+ * IXB_PREC_FP32_REFINED (with IXB_SOLVER_HYBRID): every row is assembled in
+ * binary64, scaled to a unit diagonal, and its line staged and solved in
+ * binary32.  The u, v and T sweeps are defect corrections: the residual
+ * d - A x of the current values is evaluated in binary64, the correction is
+ * solved for in binary32 and added back in binary64, so the converged fields
+ * are the binary64 ones.  The p' lines are solved outright in binary32 around
+ * a binary64 mass source b_o; the p update and the convergence norms stay in
+ * binary64.
  * IXB_SOLVER_EXACT ignores the mode and runs the binary64 reference order. */
 #define IXB_PREC_FP64 0
 #define IXB_PREC_FP32_REFINED 1

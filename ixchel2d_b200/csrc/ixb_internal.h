@@ -60,19 +60,21 @@ struct EqIsX { static constexpr bool value = (EQ & 1) != 0; };
 
 // Arithmetic types of one sweep.  The binary64 solvers use binary64
 // throughout.  The mixed solver (handle precision IXB_PREC_FP32_REFINED)
-// stages and solves every line in binary32.  The u, v and T rows are
-// assembled in binary64 and turned into a defect correction (DC): the
+// assembles every row in binary64 and stages and solves the lines in
+// binary32, each row scaled to a unit diagonal first (so that immersed-body
+// penalties of ~1e51, or the vanishing p' coefficients inside a body, stay
+// representable).  The u, v and T rows are a defect correction (DC): the
 // binary64 residual d - A x of the current values is solved for in binary32
 // and the correction added back in binary64, so the fixed point of these
-// equations is the binary64 one.  The p' rows are assembled and solved in
-// binary32 (p' only steers the iteration; it vanishes at convergence), with
-// their mass source b_o evaluated in binary64.
+// equations is the binary64 one.  The p' rows are solved outright in
+// binary32 (p' only steers the iteration; it vanishes at convergence), around
+// a binary64 mass source b_o.
 template <int SOLVER, int EQ>
 struct SweepTypes {
   static constexpr bool MIX = SOLVER == SOLVER_MIXED;
   static constexpr bool DC = MIX && EQ != EQ_PY && EQ != EQ_PX;
-  using S = typename std::conditional<MIX, float, double>::type;        // staged rows, line solve
-  using A = typename std::conditional<MIX && !DC, float, double>::type;  // coefficient assembly
+  using S = typename std::conditional<MIX, float, double>::type;  // staged rows, line solve
+  using A = double;                                               // row assembly
 };
 
 // x-sweep tiles: 64 consecutive rows of 8 lines; y-sweep tiles: 32 lines

@@ -123,6 +123,14 @@ __device__ __forceinline__ Row<typename SweepTypes<SOLVER, EQ>::A> staged_row(
     res = fma(-row.c, xp, res);
     row.d = res;
   }
+  if constexpr (ST::MIX) {
+    // unit diagonal before the binary32 staging; the solution is unchanged
+    const double sc = 1.0 / row.b;
+    row.a *= sc;
+    row.c *= sc;
+    row.d *= sc;
+    row.b = 1.0;
+  }
   return row;
 }
 

@@ -113,3 +113,30 @@ def test_refined_exact_solver_ignores_the_mode():
     gs, os_ = g.download(), o.get_state()
     for k in STATE:
         assert np.array_equal(gs[k], os_[k]), k
+
+
+def test_refined_immersed_body_penalties():
+    # an immersed block with the penalty sources of definir_cuerpo
+    # ('chime', mod_front_inmersa.f90:150-167): ~1e51 on the u, v and T
+    # diagonals, beyond the binary32 range
+    case = cases.natural_cavity(32, 32, Ra=1e4)
+    mi, nj = case.mi, case.nj
+    fu = np.zeros((mi, nj + 1), order="F"); lu = np.zeros_like(fu)
+    fv = np.zeros((mi + 1, nj), order="F"); lv = np.zeros_like(fv)
+    ft = np.zeros((mi + 1, nj + 1), order="F"); lt = np.zeros_like(ft)
+    for f, l in ((fu, lu), (fv, lv)):
+        f[12:18, 12:18] = 10.0e50 * 10.0e-12
+        l[12:18, 12:18] = -10.0e50
+    ft[12:18, 12:18] = 10e50 * 0.5
+    lt[12:18, 12:18] = -10e50
+    case.sources = {0: (fu, lu), 1: (fv, lv), 2: (ft, lt)}
+    g32 = Simple2D.from_case(case, prec=F.PREC_FP32_REFINED)
+    g64 = Simple2D.from_case(case)
+    g32.iterations(200)
+    g64.iterations(200)
+    a, b = g32.download(), g64.download()
+    for k in ("u", "v", "T"):
+        assert np.all(np.isfinite(a[k])), k
+        assert rel_l2(a[k], b[k]) < 1e-4, (k, rel_l2(a[k], b[k]))
+    # the block holds T = fcon / -flin = 0.5
+    assert np.allclose(a["T"][13:17, 13:17], 0.5, atol=1e-9)
