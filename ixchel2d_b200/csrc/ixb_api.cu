@@ -41,27 +41,12 @@ namespace {
 Geo<double> make_geo(const ixb_handle* h) {
   Geo<double> G{};
   G.mi = h->mi; G.nj = h->nj; G.LD = h->LD; G.mstride = h->mstride; G.m = h->metrics;
-  G.tstride = h->fsz; G.tab = h->tables; G.m64 = h->metrics;
+  G.tstride = h->fsz; G.tab = h->tables;
   G.gm = h->prm.gamma_momen; G.ge = h->prm.gamma_energ; G.Ri = h->prm.Ri; G.Riy = h->prm.Riy;
   G.dt = h->prm.dt; G.rel_vel = h->prm.rel_vel; G.rel_pres = h->prm.rel_pres; G.rel_ener = h->prm.rel_ener;
   G.p_update = h->prm.p_update;
   G.inv_gm = 1.0 / G.gm; G.inv_dt = 1.0 / G.dt; G.inv_rel_vel = 1.0 / G.rel_vel;
   G.inv_rel_pres = 1.0 / G.rel_pres; G.inv_rel_ener = 1.0 / G.rel_ener;
-  return G;
-}
-
-// binary32 view of the mesh for the mixed-precision sweeps (the binary64
-// metrics stay reachable for the mass source b_o)
-Geo<float> make_geo32(const ixb_handle* h) {
-  const Geo<double> D = make_geo(h);
-  Geo<float> G{};
-  G.mi = D.mi; G.nj = D.nj; G.LD = D.LD; G.mstride = D.mstride; G.tstride = D.tstride;
-  G.m = h->metrics32; G.m64 = h->metrics; G.tab = h->tables32;
-  G.gm = (float)D.gm; G.ge = (float)D.ge; G.Ri = (float)D.Ri; G.Riy = (float)D.Riy; G.dt = (float)D.dt;
-  G.rel_vel = (float)D.rel_vel; G.rel_pres = (float)D.rel_pres; G.rel_ener = (float)D.rel_ener;
-  G.p_update = (float)D.p_update;
-  G.inv_gm = (float)D.inv_gm; G.inv_dt = (float)D.inv_dt; G.inv_rel_vel = (float)D.inv_rel_vel;
-  G.inv_rel_pres = (float)D.inv_rel_pres; G.inv_rel_ener = (float)D.inv_rel_ener;
   return G;
 }
 
@@ -89,10 +74,6 @@ int ensure_tables(ixb_handle* h) {
   if (!h->tables_dirty) return IXB_OK;
   Geo<double> G = make_geo(h);
   CK(launch_tables_f64(G, h->metrics, h->tables, h->stream));
-  if (h->metrics32) {
-    CK(launch_narrow_f32(h->metrics, h->metrics32, (size_t)M_COUNT * h->mstride, h->stream));
-    CK(launch_narrow_f32(h->tables, h->tables32, (size_t)T_COUNT * h->fsz, h->stream));
-  }
   CK(cudaStreamSynchronize(h->stream));
   h->tables_dirty = false;
   return IXB_OK;
@@ -165,9 +146,8 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm, const CtlRe
   if (h->shape_tl[eq] == 0) pick_shape(h, eq);
   SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), h->shape_tl[eq], h->shape_g[eq]);
   const SweepIO<double> io = sweep_io(h, eq, prev, with_norm);
-  const Geo<float> Gf = h->metrics32 ? make_geo32(h) : Geo<float>{};
   const StageBuf stage{h->stage, h->stage_stride, h->stage_P};
-  CK(launch_sweep_f64(eq, solver_form(h), s, G, Gf, io, stage, h->stream, ctl));
+  CK(launch_sweep_f64(eq, solver_form(h), s, G, io, stage, h->stream, ctl));
   return IXB_OK;
 }
 
@@ -419,10 +399,8 @@ void free_all(ixb_handle* h) {
                      &h->fcon[0], &h->fcon[1], &h->fcon[2], &h->flin[0], &h->flin[1], &h->flin[2],
                      &h->metrics, &h->tables, &h->xp_d, &h->yp_d, &h->partials, &h->norms, &h->nu_d};
   for (auto b : bufs) if (*b) cudaFree(*b);
-  if (h->metrics32) cudaFree(h->metrics32);
   if (h->stage) cudaFree(h->stage);
   if (h->adj_pool) cudaFree(h->adj_pool);
-  if (h->tables32) cudaFree(h->tables32);
   if (h->bc) cudaFree(h->bc);
   if (h->counters) cudaFree(h->counters);
   if (h->ctl_d) cudaFree(h->ctl_d);
@@ -520,10 +498,6 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
   if (cudaMemset(h->metrics, 0, (size_t)M_COUNT * h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ECUDA);
   if (cudaMalloc(&h->tables, (size_t)T_COUNT * fb) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMemset(h->tables, 0, (size_t)T_COUNT * fb) != cudaSuccess) return fail(IXB_ECUDA);
-  if (prec_mode == IXB_PREC_FP32_REFINED) {
-    if (cudaMalloc(&h->metrics32, (size_t)M_COUNT * h->mstride * sizeof(float)) != cudaSuccess) return fail(IXB_ENOMEM);
-    if (cudaMalloc(&h->tables32, (size_t)T_COUNT * h->fsz * sizeof(float)) != cudaSuccess) return fail(IXB_ENOMEM);
-  }
   if (cudaMalloc(&h->xp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   if (cudaMalloc(&h->yp_d, (size_t)h->mstride * sizeof(double)) != cudaSuccess) return fail(IXB_ENOMEM);
   h->bcstride = std::max(mi, nj) + 3;
@@ -1001,7 +975,6 @@ int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float*
 
 namespace ixb {
 Geo<double> handle_geo(const ixb_handle* h) { return make_geo(h); }
-Geo<float> handle_geo32(const ixb_handle* h) { return h->metrics32 ? make_geo32(h) : Geo<float>{}; }
 int handle_solver_form(const ixb_handle* h) { return solver_form(h); }
 int handle_ready(ixb_handle* h) { return ready(h); }
 SweepIO<double> handle_sweep_io(ixb_handle* h, int eq, const double* prev) { return sweep_io(h, eq, prev, false); }

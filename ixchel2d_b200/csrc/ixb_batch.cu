@@ -132,14 +132,13 @@ int form_of(const ixb_batch* b) { return b->prec == IXB_PREC_FP32_REFINED ? SOLV
 template <int EQ, int SOLVER>
 cudaError_t build_asm(ixb_batch* b, const std::vector<SweepIO<double>>& io, std::vector<int2>& items) {
   using ST = SweepTypes<SOLVER, EQ>;
-  using A = typename ST::A;
   using S = typename ST::S;
-  std::vector<AsmInst<A, S>> v(b->count);
+  std::vector<AsmInst<S>> v(b->count);
   for (int i = 0; i < b->count; ++i) {
     ixb_handle* h = b->h[i];
     const SweepShape s = sweep_shape(EQ, h->mi, h->nj, (int)sizeof(S), 1, 128);
-    AsmInst<A, S>& d = v[i];
-    if constexpr (std::is_same<A, float>::value) d.G = handle_geo32(h); else d.G = handle_geo(h);
+    AsmInst<S>& d = v[i];
+    d.G = handle_geo(h);
     d.io = io[i];
     S* base = static_cast<S*>(h->stage);
     d.co.a = base; d.co.b = base + h->stage_stride; d.co.c = base + 2 * h->stage_stride;
@@ -149,7 +148,7 @@ cudaError_t build_asm(ixb_batch* b, const std::vector<SweepIO<double>>& io, std:
     d.count = asm_tiles(EqIsX<EQ>::value, s.n, s.line_hi - s.line_lo + 1);
     for (int t = 0; t < d.count; ++t) items.push_back(make_int2(i, t));
   }
-  AsmInst<A, S>* dv = nullptr;
+  AsmInst<S>* dv = nullptr;
   cudaError_t e = upload(&dv, v);
   b->asm_inst[EQ] = dv;
   return e;

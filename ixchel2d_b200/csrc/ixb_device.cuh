@@ -82,26 +82,15 @@ __device__ __forceinline__ R ldg(const R* p, int i) { return __ldg(p + i); }
 // the field and the arithmetic are both binary64)
 template <class R, class F>
 __device__ __forceinline__ R ld(const F* p, int i) { return R(__ldg(p + i)); }
-// ... saturated at 1e38 when narrowed to binary32: au/av hold the
-// reference's 1e40 "no coefficient" marker (main.f90:309-310) on boundary
-// nodes, which would otherwise become an infinity
-template <class R, class F>
-__device__ __forceinline__ R ld_sat(const F* p, int i) {
-  if constexpr (sizeof(R) < sizeof(F)) return R(fmin(__ldg(p + i), F(1e38)));
-  else return R(__ldg(p + i));
-}
-
 template <class R>
 struct Geo {
   int mi, nj, LD, mstride;
   int tstride;     // elements per 2-D table (fields stay below 2^31 elements)
   const R* m;      // M_COUNT 1-D arrays
-  const double* m64;  // the same arrays in binary64 (== m when R is double)
   const R* tab;    // T_COUNT 2-D tables
   R gm, ge, Ri, Riy, dt, rel_vel, rel_pres, rel_ener, p_update;
   R inv_gm, inv_dt, inv_rel_vel, inv_rel_pres, inv_rel_ener;  // fast form
   __device__ __forceinline__ R met(int which, int k) const { return __ldg(m + which * mstride + k); }
-  __device__ __forceinline__ double met64(int which, int k) const { return __ldg(m64 + which * mstride + k); }
   __device__ __forceinline__ int at(int ii, int jj) const { return (jj - 1) * LD + (ii - 1); }
   __device__ __forceinline__ R t(int which, int ii, int jj) const { return __ldg(tab + which * tstride + at(ii, jj)); }
 };
@@ -403,14 +392,14 @@ template <class R, class F>
 __device__ __forceinline__ F mass_residual(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
   const int c0 = G.at(ii, jj);
   const F ud = ldg(io.u, c0), ui = ldg(io.u, G.at(ii - 1, jj)), vn = ldg(io.v, c0), vs = ldg(io.v, G.at(ii, jj - 1));
-  return (ui - ud) * F(G.met64(M_DYP, jj)) + (vs - vn) * F(G.met64(M_DXP, ii));
+  return (ui - ud) * F(G.met(M_DYP, jj)) + (vs - vn) * F(G.met(M_DXP, ii));
 }
 
 template <bool FAST, class R, class F>
 __device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj, F& bo) {
   const int c0 = G.at(ii, jj);
-  const R ai = ld_sat<R>(io.au, G.at(ii - 1, jj)), ad = ld_sat<R>(io.au, c0), as = ld_sat<R>(io.av, G.at(ii, jj - 1)),
-          an = ld_sat<R>(io.av, c0);
+  const R ai = ld<R>(io.au, G.at(ii - 1, jj)), ad = ld<R>(io.au, c0), as = ld<R>(io.av, G.at(ii, jj - 1)),
+          an = ld<R>(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   Row<R> r;
   r.a = -qdiv<FAST>(dyp * dyp, ai);
@@ -427,8 +416,8 @@ __device__ __forceinline__ Row<R> assemble_px(const Geo<R>& G, const SweepIO<F>&
 template <bool FAST, class R, class F>
 __device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<F>& io, int ii, int jj) {
   const int c0 = G.at(ii, jj);
-  const R ai = ld_sat<R>(io.au, G.at(ii - 1, jj)), ad = ld_sat<R>(io.au, c0), as = ld_sat<R>(io.av, G.at(ii, jj - 1)),
-          an = ld_sat<R>(io.av, c0);
+  const R ai = ld<R>(io.au, G.at(ii - 1, jj)), ad = ld<R>(io.au, c0), as = ld<R>(io.av, G.at(ii, jj - 1)),
+          an = ld<R>(io.av, c0);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   const R AI = -qdiv<FAST>(dyp * dyp, ai);
   const R AD = -qdiv<FAST>(dyp * dyp, ad);

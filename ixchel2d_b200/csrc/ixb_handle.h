@@ -48,8 +48,6 @@ struct ixb_handle {
   double* metrics = nullptr;
   int mstride = 0;
   double* tables = nullptr;  // T_COUNT mesh-constant 2-D tables
-  float* metrics32 = nullptr;  // binary32 copies (IXB_PREC_FP32_REFINED)
-  float* tables32 = nullptr;
   bool tables_dirty = true;
   double *xp_d = nullptr, *yp_d = nullptr;
   std::vector<double> xu, yv, xp, yp;
@@ -85,7 +83,6 @@ struct ixb_handle {
 namespace ixb {
 // views and state of a handle used by the batched driver (defined in ixb_api.cu)
 Geo<double> handle_geo(const ixb_handle* h);
-Geo<float> handle_geo32(const ixb_handle* h);
 int handle_solver_form(const ixb_handle* h);
 int handle_ready(ixb_handle* h);  // mesh, params and boundary tables set; mesh tables built
 // inputs/outputs of sweep `eq` at the current buffer parity (flips it), no norms

@@ -74,7 +74,6 @@ struct SweepTypes {
   static constexpr bool MIX = SOLVER == SOLVER_MIXED;
   static constexpr bool DC = MIX && EQ != EQ_PY && EQ != EQ_PX;
   using S = typename std::conditional<MIX, float, double>::type;  // staged rows, line solve
-  using A = double;                                               // row assembly
 };
 
 // x-sweep tiles: 64 consecutive rows of 8 lines; y-sweep tiles: 32 lines
@@ -129,9 +128,9 @@ constexpr int kAsmGridCap = 148 * 8;
 
 // One instance of a batched launch (see ixb_batch.cu): its views, and its
 // work items first .. first+count-1 in the launch's item list.
-template <class A, class S>
+template <class S>
 struct AsmInst {
-  Geo<A> G;
+  Geo<double> G;
   SweepIO<double> io;
   Coef<S> co;
   int n, line_lo, line_hi;
@@ -141,8 +140,8 @@ struct AsmInst {
 // per-equation assembly launchers (ixb_sweep_<eq>.cu: exact,
 // ixb_sweep_<eq>_fast.cu: hybrid, ixb_sweep_<eq>_mixed.cu: mixed precision)
 template <int EQ, int SOLVER>
-cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
-                            const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st);
+cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io,
+                            const StageBuf& buf, cudaStream_t st);
 template <int EQ, int SOLVER>
 cudaError_t assemble_batch_launch(const void* inst, const int2* items, int nitems, const int* active,
                                   const BatchNorm& bn, cudaStream_t st);
@@ -196,8 +195,8 @@ cudaError_t residual_batch_launch(const CellInst* inst, const int2* items, int n
 
 // kernel launchers (ixb_kernels.cu); return cudaError_t
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
-                             const Geo<float>& Gf, const SweepIO<double>& io, const StageBuf& buf,
-                             cudaStream_t st, const CtlRef& ctl = CtlRef{});
+                             const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st,
+                             const CtlRef& ctl = CtlRef{});
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
                                const double* au, const double* av, int fast, cudaStream_t st,
                                const CtlRef& gate = CtlRef{});
@@ -212,7 +211,6 @@ cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const doub
                                int vertical, int k0, int k1, double* out2, cudaStream_t st);
 cudaError_t sweep_set_smem_limits();
 cudaError_t launch_tables_f64(const Geo<double>& G, double* met, double* tab, cudaStream_t st);
-cudaError_t launch_narrow_f32(const double* src, float* dst, size_t n, cudaStream_t st);
 
 // batched standalone tridiagonal solvers (ixb_tridiag.cu)
 cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,

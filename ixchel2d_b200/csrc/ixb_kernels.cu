@@ -288,17 +288,17 @@ cudaError_t sweep_set_smem_limits() {
 // One sweep: the cell-parallel assembly stages the rows of every solved
 // line in `buf`, then the line solve writes the field.
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
-                             const Geo<float>& Gf, const SweepIO<double>& io, const StageBuf& buf,
-                             cudaStream_t st, const CtlRef& ctl) {
+                             const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st,
+                             const CtlRef& ctl) {
   cudaError_t e;
   if (solver == IXB_SOLVER_EXACT) {
-    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, IXB_SOLVER_EXACT>(s, G, Gf, io, buf, st)) };
+    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, IXB_SOLVER_EXACT>(s, G, io, buf, st)) };
     e = f();
   } else if (solver == SOLVER_MIXED) {
-    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, SOLVER_MIXED>(s, G, Gf, io, buf, st)) };
+    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, SOLVER_MIXED>(s, G, io, buf, st)) };
     e = f();
   } else {
-    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, IXB_SOLVER_HYBRID>(s, G, Gf, io, buf, st)) };
+    auto f = [&]() -> cudaError_t { IXB_EQ_SWITCH(return assemble_launch<E_, IXB_SOLVER_HYBRID>(s, G, io, buf, st)) };
     e = f();
   }
   if (e != cudaSuccess) return e;
@@ -307,17 +307,6 @@ cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<
   so.in = io.in; so.out = io.out; so.prev = io.prev; so.nrm0 = io.nrm0; so.ctl = ctl;
   so.LD = G.LD; so.m = s.m; so.mp = s.mp;
   return solve_launch(solver, eq_is_x(eq), eq_dc(eq, solver), s, so, st);
-}
-
-__global__ void narrow_f32_kernel(const double* __restrict__ src, float* __restrict__ dst, size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    dst[i] = (float)src[i];
-}
-
-cudaError_t launch_narrow_f32(const double* src, float* dst, size_t n, cudaStream_t st) {
-  const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
-  if (n) narrow_f32_kernel<<<grid, 256, 0, st>>>(src, dst, n);
-  return cudaGetLastError();
 }
 
 cudaError_t launch_preset_f64(double* pc, size_t n, const CtlRef& gate, cudaStream_t st) {

@@ -63,11 +63,6 @@ __device__ __forceinline__ Row<R> assemble_cell(const Geo<R>& G, const SweepIO<F
   }
 }
 
-template <class A>
-__host__ __device__ inline const Geo<A>& pick_geo(const Geo<double>& d, const Geo<float>& f) {
-  if constexpr (std::is_same<A, float>::value) return f; else return d;
-}
-
 // Boundary rows of impone_cond_frontera (source/mod_cond_frontera.f90:280-416):
 // first row of a line: diri (0,1,0|val), neum (0,-1,1|val);
 // last row: diri (0,1,0|val), neum (-1,1,0|val).  p' rows are hard-coded
@@ -95,11 +90,11 @@ __device__ __forceinline__ Row<R> bc_last_row(const BCEntry* t, int L) {
 // at the nearest interior cell and then replaced, so every load is in bounds
 // and no branch separates a thread's loads.
 template <int EQ, int SOLVER>
-__device__ __forceinline__ Row<typename SweepTypes<SOLVER, EQ>::A> staged_row(
-    const Geo<typename SweepTypes<SOLVER, EQ>::A>& Gm, const SweepIO<double>& io, int L, int r, int n, int line_lo,
+__device__ __forceinline__ Row<double> staged_row(
+    const Geo<double>& Gm, const SweepIO<double>& io, int L, int r, int n, int line_lo,
     int line_hi, bool valid, double& acc_bo) {
   using ST = SweepTypes<SOLVER, EQ>;
-  using A = typename ST::A;
+  using A = double;
   constexpr bool X = EqIsX<EQ>::value;
   const int Lc = min(max(L, line_lo), line_hi);
   const int rc = min(max(r, 1), n - 2);
@@ -138,7 +133,7 @@ __device__ __forceinline__ Row<typename SweepTypes<SOLVER, EQ>::A> staged_row(
 // written to `co` (line L at (L - line_lo) * P).  Called by all threads of
 // the CTA (a y tile holds barriers around its shared-memory transpose).
 template <int EQ, int SOLVER>
-__device__ __forceinline__ void assemble_tile(const Geo<typename SweepTypes<SOLVER, EQ>::A>& G_,
+__device__ __forceinline__ void assemble_tile(const Geo<double>& G_,
                                               const SweepIO<double>& io,
                                               const Coef<typename SweepTypes<SOLVER, EQ>::S>& co, const int n,
                                               const int line_lo, const int line_hi, const int tile, double& acc_bo,
@@ -194,7 +189,7 @@ __device__ __forceinline__ void assemble_tile(const Geo<typename SweepTypes<SOLV
 // Grid-stride over tiles; the b_o norm (p'-x) is reduced over the grid.
 template <int EQ, int SOLVER>
 __global__ void __launch_bounds__(kAsmThreads)
-    assemble_kernel(const Geo<typename SweepTypes<SOLVER, EQ>::A> G_, const SweepIO<double> io,
+    assemble_kernel(const Geo<double> G_, const SweepIO<double> io,
                     const Coef<typename SweepTypes<SOLVER, EQ>::S> co, const int n, const int line_lo,
                     const int line_hi) {
   IXB_PDL_ENTRY();
@@ -215,7 +210,7 @@ __global__ void __launch_bounds__(kAsmThreads)
 // b_o norm is reduced per instance over its items (finish_item_norm).
 template <int EQ, int SOLVER>
 __global__ void __launch_bounds__(kAsmThreads)
-    assemble_batch_kernel(const AsmInst<typename SweepTypes<SOLVER, EQ>::A, typename SweepTypes<SOLVER, EQ>::S>*
+    assemble_batch_kernel(const AsmInst<typename SweepTypes<SOLVER, EQ>::S>*
                               __restrict__ inst,
                           const int2* __restrict__ items, const int nitems, const int* __restrict__ active,
                           const BatchNorm bn) {
@@ -238,22 +233,20 @@ cudaError_t assemble_batch_launch(const void* inst, const int2* items, int nitem
   using ST = SweepTypes<SOLVER, EQ>;
   const int grid = std::max(1, std::min(nitems, kAsmGridCap * 4));
   return launch_k(assemble_batch_kernel<EQ, SOLVER>, grid, kAsmThreads, 0, st,
-                  static_cast<const AsmInst<typename ST::A, typename ST::S>*>(inst), items, nitems, active, bn);
+                  static_cast<const AsmInst<typename ST::S>*>(inst), items, nitems, active, bn);
 }
 
 template <int EQ, int SOLVER>
-cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& Gd, const Geo<float>& Gf,
-                            const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st) {
-  using ST = SweepTypes<SOLVER, EQ>;
-  using S = typename ST::S;
-  const auto& Gm = pick_geo<typename ST::A>(Gd, Gf);
+cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io,
+                            const StageBuf& buf, cudaStream_t st) {
+  using S = typename SweepTypes<SOLVER, EQ>::S;
   Coef<S> co;
   S* base = static_cast<S*>(buf.base);
   co.a = base; co.b = base + buf.stride; co.c = base + 2 * buf.stride; co.d = base + 3 * buf.stride;
   co.P = buf.P;
   const int tiles = asm_tiles(EqIsX<EQ>::value, s.n, s.line_hi - s.line_lo + 1);
   const int grid = std::max(1, std::min(tiles, kAsmGridCap));
-  return launch_k(assemble_kernel<EQ, SOLVER>, grid, kAsmThreads, 0, st, Gm, io, co, s.n, s.line_lo, s.line_hi);
+  return launch_k(assemble_kernel<EQ, SOLVER>, grid, kAsmThreads, 0, st, G, io, co, s.n, s.line_lo, s.line_hi);
 }
 
 }  // namespace ixb

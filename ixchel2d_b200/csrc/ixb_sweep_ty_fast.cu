@@ -2,7 +2,7 @@
 #include "ixb_sweep.cuh"
 
 namespace ixb {
-template cudaError_t assemble_launch<EQ_TY, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&, const Geo<float>&,
+template cudaError_t assemble_launch<EQ_TY, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&,
                                                                const SweepIO<double>&, const StageBuf&, cudaStream_t);
 template cudaError_t assemble_batch_launch<EQ_TY, IXB_SOLVER_HYBRID>(const void*, const int2*, int, const int*, const BatchNorm&,
                                                            cudaStream_t);

@@ -2,6 +2,6 @@
 #include "ixb_sweep.cuh"
 
 namespace ixb {
-template cudaError_t assemble_launch<EQ_VY, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&, const Geo<float>&,
+template cudaError_t assemble_launch<EQ_VY, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&,
                                                               const SweepIO<double>&, const StageBuf&, cudaStream_t);
 }  // namespace ixb
