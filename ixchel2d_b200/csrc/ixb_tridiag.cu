@@ -8,12 +8,16 @@
 // coalesced.
 //
 // layout 1 (systems interleaved, row i of system s at i*nsys+s, like the
-// y-lines of a column-major field): one thread per system walks the rows;
-// consecutive threads touch consecutive addresses.  The forward sweep keeps
-// its modified diagonal (exact) or normalised super-diagonal (hybrid) in a
+// y-lines of a column-major field): the hybrid solver runs the cluster
+// kernel below (tri_strided_kernel: groups of 128-byte row segments in 2-D
+// tensor tiles, n <= 4096).  The exact solver, and sizes or alignments that
+// kernel does not take, use one thread per system walking the rows;
+// consecutive threads touch consecutive addresses.  Its forward sweep keeps
+// the modified diagonal (exact) or normalised super-diagonal (hybrid) in a
 // scratch array of n*nsys elements taken from the stream-ordered allocator,
 // and the modified right-hand side in x.
 #include <cooperative_groups.h>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -333,72 +337,271 @@ cudaError_t stream_solve(const R* a, const R* b, const R* c, const R* d, R* x, i
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Interleaved systems (row i of system s at i*nsys + s), hybrid solver: a
-// thread-block cluster of Q CTAs solves W adjacent systems at a time, CTA q
-// holding rows q*R .. q*R+R-1 (R = (T/W)*M) of all W systems.  Thread t owns
-// rows k*M .. k*M+M-1 (k = t / W) of system w = t % W, so a warp's loads and
-// stores cover 32/W rows of W adjacent systems: whole 32-byte sectors.  Each
-// thread eliminates its rows in registers (modified Thomas) to two rows; the
-// 2*Q*(T/W) reduced rows of system w are gathered in the shared memory of
-// cluster rank w (distributed shared memory) and solved there by PCR; every
-// thread reads its two solutions back and back-substitutes.  The reduced
-// rows are double-buffered across system groups, so a group costs two
-// cluster barriers.  No bulk copies: plain coalesced loads from registers of
-// several resident clusters per SM keep the memory system busy.
+// Interleaved systems (row i of system s at i*nsys + s), hybrid solver.
+// A group of W adjacent systems occupies W*sizeof(R) = 128 contiguous bytes
+// of every row: whole 128-byte segments, the narrowest access that streams
+// from HBM at full rate (32-byte segments, 4 binary64 systems, stream at
+// under 40 % of it).  A thread-block cluster of Q CTAs (one per SM) solves
+// one group at a time, CTA q holding rows q*256 .. q*256+255 of all W
+// systems: thread t owns rows k*16 .. k*16+15 (k = t / W) of system
+// w = t % W.  Each group arrives as four 2-D tiles (a, b, c, d; box W x 256
+// rows, copied by the tensor engine without multicast) in shared memory
+// while the CTA is still solving the previous group from registers.  Every
+// thread eliminates its 16 rows (modified Thomas) to two rows coupled to the
+// neighbouring chunks.  The 32Q reduced rows of system w are solved in
+// cluster rank w % Q (its owner) by one warp (Thomas-PCR on 32 lanes): every
+// CTA stages its reduced rows in the owners' layout and sends each owner its
+// runs by bulk shared-to-shared copies that complete on the owner's mbarrier.
+// After a cluster barrier every thread reads its two solutions back and
+// back-substitutes into a solution tile that the tensor engine stores.  The
+// reduced rows are double-buffered across groups.  Every wait on a copy is
+// bounded (g_tri_timeout, as above).
 // ---------------------------------------------------------------------------
 namespace {
 
 namespace cg = cooperative_groups;
 
-template <int W, int T, int M>
-struct StridedShape {
-  static constexpr int C = T / W;  // chunks per CTA per system
-  static constexpr int R = C * M;  // rows per CTA
+constexpr int kStrRows = 256;            // rows per CTA (one 2-D tile box)
+constexpr int kStrM = 16;                // rows per thread
+constexpr int kStrC = kStrRows / kStrM;  // chunks per CTA per system
+
+template <class R>
+struct StridedCfg {
+  static constexpr int W = 128 / (int)sizeof(R);  // systems per group: 16 (binary64) or 32 (binary32)
+  static constexpr int T = W * kStrC;             // threads per CTA: 256 or 512
+  static constexpr int TILE = W * kStrRows;       // elements per tile
+  // one set of gathered reduced rows: a | c | d of the W / Q owned systems,
+  // 32 lane chunks of Q rows at pitch Q + 2 each (even, so that a chunk's
+  // two reduced rows are one aligned pair): at most 48 W rows (Q = 4)
+  static constexpr int SETA = 48 * W;
+  // a CTA's rows for one owned system of one owner are one run of
+  // (32 / Q) lane chunks: at most 48 elements (Q = 4); W runs per array
+  static constexpr int RUN = 48;
 };
 
-// reduced-row buffers of one CTA: 2 sets x ((a | c | d) x NR gathered rows
-// + the PCR buffers of T threads)
+// shared memory (bytes): 4 input tiles, the solution tile, 2 sets of
+// gathered reduced rows, the outgoing runs, 3 mbarriers (tiles, 2 sets)
 template <class R>
-__host__ __device__ constexpr size_t strided_set_elems(int nr, int t) {
-  return (size_t)3 * nr + (size_t)12 * t;
-}
-template <class R>
-__host__ __device__ constexpr size_t strided_smem_bytes(int nr, int t) {
-  return 2 * strided_set_elems<R>(nr, t) * sizeof(R);
+__host__ __device__ constexpr size_t strided_smem_bytes() {
+  using SC = StridedCfg<R>;
+  return ((size_t)5 * SC::TILE + 2 * 3 * (size_t)SC::SETA + 3 * (size_t)SC::W * SC::RUN) * sizeof(R) + 32;
 }
 
-template <class R, int W, int T, int M>
-__global__ void __launch_bounds__(T) tri_strided_kernel(const R* __restrict__ a, const R* __restrict__ b,
-                                                        const R* __restrict__ c, const R* __restrict__ d,
-                                                        R* __restrict__ x, int n, int nsys) {
-  using SS = StridedShape<W, T, M>;
+__device__ __forceinline__ void tile_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tile_store_2d(const CUtensorMap* map, int x, int y, const void* src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(smem_u32(src))
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// shared::cluster address of `local`'s counterpart in cluster rank `rank`
+__device__ __forceinline__ unsigned cluster_smem_addr(const void* local, int rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(local)), "r"(rank));
+  return r;
+}
+
+// bulk copy from this CTA's shared memory to cluster shared memory,
+// completing on the destination's mbarrier
+__device__ __forceinline__ void bulk_send(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst),
+               "r"(smem_u32(src)), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// One warp solves a system of 32*m rows (m >= 2) with unit diagonals:
+// x_i + a_i x_{i-1} + c_i x_{i+1} = d_i, lane l's rows at l*pitch ..
+// l*pitch+m-1 of the arrays a, c, d.  Each lane eliminates its rows to the
+// first and last (modified Thomas, as in thomas_pcr_warp, its intermediate
+// rows in the scratch arrays sa, sc, sd so that the inputs are only read),
+// the 64 rows are solved by PCR over register shuffles, and each lane
+// back-substitutes.  The solution replaces d.
+template <class R, int m>
+__device__ __forceinline__ void warp_unit_solve(const R* __restrict__ a, const R* __restrict__ c, R* __restrict__ d,
+                                                R* __restrict__ sa, R* __restrict__ sc, R* __restrict__ sd,
+                                                int pitch) {
+  const int lane = threadIdx.x & 31;
+  const R* la = a + lane * pitch;
+  const R* lc = c + lane * pitch;
+  R* ld = d + lane * pitch;
+  R* xa = sa + lane * pitch;
+  R* xc = sc + lane * pitch;
+  R* xd = sd + lane * pitch;
+  R eA, eC, eD, oA, oC, oD;
+  if constexpr (m == 2) {
+    eA = la[0]; eC = lc[0]; eD = ld[0];
+    oA = la[1]; oC = lc[1]; oD = ld[1];
+  } else {
+    // forward: rows 1..m-1 -> x_k + a'_k x_0 + c'_k x_{k+1} = d'_k
+    R ap = la[1], cp = lc[1], dp = ld[1];
+    xa[1] = ap; xc[1] = cp; xd[1] = dp;
+#pragma unroll
+    for (int k = 2; k < m; ++k) {
+      const R ak = la[k];
+      const R r = fast_rcp(fmaT(-ak, cp, R(1)));
+      ap = -ak * ap * r;
+      dp = fmaT(-ak, dp, ld[k]) * r;
+      cp = lc[k] * r;
+      xa[k] = ap; xc[k] = cp; xd[k] = dp;
+    }
+    oA = ap; oC = cp; oD = dp;
+    // backward: rows m-3..1 -> x_k + a''_k x_0 + c''_k x_{m-1} = d''_k
+    R an = xa[m - 2], cn = xc[m - 2], dn = xd[m - 2];
+#pragma unroll
+    for (int k = m - 3; k >= 1; --k) {
+      const R ck = xc[k];
+      dn = fmaT(-ck, dn, xd[k]);
+      an = fmaT(-ck, an, xa[k]);
+      cn = -ck * cn;
+      xa[k] = an; xc[k] = cn; xd[k] = dn;
+    }
+    const R c0 = lc[0];
+    const R r0 = fast_rcp(fmaT(-c0, an, R(1)));
+    eA = la[0] * r0; eC = -c0 * cn * r0; eD = fmaT(-c0, dn, ld[0]) * r0;
+  }
+  // PCR on the 64 interleaved rows (even: first rows, odd: last rows), unit
+  // diagonals kept by normalising every step
+  auto step = [](R& A, R& C, R& D, R lA, R lC, R lD, R hA, R hC, R hD) {
+    const R r = fast_rcp(fmaT(-C, hA, fmaT(-A, lC, R(1))));
+    const R nA = -A * lA * r, nC = -C * hC * r, nD = fmaT(-C, hD, fmaT(-A, lD, D)) * r;
+    A = nA; C = nC; D = nD;
+  };
+  {  // row stride 1: even rows see the odd row of lane-1 and their own; odd rows their own even and lane+1's
+    R lA = shfl_up_r(oA, 1), lC = shfl_up_r(oC, 1), lD = shfl_up_r(oD, 1);
+    R hA = shfl_dn_r(eA, 1), hC = shfl_dn_r(eC, 1), hD = shfl_dn_r(eD, 1);
+    if (lane == 0) { lA = R(0); lC = R(0); lD = R(0); }
+    if (lane == 31) { hA = R(0); hC = R(0); hD = R(0); }
+    const R e0A = eA, e0C = eC, e0D = eD;
+    step(eA, eC, eD, lA, lC, lD, oA, oC, oD);
+    step(oA, oC, oD, e0A, e0C, e0D, hA, hC, hD);
+  }
+#pragma unroll
+  for (int dl = 1; dl < 32; dl <<= 1) {  // row stride 2*dl: same-parity rows of lanes +-dl
+    R lEA = shfl_up_r(eA, dl), lEC = shfl_up_r(eC, dl), lED = shfl_up_r(eD, dl);
+    R hEA = shfl_dn_r(eA, dl), hEC = shfl_dn_r(eC, dl), hED = shfl_dn_r(eD, dl);
+    R lOA = shfl_up_r(oA, dl), lOC = shfl_up_r(oC, dl), lOD = shfl_up_r(oD, dl);
+    R hOA = shfl_dn_r(oA, dl), hOC = shfl_dn_r(oC, dl), hOD = shfl_dn_r(oD, dl);
+    if (lane < dl) { lEA = R(0); lEC = R(0); lED = R(0); lOA = R(0); lOC = R(0); lOD = R(0); }
+    if (lane + dl > 31) { hEA = R(0); hEC = R(0); hED = R(0); hOA = R(0); hOC = R(0); hOD = R(0); }
+    step(eA, eC, eD, lEA, lEC, lED, hEA, hEC, hED);
+    step(oA, oC, oD, lOA, lOC, lOD, hOA, hOC, hOD);
+  }
+  const R x0 = eD, xl = oD;
+  ld[0] = x0;
+#pragma unroll
+  for (int k = 1; k < m - 1; ++k) ld[k] = fmaT(-xc[k], xl, fmaT(-xa[k], x0, xd[k]));
+  ld[m - 1] = xl;
+}
+
+// pairs of adjacent elements (16 bytes in binary64, 8 in binary32)
+template <class R>
+struct Pair2;
+template <>
+struct Pair2<double> { using type = double2; };
+template <>
+struct Pair2<float> { using type = float2; };
+
+template <class R>
+__global__ void __launch_bounds__(StridedCfg<R>::T, 1)
+    tri_strided_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                       const __grid_constant__ CUtensorMap mapC, const __grid_constant__ CUtensorMap mapD,
+                       const __grid_constant__ CUtensorMap mapX, int n, int nsys) {
+  using SC = StridedCfg<R>;
+  using P2 = typename Pair2<R>::type;
+  constexpr int W = SC::W, T = SC::T, M = kStrM;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  R* sm = reinterpret_cast<R*>(smem_raw);
+  R* tile = reinterpret_cast<R*>(smem_raw);  // a | b | c | d, [row][system] each
+  R* xt = tile + 4 * SC::TILE;               // solution tile
+  R* sets = xt + SC::TILE;                   // 2 x (a | c | d), SETA each
+  R* outr = sets + 2 * 3 * SC::SETA;         // outgoing runs: [array][w][RUN]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(outr + 3 * W * SC::RUN);  // tiles
+  uint64_t* rbar = bar + 1;                                            // reduced rows of set 0, 1
   cg::cluster_group cluster = cg::this_cluster();
-  const int Q = (int)cluster.num_blocks();
+  const int Q = (int)cluster.num_blocks();  // 4, 8 or 16
   const int rank = (int)cluster.block_rank();
-  const int NR = 2 * Q * SS::C;  // reduced rows per system
+  const int S = W / Q;                       // systems each CTA owns
+  const int pitch = Q + 2;                   // lane chunks of Q reduced rows, padded
+  const int sysP = 32 * pitch;               // one owned system in a set array
+  const int run = (32 / Q) * pitch;          // this CTA's part of one owned system
   const int tid = threadIdx.x;
   const int w = tid % W, k = tid / W;
-  const int row0 = rank * SS::R + k * M;
+  const int owner = w % Q, slot = w / Q;  // system w's reduced rows: rank `owner`, slot `slot`
+  const int row0 = rank * kStrRows + k * M;
   const int nclusters = gridDim.x / Q;
   const int cl = blockIdx.x / Q;
   const int ngroups = (nsys + W - 1) / W;
+  const bool stores = rank * kStrRows < n;  // CTAs wholly past the last row store nothing
+  // this chunk's reduced rows 2i, 2i+1 (i = rank*C + k): their pair in the
+  // run for system w and in the owner's set (Q and 2i are even: one lane
+  // chunk, even position)
+  const int i2 = 2 * (rank * kStrC + k);
+  const int q_run = ((2 * k) / Q) * pitch + (2 * k) % Q;
+  const int p_e = slot * sysP + (i2 / Q) * pitch + i2 % Q;
+  // bytes an owner receives per group: Q senders x S systems x 3 arrays x run
+  const unsigned recv_bytes = (unsigned)(3 * W * run * sizeof(R));
+  constexpr unsigned kTileBytes = (unsigned)(SC::TILE * sizeof(R));
+  auto issue = [&](int g) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of the tiles precede the copies
+    mbar_expect_tx(bar, 4 * kTileBytes);
+    tile_load_2d(tile, &mapA, g * W, rank * kStrRows, bar);
+    tile_load_2d(tile + SC::TILE, &mapB, g * W, rank * kStrRows, bar);
+    tile_load_2d(tile + 2 * SC::TILE, &mapC, g * W, rank * kStrRows, bar);
+    tile_load_2d(tile + 3 * SC::TILE, &mapD, g * W, rank * kStrRows, bar);
+  };
+  if (tid == 0) {
+    mbar_init(bar);
+    mbar_init(rbar);
+    mbar_init(rbar + 1);
+  }
+  cluster.sync();  // every CTA of the cluster runs and its mbarriers are set up
+  if (tid == 0 && cl < ngroups) issue(cl);
+  unsigned parity = 0, rpar = 0;
+  bool failed = false;
   int set = 0;
   for (int g = cl; g < ngroups; g += nclusters, set ^= 1) {
     const int sys = g * W + w;
     const bool live = sys < nsys;
+    if (tid == 0) mbar_expect_tx(rbar + set, recv_bytes);  // this group's reduced rows, from every CTA
+    if (!failed) {
+      const bool ok = mbar_wait_bounded(bar, parity);
+      failed = __syncthreads_or(!ok);
+      parity ^= 1;
+    }
+    // own rows into registers; row 0 has no a, row n-1 no c, and rows or
+    // systems outside the problem (zeros in the tiles) become identity rows
     R ra[M], rb[M], rc[M], rd[M];
 #pragma unroll
     for (int j = 0; j < M; ++j) {
-      const int r = row0 + j;
-      const bool in = live && r < n;
-      const size_t o = (size_t)(in ? r : 0) * nsys + (live ? sys : 0);
-      ra[j] = (in && r > 0) ? __ldg(a + o) : R(0);
-      rb[j] = in ? __ldg(b + o) : R(1);
-      rc[j] = (in && r < n - 1) ? __ldg(c + o) : R(0);
-      rd[j] = in ? __ldg(d + o) : R(0);
+      const int o = (k * M + j) * W + w;
+      ra[j] = tile[o];
+      rb[j] = tile[SC::TILE + o];
+      rc[j] = tile[2 * SC::TILE + o];
+      rd[j] = tile[3 * SC::TILE + o];
     }
+    if (!(live && row0 >= 1 && row0 + M <= n - 1)) {
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const int r = row0 + j;
+        if (!(live && r < n)) {
+          ra[j] = R(0); rb[j] = R(1); rc[j] = R(0); rd[j] = R(0);
+        } else {
+          if (r == 0) ra[j] = R(0);
+          if (r == n - 1) rc[j] = R(0);
+        }
+      }
+    }
+    __syncthreads();  // the tiles are free: start loading the cluster's next group
+    if (tid == 0 && !failed && g + nclusters < ngroups) issue(g + nclusters);
     // modified Thomas on the own rows (as in the contiguous kernels)
     R inv = fast_rcp(rb[1]);
     R ap = ra[1] * inv, cp = rc[1] * inv, dp = rd[1] * inv;
@@ -423,117 +626,149 @@ __global__ void __launch_bounds__(T) tri_strided_kernel(const R* __restrict__ a,
     }
     const R r0 = fast_rcp(fmaT(-rc[0], an, rb[0]));
     const R eA = ra[0] * r0, eC = -rc[0] * cn * r0, eD = fmaT(-rc[0], dn, rd[0]) * r0;
-    // reduced rows 2i, 2i+1 (i = rank*C + k) of system w -> shared memory of rank w
-    R* base = sm + (size_t)set * strided_set_elems<R>(NR, T);  // this set: a | c | d, then PCR buffers
+    // the chunk's reduced rows -> the run for its system, then every run to
+    // its owner (the previous group's runs were read before its barrier)
     {
-      R* dst = cluster.map_shared_rank(base, w % Q);
-      const int i = 2 * (rank * SS::C + k);
-      dst[i] = eA; dst[NR + i] = eC; dst[2 * NR + i] = eD;
-      dst[i + 1] = ap; dst[NR + i + 1] = cp; dst[2 * NR + i + 1] = dp;
+      P2* o = reinterpret_cast<P2*>(outr + w * SC::RUN + q_run);
+      o[0] = P2{eA, ap};
+      o[W * SC::RUN / 2] = P2{eC, cp};
+      o[W * SC::RUN] = P2{eD, dp};
     }
-    cluster.sync();
-    if (rank < W) {  // owner of system `rank` of this group: solve its NR reduced rows
-      // every thread takes RPT consecutive rows (padding rows beyond NR are
-      // identity rows, decoupled); with 4 rows it first eliminates its two
-      // middle rows (modified Thomas on 4 rows), so the PCR runs on 2 rows
-      // per thread
-      constexpr int RPT = 16 / W;  // NR / T: 4 (binary64, W = 4) or 2 (binary32, W = 8)
-      R ea[RPT], ec[RPT], ed[RPT];
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        const int i = RPT * tid + q;
-        const bool in = i < NR;
-        ea[q] = in ? base[i] : R(0);
-        ec[q] = in ? base[NR + i] : R(0);
-        ed[q] = in ? base[2 * NR + i] : R(0);
-      }
-      R eA, eC, eD, oA, oC, oD, x0, xl;
-      R m1a = R(0), m1c = R(0), m1d = R(0), m2a = R(0), m2c = R(0), m2d = R(0);
-      if constexpr (RPT == 4) {
-        // forward: rows 1..3 -> x_k + a'_k x_0 + c'_k x_{k+1} = d'_k (unit diagonals)
-        R ap = ea[1], cp = ec[1], dp = ed[1];
-        m1a = ap; m1c = cp; m1d = dp;
-        R r = fast_rcp(fmaT(-ea[2], cp, R(1)));
-        ap = -ea[2] * ap * r; dp = fmaT(-ea[2], dp, ed[2]) * r; cp = ec[2] * r;
-        m2a = ap; m2c = cp; m2d = dp;
-        r = fast_rcp(fmaT(-ea[3], cp, R(1)));
-        oA = -ea[3] * ap * r; oD = fmaT(-ea[3], dp, ed[3]) * r; oC = ec[3] * r;
-        // backward: row 1 -> x_1 + a''_1 x_0 + c''_1 x_3 = d''_1
-        const R dn = fmaT(-m1c, m2d, m1d), an = fmaT(-m1c, m2a, m1a), cn = -m1c * m2c;
-        m1a = an; m1c = cn; m1d = dn;
-        const R r0 = fast_rcp(fmaT(-ec[0], an, R(1)));
-        eA = ea[0] * r0; eC = -ec[0] * cn * r0; eD = fmaT(-ec[0], dn, ed[0]) * r0;
-      } else {
-        eA = ea[0]; eC = ec[0]; eD = ed[0];
-        oA = ea[RPT - 1]; oC = ec[RPT - 1]; oD = ed[RPT - 1];
-      }
-      reduced_pcr<R, T>(base + 3 * NR, tid, true, eA, eC, eD, oA, oC, oD, x0, xl);
-      // solutions of the owned rows -> base[2*NR + i], where the other CTAs read them
-      if (RPT * tid < NR) {
-        base[2 * NR + RPT * tid] = x0;
-        if constexpr (RPT == 4) {
-          base[2 * NR + 4 * tid + 1] = fmaT(-m1c, xl, fmaT(-m1a, x0, m1d));
-          base[2 * NR + 4 * tid + 2] = fmaT(-m2c, xl, fmaT(-m2a, x0, m2d));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> copy engine
+    __syncthreads();
+    R* own = sets + (size_t)set * 3 * SC::SETA;  // this group's set: a | c | d
+    if (tid < 3 * W && !failed) {
+      const int arr = tid / W, ws = tid % W;  // run of system ws, array arr
+      const int dst = arr * SC::SETA + (ws / Q) * sysP + (32 / Q) * rank * pitch;
+      bulk_send(cluster_smem_addr(own + dst, ws % Q), outr + (arr * W + ws) * SC::RUN,
+                (unsigned)(run * sizeof(R)), cluster_smem_addr(rbar + set, ws % Q));
+    }
+    if (!failed) {
+      const bool ok = mbar_wait_bounded(rbar + set, (rpar >> set) & 1u);
+      failed = __syncthreads_or(!ok);
+      rpar ^= 1u << set;
+    }
+    // one warp per owned system (S of them, 32Q rows each); the other set,
+    // idle until this group's barrier, holds the intermediate rows
+    {
+      R* scr = sets + (size_t)(set ^ 1) * 3 * SC::SETA;
+      for (int s = tid >> 5; s < S; s += T / 32) {
+        const int o = s * sysP;
+        R* A = own + o;
+        R* Cc = own + SC::SETA + o;
+        R* D = own + 2 * SC::SETA + o;
+        R* sa = scr + o;
+        R* sc = scr + SC::SETA + o;
+        R* sd = scr + 2 * SC::SETA + o;
+        switch (Q) {
+          case 4: warp_unit_solve<R, 4>(A, Cc, D, sa, sc, sd, pitch); break;
+          case 8: warp_unit_solve<R, 8>(A, Cc, D, sa, sc, sd, pitch); break;
+          default: warp_unit_solve<R, 16>(A, Cc, D, sa, sc, sd, pitch); break;
         }
-        base[2 * NR + RPT * tid + RPT - 1] = xl;
       }
     }
+    if (tid == 0) bulk_store_wait_read();  // the previous solution tile has been read out
     cluster.sync();
-    // solutions of the own reduced rows, from rank w
-    const R* sol = cluster.map_shared_rank(base + 2 * NR, w % Q);
-    const int i = 2 * (rank * SS::C + k);
-    const R x0 = sol[i], xl = sol[i + 1];
+    const P2 sol = *reinterpret_cast<const P2*>(cluster.map_shared_rank(own + 2 * SC::SETA, owner) + p_e);
+    const R x0 = sol.x, xl = sol.y;
 #pragma unroll
-    for (int j = 0; j < M; ++j) {
-      const int r = row0 + j;
-      if (live && r < n) {
-        const R xv = j == 0 ? x0 : (j == M - 1 ? xl : fmaT(-rc[j], xl, fmaT(-ra[j], x0, rd[j])));
-        x[(size_t)r * nsys + sys] = xv;
-      }
+    for (int j = 0; j < M; ++j)
+      xt[(k * M + j) * W + w] = j == 0 ? x0 : (j == M - 1 ? xl : fmaT(-rc[j], xl, fmaT(-ra[j], x0, rd[j])));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor engine
+    __syncthreads();
+    // rows past n and systems past nsys fall outside the map and are not written
+    if (tid == 0 && !failed && stores) tile_store_2d(&mapX, g * W, rank * kStrRows, xt);
+  }
+  if (tid == 0) {
+    if (failed) {
+      atomicExch(&g_tri_timeout, 1);
+      mbar_wait_bounded(bar, parity);  // copies still in flight land before the CTA leaves
+      mbar_wait_bounded(rbar, rpar & 1u);
+      mbar_wait_bounded(rbar + 1, (rpar >> 1) & 1u);
     }
+    bulk_store_wait_all();
   }
   cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
 
-template <class R, int W, int T, int M>
-cudaError_t strided_launch(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
-  using SS = StridedShape<W, T, M>;
-  const int Q = (n + SS::R - 1) / SS::R;
-  if (Q < W || Q > 8) return cudaErrorInvalidValue;  // one owner CTA per system of a group
-  const int nr = 2 * Q * SS::C;
-  const size_t smem = strided_smem_bytes<R>(nr, T);
-  auto k = tri_strided_kernel<R, W, T, M>;
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependence on the driver library)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// [n rows][nsys systems] in tiles of W systems x 256 rows; rows and systems
+// past the ends read as zeros and are not written
+template <class R>
+bool strided_map(CUtensorMap* map, const R* p, int n, int nsys) {
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)nsys, (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)nsys * sizeof(R)};
+  const cuuint32_t box[2] = {(cuuint32_t)StridedCfg<R>::W, (cuuint32_t)kStrRows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(map, dt, 2, const_cast<R*>(p), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// cudaErrorInvalidValue: outside the kernel's range (n > 16*256 rows, a row
+// pitch or base address the tensor copies cannot take, or no room for a
+// cluster of Q CTAs); the caller then uses the general interleaved kernel
+template <class R>
+cudaError_t strided_solve(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
+  using SC = StridedCfg<R>;
+  if (n < 1 || n > 16 * kStrRows || nsys < 1) return cudaErrorInvalidValue;
+  const uintptr_t all = (uintptr_t)a | (uintptr_t)b | (uintptr_t)c | (uintptr_t)d | (uintptr_t)x;
+  if ((all & 15) != 0 || ((size_t)nsys * sizeof(R)) % 16 != 0) return cudaErrorInvalidValue;
+  int Q = 4;  // CTAs per cluster: a power of two >= 4 (W / Q systems of 32 lane chunks on each owner)
+  while (Q * kStrRows < n) Q <<= 1;
+  CUtensorMap maps[5];
+  if (!strided_map(&maps[0], a, n, nsys) || !strided_map(&maps[1], b, n, nsys) ||
+      !strided_map(&maps[2], c, n, nsys) || !strided_map(&maps[3], d, n, nsys) ||
+      !strided_map(&maps[4], static_cast<const R*>(x), n, nsys))
+    return cudaErrorInvalidValue;
+  auto k = tri_strided_kernel<R>;
+  const size_t smem = strided_smem_bytes<R>();
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  if (Q > 8 && (e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+    return e;
   cudaLaunchConfig_t cfg{};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = Q;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
-  cfg.blockDim = dim3(T);
+  cfg.blockDim = dim3(SC::T);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cfg.gridDim = dim3(Q);
   int max_clusters = 0;
-  if ((e = cudaOccupancyMaxActiveClusters(&max_clusters, k, &cfg)) != cudaSuccess) return e;
-  if (max_clusters < 1) return cudaErrorInvalidValue;
-  const int ngroups = (nsys + W - 1) / W;
+  if (cudaOccupancyMaxActiveClusters(&max_clusters, k, &cfg) != cudaSuccess || max_clusters < 1) {
+    cudaGetLastError();
+    return cudaErrorInvalidValue;
+  }
+  const int ngroups = (nsys + SC::W - 1) / SC::W;
   cfg.gridDim = dim3(Q * std::min(ngroups, max_clusters));
-  e = cudaLaunchKernelEx(&cfg, k, a, b, c, d, x, n, nsys);
+  e = cudaLaunchKernelEx(&cfg, k, maps[0], maps[1], maps[2], maps[3], maps[4], n, nsys);
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
-}
-
-// binary64: 4 systems (one 32-byte sector per row) x 32 chunks of 16 rows
-// per CTA of 128 threads; binary32: 8 systems x 32 chunks of 16 rows per
-// CTA of 256 threads.  Both cover up to 8 x 512 = 4096 rows per system.
-template <class R>
-cudaError_t strided_solve(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
-  if constexpr (sizeof(R) == 8) return strided_launch<R, 4, 128, 16>(a, b, c, d, x, n, nsys, st);
-  else return strided_launch<R, 8, 256, 16>(a, b, c, d, x, n, nsys, st);
 }
 
 }  // namespace

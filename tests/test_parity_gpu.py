@@ -257,7 +257,8 @@ def test_simple_before_setup_is_refused():
 # batched tridiagonal entry points (device pointers via torch)
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("layout", [0, 1])
-@pytest.mark.parametrize("n,nsys", [(5, 3), (65, 40), (702, 33), (4096, 9), (4096, 400), (2050, 333)])
+@pytest.mark.parametrize("n,nsys", [(5, 3), (65, 40), (702, 33), (4096, 9), (4096, 400), (2050, 333),
+                                    (300, 48), (700, 64), (1025, 36), (3000, 100), (4096, 512)])
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
 @pytest.mark.parametrize("solver", [F.SOLVER_EXACT, F.SOLVER_HYBRID])
 def test_tridiag_batch(layout, n, nsys, dtype, solver):
