@@ -305,6 +305,28 @@ int ixb_read_state_files(const char* ufile, const char* vfile, const char* pfile
                          double* yv, double* xp, double* yp, double* u, double* v, double* T, double* p, int* i0,
                          int* i1, int* iter, double* a);
 
+/* ---- immersed solid bodies (host only, no GPU needed) ---- */
+#define IXB_BODY_BOX 0    /* prm = {x0, x1, y0, y1}: x0 <= x <= x1, y0 <= y <= y1 */
+#define IXB_BODY_REGION 1 /* prm = {y0, y1, s0, c0, s1, c1}: y0 <= y <= y1, s0*y + c0 <= x <= s1*y + c1
+                             (en_region_tipo1, source/mod_front_inmersa.f90:188-207) */
+#define IXB_BODY_TRIAN 2  /* definir_cuerpo 'trian' (mod_front_inmersa.f90:73-99): u, v */
+#define IXB_BODY_CUADR 3  /* definir_cuerpo 'cuadr' (:101-133): u, v */
+#define IXB_BODY_CHIME 4  /* definir_cuerpo 'chime' (:135-177): u, v, and T held at 1 */
+#define IXB_BODY_VEL 1    /* flags: penalty sources on u and v (held at 1e40 / 1e51 = 1e-11 in the body) */
+#define IXB_BODY_TEMP 2   /* flags: T held at t_value in the body */
+/* Penalty sources of an immersed body (definir_cuerpo, mod_front_inmersa.f90:
+ * 54-179), for ixb_set_sources: every p node (xp(ii), yp(jj)) inside the body
+ * sets fuente_lin = -1e51 and fuente_con = 1e40 (u, v) or 1e51 * t_value (T)
+ * at (ii, jj) of the u (mi, nj+1), v (mi+1, nj) and T (mi+1, nj+1) arrays,
+ * column-major; other entries are left as they are, so bodies accumulate.
+ * The reference also writes u at ii = mi+1 and v at jj = nj+1, past the ends
+ * of those arrays; those writes are dropped.  For the three fixed shapes prm,
+ * flags and t_value are ignored.  Arrays of variables the body does not touch
+ * may be NULL. */
+int ixb_body_sources(int mi, int nj, const double* xp, const double* yp, int shape, const double* prm, int flags,
+                     double t_value, double* fcon_u, double* flin_u, double* fcon_v, double* flin_v, double* fcon_t,
+                     double* flin_t);
+
 /* ---- host-side inputs (no GPU needed) ---- */
 /* lectura_cond_frontera index rule (source/mod_cond_frontera.f90:114-238):
  * for side 0/2 ('a'/'c') the divisions are located on `yy` (nn entries), for

@@ -20,6 +20,8 @@ module ixb
   integer(c_int), parameter :: IXB_VAR_U = 0, IXB_VAR_V = 1, IXB_VAR_T = 2
   integer(c_int), parameter :: IXB_BC_OTHER = 0, IXB_BC_DIRI = 1, IXB_BC_NEUM = 2
   integer(c_int), parameter :: IXB_MESH_UNIF = 0, IXB_MESH_TUBO = 1, IXB_MESH_CENT = 2, IXB_MESH_TANH = 3
+  integer(c_int), parameter :: IXB_BODY_BOX = 0, IXB_BODY_REGION = 1, IXB_BODY_TRIAN = 2, IXB_BODY_CUADR = 3
+  integer(c_int), parameter :: IXB_BODY_CHIME = 4, IXB_BODY_VEL = 1, IXB_BODY_TEMP = 2
 
   type, bind(C) :: ixb_params
      real(c_double) :: gamma_momen, gamma_energ, Ri, Riy, dt
@@ -134,6 +136,15 @@ module ixb
        integer(c_int), value :: j0, j1
        real(c_double), intent(out) :: nu0, nu1
      end function ixb_nusselt_x
+
+     integer(c_int) function ixb_body_sources(mi, nj, xp, yp, shape, prm, flags, t_value, fcon_u, flin_u, &
+          fcon_v, flin_v, fcon_t, flin_t) bind(C, name="ixb_body_sources")
+       import :: c_int, c_double
+       integer(c_int), value :: mi, nj, shape, flags
+       real(c_double), intent(in) :: xp(*), yp(*), prm(*)
+       real(c_double), value :: t_value
+       real(c_double), intent(inout) :: fcon_u(*), flin_u(*), fcon_v(*), flin_v(*), fcon_t(*), flin_t(*)
+     end function ixb_body_sources
 
      integer(c_int) function ixb_staggered_mesh(mi, nj, xkind, xparam, ykind, yparam, ao, bo, xu, yv, xp, yp) &
           bind(C, name="ixb_staggered_mesh")

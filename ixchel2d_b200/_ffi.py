@@ -21,6 +21,8 @@ SOLVER_HYBRID, SOLVER_EXACT = 0, 1
 VAR_U, VAR_V, VAR_T = 0, 1, 2
 BC_OTHER, BC_DIRI, BC_NEUM = 0, 1, 2
 MESH_UNIF, MESH_TUBO, MESH_CENT, MESH_TANH = 0, 1, 2, 3
+BODY_BOX, BODY_REGION, BODY_TRIAN, BODY_CUADR, BODY_CHIME = 0, 1, 2, 3, 4
+BODY_VEL, BODY_TEMP = 1, 2
 
 
 class Params(C.Structure):
@@ -108,6 +110,7 @@ SIGNATURES = [
      [C.c_int, C.c_int, C.c_int, C.c_double]),
     ("ixb_read_state_files", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_int] + [_vp] * 8 +
      [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("ixb_body_sources", C.c_int, [C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double] + [_vp] * 6),
     ("ixb_bc_locate", C.c_int, [C.c_int, C.c_int, _dp, C.POINTER(C.c_int), _dp, _dp, C.c_int, _dp, C.c_int,
                                 C.POINTER(BCSide)]),
     ("ixb_read_bc_file", C.c_int, [C.c_char_p, _dp, C.c_int, _dp, C.c_int, C.POINTER(BCSide)]),

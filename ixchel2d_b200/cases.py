@@ -119,6 +119,32 @@ class Case:
         return (self.mi + 1) * (self.nj + 1)
 
 
+def add_body(case: Case, shape: int, prm=None, flags: int = 0, t_value: float = 0.0) -> Case:
+    """Adds an immersed body's penalty sources (ixb_body_sources, the masks of
+    definir_cuerpo, source/mod_front_inmersa.f90:54-179) to case.sources;
+    existing sources are kept, so bodies accumulate."""
+    mi, nj = case.mi, case.nj
+    sh = {0: (mi, nj + 1), 1: (mi + 1, nj), 2: (mi + 1, nj + 1)}
+    arrs = {}
+    for var in (0, 1, 2):
+        if var in case.sources:
+            f, l = case.sources[var]
+            arrs[var] = (np.array(f, dtype=np.float64, order="F"), np.array(l, dtype=np.float64, order="F"))
+        else:
+            arrs[var] = (np.zeros(sh[var], order="F"), np.zeros(sh[var], order="F"))
+    p = None if prm is None else np.ascontiguousarray(prm, dtype=np.float64)
+    xp = np.ascontiguousarray(case.xp, dtype=np.float64)
+    yp = np.ascontiguousarray(case.yp, dtype=np.float64)
+    check(lib.ixb_body_sources(mi, nj, dptr(xp), dptr(yp), shape, None if p is None else dptr(p), flags,
+                               float(t_value), dptr(arrs[0][0]), dptr(arrs[0][1]), dptr(arrs[1][0]),
+                               dptr(arrs[1][1]), dptr(arrs[2][0]), dptr(arrs[2][1])), "ixb_body_sources")
+    for var in (0, 1, 2):
+        f, l = arrs[var]
+        if var in case.sources or np.any(l != 0.0) or np.any(f != 0.0):
+            case.sources[var] = (f, l)
+    return case
+
+
 def shapes(mi: int, nj: int) -> dict:
     return {"u": (mi, nj + 1), "v": (mi + 1, nj), "p": (mi + 1, nj + 1), "T": (mi + 1, nj + 1),
             "u_ant": (mi, nj + 1), "v_ant": (mi + 1, nj), "T_ant": (mi + 1, nj + 1)}

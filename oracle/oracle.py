@@ -92,6 +92,61 @@ def tridiagonal(a, b, c, r):
     return r
 
 
+def definir_cuerpo(opcion: str, mi: int, nj: int, xp, yp) -> dict:
+    """Penalty sources of an immersed body, restating definir_cuerpo
+    (source/mod_front_inmersa.f90:54-179) loop by loop: for every p node
+    (xp(ii), yp(jj)) inside the body, fuente_lin = -10.0e50 and fuente_con =
+    10.0e50*10.0e-12 on u and v (T: 10e50*1.0 for 'chime') at (ii, jj).  The
+    reference's writes to u at ii = mi+1 and v at jj = nj+1 fall outside
+    those arrays and are dropped.  Returns var -> (fcon, flin), var 0/1/2 =
+    u/v/T, in the Fortran shapes."""
+    xp = [float(x) for x in xp]
+    yp = [float(y) for y in yp]
+    fu = np.zeros((mi, nj + 1), order="F"); lu = np.zeros_like(fu)
+    fv = np.zeros((mi + 1, nj), order="F"); lv = np.zeros_like(fv)
+    ft = np.zeros((mi + 1, nj + 1), order="F"); lt = np.zeros_like(ft)
+
+    def recta_mxb1(x):  # :210-215
+        mm = 1.0 / 2.0
+        bb = -(0.1 - mm * 6.0) / mm
+        return x / mm + bb
+
+    def recta_mxb2(x):  # :226-231
+        mm = -1.0 / 2.0
+        bb = -(0.1 - mm * 6.0) / mm
+        return x / mm + bb
+
+    def en_region_tipo1(xx, yy, aa, bb, f1, f2):  # :188-207
+        return aa <= xx <= bb and f1(xx) <= yy <= f2(xx)
+
+    def put(ii, jj, temp):  # 1-based (ii, jj)
+        if ii <= mi:
+            lu[ii - 1, jj - 1] = -10.0e50
+            fu[ii - 1, jj - 1] = 10.0e50 * 10.0e-12
+        if jj <= nj:
+            lv[ii - 1, jj - 1] = -10.0e50
+            fv[ii - 1, jj - 1] = 10.0e50 * 10.0e-12
+        if temp:
+            lt[ii - 1, jj - 1] = -10e50
+            ft[ii - 1, jj - 1] = 10e50 * 1.0
+
+    if opcion == "trian":
+        yv, hh = 0.1, 0.1
+        for jj in range(1, nj + 2):
+            if yv - hh <= yp[jj - 1] <= yv:
+                for ii in range(1, mi + 2):
+                    if en_region_tipo1(yp[jj - 1], xp[ii - 1], yv - hh, yv, recta_mxb1, recta_mxb2):
+                        put(ii, jj, False)
+    elif opcion in ("cuadr", "chime"):
+        yv, xv, hh = (0.05, 6.0, 0.1) if opcion == "cuadr" else (0.5, 8.5, 0.3)
+        for jj in range(1, nj + 2):
+            if yv - hh / 2.0 <= yp[jj - 1] <= yv + hh / 2.0:
+                for ii in range(1, mi + 2):
+                    if xv - hh / 2.0 <= xp[ii - 1] <= xv + hh / 2.0:
+                        put(ii, jj, opcion == "chime")
+    return {0: (fu, lu), 1: (fv, lv), 2: (ft, lt)}
+
+
 def tridiagonal_batch(a, b, c, d):
     """Independent contiguous systems (rows of 2-D arrays); returns x."""
     a, b, c, d = (np.array(x, dtype=np.float64, order="C") for x in (a, b, c, d))

@@ -214,6 +214,26 @@ def test_sources_immersed_block():
         assert np.array_equal(gs[k], os_[k]), k
 
 
+def test_sources_body_holding_temperature():
+    # a solid block from ixb_body_sources: u, v and T penalty sources, T held
+    # at 0.25 (definir_cuerpo's 'chime' form, mod_front_inmersa.f90:135-177)
+    case = cases.natural_cavity(24, 24, Ra=1e4)
+    cases.add_body(case, F.BODY_BOX, [0.4, 0.6, 0.3, 0.55], F.BODY_VEL | F.BODY_TEMP, 0.25)
+    assert set(case.sources) == {0, 1, 2}
+    g, o = _pair(case, solver=F.SOLVER_EXACT)
+    g.iterations(30)
+    o.iterations(30)
+    gs, os_ = g.download(), o.get_state()
+    for k in STATE:
+        assert np.array_equal(gs[k], os_[k]), k
+    body = case.sources[2][1] != 0
+    assert body.sum() > 4
+    assert np.allclose(gs["T"][body], 0.25, rtol=0, atol=1e-12)
+    # the reference's pair (1e40, -1e51) holds u and v at 1e-11
+    ub = gs["u"][case.sources[0][1] != 0]
+    assert np.allclose(ub, 1e-11, rtol=1e-9, atol=0)
+
+
 def test_nusselt_matches_oracle():
     case = cases.natural_cavity(32, 32, Ra=1e4)
     g, o = _pair(case)
