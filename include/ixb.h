@@ -203,6 +203,14 @@ int ixb_tridiag_f64(const double* a, const double* b, const double* c, const dou
                     int nsys, int layout, int solver, void* stream);
 int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float* d, float* x, int n,
                     int nsys, int layout, int solver, void* stream);
+/* The hybrid solves above run their copies through the tensor/bulk-copy
+ * engine and wait on them for a bounded time; a wait that expires leaves the
+ * affected systems unwritten and is recorded on the device.  This call waits
+ * for all work on the current device, then returns IXB_ETIMEOUT if such a
+ * wait expired since the previous call (and clears the record), IXB_ECUDA if
+ * the device reports an error, else IXB_OK.  No counterpart in the
+ * reference, whose solver has no waits. */
+int ixb_tridiag_status(void);
 
 /* Allocation-free form of ixb_tridiag_f64 (no counterpart in the reference),
  * for callers that cannot let a library allocate device memory during their
@@ -236,7 +244,8 @@ int ixb_tridiag_f64_noalloc(const double* a, const double* b, const double* c, c
  * grad[jj-1] = d nu0 / d value(jj), jj = 1..nj+1 (zero where the line is not
  * solved).  The map is affine in T with u, v fixed, so the gradient is exact
  * (transposed line solves, no stored forward states); the state is left
- * unchanged.  ixb_set_bc_values sets the per-line values of one side of a
+ * unchanged; IXB_ETIMEOUT if a transposed line solve's copies did not arrive
+ * within their bounded wait.  ixb_set_bc_values sets the per-line values of one side of a
  * boundary table (a per-node profile, beyond the reference's 15 segments),
  * keeping each line's type. */
 int ixb_energy_iterations(ixb_handle* h, int n);

@@ -219,6 +219,9 @@ extern "C" int ixb_adjoint_energy(ixb_handle* h, int K, int j0, int j1, double* 
   std::vector<double> g(nj + 2);
   ACK(cudaMemcpyAsync(g.data(), gd, (nj + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
   ACK(cudaStreamSynchronize(st));
+  int timed_out = 0;
+  ACK(tridiag_take_timeout(&timed_out));  // a line solve whose copies did not arrive in time
+  if (timed_out) return IXB_ETIMEOUT;
   for (int jj = 1; jj <= nj + 1; ++jj) grad[jj - 1] = g[jj];
   return IXB_OK;
 }

@@ -971,6 +971,13 @@ int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float*
   return e == cudaSuccess ? IXB_OK : IXB_ECUDA;
 }
 
+int ixb_tridiag_status(void) {
+  if (cudaDeviceSynchronize() != cudaSuccess) return IXB_ECUDA;
+  int flag = 0;
+  if (tridiag_take_timeout(&flag) != cudaSuccess) return IXB_ECUDA;
+  return flag ? IXB_ETIMEOUT : IXB_OK;
+}
+
 }  // extern "C"
 
 namespace ixb {

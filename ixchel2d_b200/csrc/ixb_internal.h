@@ -217,5 +217,8 @@ cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const
                         int nsys, int layout, int solver, cudaStream_t st);
 cudaError_t tridiag_f32(const float* a, const float* b, const float* c, const float* d, float* x, int n,
                         int nsys, int layout, int solver, cudaStream_t st);
+// reads and clears the flag set when a line-solve kernel's bounded wait on
+// its copies expired (synchronous)
+cudaError_t tridiag_take_timeout(int* flag);
 
 }  // namespace ixb

@@ -822,6 +822,20 @@ static cudaError_t tridiag_impl(const R* a, const R* b, const R* c, const R* d, 
   return e != cudaSuccess ? e : e2;
 }
 
+// Reads and clears the timeout flag the streamed and interleaved kernels set
+// when a bounded wait on their copies expires (synchronous).
+cudaError_t tridiag_take_timeout(int* flag) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_tri_timeout, sizeof(int));
+  if (e != cudaSuccess) return e;
+  if (v) {
+    const int zero = 0;
+    if ((e = cudaMemcpyToSymbol(g_tri_timeout, &zero, sizeof(int))) != cudaSuccess) return e;
+  }
+  *flag = v;
+  return cudaSuccess;
+}
+
 cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,
                         int nsys, int layout, int solver, cudaStream_t st) {
   if (solver == IXB_SOLVER_EXACT) return tridiag_impl<double, IXB_SOLVER_EXACT>(a, b, c, d, x, n, nsys, layout, st);

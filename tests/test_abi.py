@@ -51,6 +51,12 @@ def test_create_without_gpu_fails_cleanly():
     assert not h.value
 
 
+def test_tridiag_status_without_gpu():
+    if F.lib.ixb_device_count() > 0:
+        pytest.skip("a GPU is present")
+    assert F.lib.ixb_tridiag_status() == F.ECUDA
+
+
 def _locate_ref(coord, x1s, size):
     """lectura_cond_frontera, source/mod_cond_frontera.f90:125-149."""
     idx = [2]

@@ -305,3 +305,4 @@ def test_tridiag_batch(layout, n, nsys, dtype, solver):
     else:
         tol = 1e-12 if dtype == "f64" else 2e-5
         assert relerr(x, ref) < tol, relerr(x, ref)
+    assert F.lib.ixb_tridiag_status() == F.OK  # no bounded copy wait expired
