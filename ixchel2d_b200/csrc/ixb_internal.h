@@ -19,6 +19,8 @@ namespace ixb {
 // unchanged.  Off by default: at 701x301 it measured 193 us per outer
 // iteration against 162 us without it.
 bool pdl_enabled();
+// fused x-sweeps (one kernel per x-sweep) unless IXB_SPLIT_X=1
+bool fused_x_enabled();
 template <class... KArgs, class... Args>
 inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
                             Args&&... args) {
@@ -159,6 +161,12 @@ struct SolveIO {
   int LD;
   int m, mp;            // chunk rows per thread, padded pitch
 };
+// fused x-sweep (assembly into the solve's shared memory, one launch;
+// ixb_sweep.cuh), x-sweeps only; cudaErrorNotSupported for shapes other
+// than one line per CTA with 128 or 256 threads
+template <int EQ, int SOLVER>
+cudaError_t fused_x_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
+                           cudaStream_t st);
 // one instance of a batched line solve
 struct SolveInst {
   SolveIO io;

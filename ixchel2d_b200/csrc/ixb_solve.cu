@@ -17,13 +17,14 @@
 #include "ixb_ctl.cuh"
 #include "ixb_internal.h"
 #include "ixb_reduce.cuh"
+#include "ixb_solve.cuh"
 
 namespace ixb {
 namespace {
 
-// Lines L0 .. L0+TL-1 of one sweep: staged rows -> shared memory -> solve ->
-// field.  Returns this thread's share of ||new - prev||^2.  Called by all
-// threads of the CTA (it holds barriers).
+// Lines L0 .. L0+TL-1 of one sweep: staged rows -> shared memory, then
+// solve_lines (solve -> field).  Returns this thread's share of
+// ||new - prev||^2.  Called by all threads of the CTA (it holds barriers).
 template <class S, bool X, bool DC, bool EXACT, int TL, int G, int M>
 __device__ __forceinline__ double solve_group(S* sm, const SolveIO& io, const int n, const int line_lo,
                                               const int line_hi, const int nfull, const int L0) {
@@ -59,48 +60,7 @@ __device__ __forceinline__ double solve_group(S* sm, const SolveIO& io, const in
     sm[off + 3 * arr] = d;
   }
   __syncthreads();
-
-  // phase 2: line solves
-  {
-    const int l = threadIdx.x / G;
-    const int L = L0 + l;
-    const bool active = (L >= line_lo && L <= line_hi);
-    S* line = sm + l * LS;
-    if constexpr (EXACT) {
-      if (active && threadIdx.x % G == 0) thomas_exact(line, line + arr, line + 2 * arr, line + 3 * arr, n, m, mp);
-    } else {
-      chunk_solve<S, G>(line, m, mp, active, RS_PCR);
-    }
-  }
-  __syncthreads();
-
-  // phase 3: write the new field (unsolved lines keep their values) and
-  // accumulate ||new - prev|| over the interior rows of the solved lines;
-  // y-lines are written TL adjacent ii at a time
-  double acc = 0.0;
-  for (int idx = threadIdx.x; idx < TL * n; idx += NT) {
-    int l, r;
-    if (X) { l = TL == 1 ? 0 : idx / n; r = idx - l * n; }
-    else { l = idx % TL; r = idx / TL; }
-    const int L = L0 + l;
-    if (L > nfull) continue;
-    const int g = X ? (L - 1) * io.LD + r : r * io.LD + (L - 1);
-    double x;
-    if (L >= line_lo && L <= line_hi) {
-      const int ch = r / m;
-      const S xs = sm[l * LS + 3 * arr + ch * mp + (r - ch * m)];
-      if constexpr (DC) x = io.in[g] + double(xs);
-      else x = double(xs);
-      if (r >= 1 && r <= n - 2) {
-        const double dv = x - (io.prev ? io.prev[g] : 0.0);
-        acc += dv * dv;
-      }
-    } else {
-      x = io.in[g];
-    }
-    io.out[g] = x;
-  }
-  return acc;
+  return solve_lines<S, X, DC, EXACT, TL, G, M>(sm, io, n, line_lo, line_hi, nfull, L0);
 }
 
 template <class S, bool X, bool DC, bool EXACT, int TL, int G, int M>

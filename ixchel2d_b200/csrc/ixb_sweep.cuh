@@ -18,8 +18,10 @@
 #include <algorithm>
 #include <type_traits>
 
+#include "ixb_ctl.cuh"
 #include "ixb_internal.h"
 #include "ixb_reduce.cuh"
+#include "ixb_solve.cuh"
 
 namespace ixb {
 
@@ -247,6 +249,88 @@ cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& G, const Swe
   const int tiles = asm_tiles(EqIsX<EQ>::value, s.n, s.line_hi - s.line_lo + 1);
   const int grid = std::max(1, std::min(tiles, kAsmGridCap));
   return launch_k(assemble_kernel<EQ, SOLVER>, grid, kAsmThreads, 0, st, G, io, co, s.n, s.line_lo, s.line_hi);
+}
+
+// ---------------------------------------------------------------------------
+// Fused x-sweep: one CTA per x-line (TL = 1) assembles the line's rows
+// straight into the chunk layout of the line solve in shared memory (a warp
+// takes 32 consecutive cells of the line: coalesced field reads), solves
+// and writes the line, then finishes the b_o norm (p'-x) and the pass norm
+// with its loop test.  One launch per sweep instead of two, and no staging
+// of the rows through global memory.
+// ---------------------------------------------------------------------------
+template <int EQ, int SOLVER, int TL, int G, int M>
+__global__ void __launch_bounds__(TL * G)
+    fused_x_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n, const int line_lo,
+                   const int line_hi, const int nfull) {
+  IXB_PDL_ENTRY();
+  using ST = SweepTypes<SOLVER, EQ>;
+  using S = typename ST::S;
+  constexpr int NT = TL * G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);
+  const int m = M > 0 ? M : so.m;
+  const int mp = M > 0 ? (M | 1) : so.mp;
+  const int npad = G * m;
+  const int LS = (int)line_smem_elems(G, mp);
+  const int arr = G * mp;
+  const int L0 = 1 + blockIdx.x * TL;
+  double acc_bo = 0.0;
+#pragma unroll
+  for (int it = 0; it < (M > 0 ? M : m); ++it) {  // with M > 0 a thread's M cells are assembled together
+    const int idx = threadIdx.x + it * NT;
+    const int l = TL == 1 ? 0 : idx / npad;
+    const int r = idx - l * npad;
+    const int L = L0 + l;
+    const bool valid = L >= line_lo && L <= line_hi && r < n;
+    Row<double> row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
+    if (!valid) row = Row<double>{0.0, 1.0, 0.0, 0.0};  // identity rows pad the line to G*m rows
+    const int ch = r / m;
+    const int off = l * LS + ch * mp + (r - ch * m);
+    sm[off] = S(row.a);
+    sm[off + arr] = S(row.b);
+    sm[off + 2 * arr] = S(row.c);
+    sm[off + 3 * arr] = S(row.d);
+  }
+  __syncthreads();
+  const double acc =
+      solve_lines<S, true, ST::DC, SOLVER == IXB_SOLVER_EXACT, TL, G, M>(sm, so, n, line_lo, line_hi, nfull, L0);
+  if (io.nrm1.partials) finish_norm(io.nrm1, block_sum(acc_bo));
+  if (so.nrm0.partials) {
+    const bool last = finish_norm(so.nrm0, block_sum(acc));
+    if (last && so.ctl.ctl && threadIdx.x == 0) ctl_inner_step(so.ctl.ctl, so.ctl.norms, so.ctl.which, so.ctl.cond);
+  }
+}
+
+// Launch of one fused kernel; its dynamic shared-memory limit is raised the
+// first time it is asked for more than before.
+template <auto K>
+cudaError_t fused_go(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
+                     cudaStream_t st) {
+  static size_t limit = 48 * 1024 - 1024;  // default limit, less the kernel's static shared memory
+  if (s.smem > limit) {
+    const cudaError_t e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    if (e != cudaSuccess) return e;
+    limit = s.smem;
+  }
+  return launch_k(K, s.grid, s.tl * s.g, s.smem, st, G, io, so, s.n, s.line_lo, s.line_hi, s.nfull);
+}
+
+// Launches the fused form of x-sweep EQ for one-line shapes (TL = 1, 128 or
+// 256 threads); cudaErrorNotSupported for any other shape (the caller then
+// runs the two-kernel sweep).
+template <int EQ, int SOLVER>
+cudaError_t fused_x_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
+                           cudaStream_t st) {
+  static_assert(EqIsX<EQ>::value, "x-sweeps only");
+  if (s.tl != 1 || (s.g != 128 && s.g != 256)) return cudaErrorNotSupported;
+  constexpr bool EXACT = SOLVER == IXB_SOLVER_EXACT;
+  if (s.g == 128) {
+    if (!EXACT && s.m == 3) return fused_go<fused_x_kernel<EQ, SOLVER, 1, 128, 3>>(s, G, io, so, st);
+    return fused_go<fused_x_kernel<EQ, SOLVER, 1, 128, 0>>(s, G, io, so, st);
+  }
+  if (!EXACT && s.m == 3) return fused_go<fused_x_kernel<EQ, SOLVER, 1, 256, 3>>(s, G, io, so, st);
+  return fused_go<fused_x_kernel<EQ, SOLVER, 1, 256, 0>>(s, G, io, so, st);
 }
 
 }  // namespace ixb
