@@ -51,7 +51,6 @@ MEMSET_BYTES_PER_CELL = 8
 SWEEPS = ["u-y", "u-x", "v-y", "v-x", "p'-y", "p'-x", "T-y", "T-x"]
 # per outer iteration: 8 sweeps x (assembly + line solve), correction, residual,
 # and the p' reset (loop tests ride on the kernels that finish their norms)
-KERNELS_PER_ITER = 19
 METRIC = "Mcell-iter/s (SIMPLE outer iteration, p-cells): FP32+FP64-refined vs FP64"
 
 
@@ -432,6 +431,8 @@ def run_ours(args):
     sims, shapes = {}, {}
     for name, prec in modes.items():
         sims[name], shapes[name] = make_sim(case, prec, stream, loaded.get(name))
+    # kernels per outer iteration with the chosen shapes (fused sweeps launch one kernel, others two)
+    per_iter = {name: sims[name].iteration_launches() for name in modes}
     if args.save_shapes and rank == 0:
         Path(args.save_shapes).write_text(json.dumps({n: {str(k): list(v) for k, v in sh.items()}
                                                       for n, sh in shapes.items()}))
@@ -558,7 +559,8 @@ def run_ours(args):
             "cpu_baseline": None if cpu_val is None else {
                 "value": cpu_val, "unit": "Mcell-iter/s", "cores": cpu_cores, "kind": "port",
                 "sample": f"{cpu_iters} outer iterations of the same 701x301 case ({cpu_s:.1f} s)"},
-            "gpu_launches": 2 * (KERNELS_PER_ITER * ITERS + 1) * args.steps,
+            "gpu_launches": sum((per_iter[n] * ITERS + 1) * args.steps for n in modes),
+            "kernels_per_outer_iteration": per_iter,
             "clocks": clocks,
             "last_report": {k: reports["refined"][k] for k in ("maxbo", "residuo", "n_simple", "n_momen")},
             "wall_s_timed_region": wall,
@@ -571,12 +573,17 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
-def run_profile_phases(prec):
+def run_profile_phases(prec, shapes_file=None):
     """Profiling driver (no timing, no JSON): the benchmark case, three outer
     iterations, then one launch of each of the ten phases in order
-    (u-y, u-x, v-y, v-x, p'-y, p'-x, correction, T-y, T-x, residual)."""
+    (u-y, u-x, v-y, v-x, p'-y, p'-x, correction, T-y, T-x, residual), in the
+    launch shapes of `shapes_file` (from --save-shapes) when given."""
     from ixchel2d_b200 import Simple2D
     sim = Simple2D.from_case(make_case(), prec=prec)
+    if shapes_file:
+        name = "refined" if prec == 1 else "fp64"
+        for k, (tl, g, *_) in json.loads(Path(shapes_file).read_text())[name].items():
+            sim.set_sweep_shape(int(k), tl, g)
     sim.iterations(3)
     for k in range(10):
         sim.phase(k)
@@ -633,7 +640,7 @@ def main():
     ap.add_argument("--profile-batch", action="store_true", help="run the batched-cavities profiling driver")
     args = ap.parse_args()
     if args.profile_phases:
-        run_profile_phases(args.prec)
+        run_profile_phases(args.prec, args.shapes)
         return
     if args.profile_adi:
         run_profile_adi()

@@ -829,6 +829,17 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms) {
   return st;
 }
 
+int ixb_iteration_launches(ixb_handle* h, int* launches) {
+  if (!h || !launches) return IXB_EINVAL;
+  int k = 3;  // p' preset, p/u/v correction, u residual
+  for (int eq = 0; eq < EQ_COUNT; ++eq) {
+    if (h->shape_tl[eq] == 0) pick_shape(h, eq);
+    k += (fused_enabled() && fused_shape(eq, h->shape_tl[eq], h->shape_g[eq])) ? 1 : 2;
+  }
+  *launches = k;
+  return IXB_OK;
+}
+
 int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads_per_line) {
   if (!h || sweep < 0 || sweep >= EQ_COUNT) return IXB_EINVAL;
   if (lines_per_cta == 0) {  // back to the default choice

@@ -19,8 +19,8 @@ namespace ixb {
 // unchanged.  Off by default: at 701x301 it measured 193 us per outer
 // iteration against 162 us without it.
 bool pdl_enabled();
-// fused x-sweeps (one kernel per x-sweep) unless IXB_SPLIT_X=1
-bool fused_x_enabled();
+// fused sweeps (one kernel per sweep) unless IXB_SPLIT=1
+bool fused_enabled();
 template <class... KArgs, class... Args>
 inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
                             Args&&... args) {
@@ -161,11 +161,23 @@ struct SolveIO {
   int LD;
   int m, mp;            // chunk rows per thread, padded pitch
 };
-// fused x-sweep (assembly into the solve's shared memory, one launch;
-// ixb_sweep.cuh), x-sweeps only; cudaErrorNotSupported for shapes other
-// than one line per CTA with 128 or 256 threads
+// Launch shapes (lines per CTA, threads per line) of the fused sweeps:
+// x-sweeps one line per CTA; y-sweeps several adjacent lines per CTA, so
+// that a warp's field reads span adjacent lines.
+#define IXB_FUSED_X_SHAPES(X_) X_(1, 128) X_(1, 256)
+#define IXB_FUSED_Y_SHAPES(X_) X_(2, 64) X_(2, 128) X_(4, 32) X_(4, 64) X_(8, 32)
+inline bool fused_shape(int eq, int tl, int g) {
+  bool hit = false;
+#define IXB_HIT_(TL_, G_) hit = hit || (tl == TL_ && g == G_);
+  if (eq & 1) { IXB_FUSED_X_SHAPES(IXB_HIT_) }  // x-sweeps are the odd ones (EqIsX)
+  else { IXB_FUSED_Y_SHAPES(IXB_HIT_) }
+#undef IXB_HIT_
+  return hit;
+}
+// fused sweep (assembly into the solve's shared memory, one launch;
+// ixb_sweep.cuh); cudaErrorNotSupported for shapes it does not cover
 template <int EQ, int SOLVER>
-cudaError_t fused_x_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
+cudaError_t fused_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
                            cudaStream_t st);
 // one instance of a batched line solve
 struct SolveInst {

@@ -264,11 +264,11 @@ int sweep_occupancy(int eq, int solver, const SweepShape& s) {
   return solve_blocks_per_sm(solver, eq_is_x(eq), eq_dc(eq, solver), s);
 }
 
-// Fused x-sweeps are on unless IXB_SPLIT_X=1 (the two-kernel form, for
+// Fused sweeps are on unless IXB_SPLIT=1 (the two-kernel form, for
 // comparison).
-bool fused_x_enabled() {
+bool fused_enabled() {
   static const bool on = [] {
-    const char* e = getenv("IXB_SPLIT_X");
+    const char* e = getenv("IXB_SPLIT");
     return !(e && e[0] == '1');
   }();
   return on;
@@ -301,19 +301,14 @@ cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<
                              const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st,
                              const CtlRef& ctl) {
   cudaError_t e;
-  if (eq_is_x(eq) && fused_x_enabled()) {
-    // x-sweeps with one line per CTA: assembly and solve in one kernel
+  if (fused_enabled() && fused_shape(eq, s.tl, s.g)) {
+    // assembly and solve in one kernel where the launch shape allows it
     SolveIO so{};
     so.in = io.in; so.out = io.out; so.prev = io.prev; so.nrm0 = io.nrm0; so.ctl = ctl;
     so.LD = G.LD; so.m = s.m; so.mp = s.mp;
     auto fx = [&](auto solver_c) -> cudaError_t {
       constexpr int SV = decltype(solver_c)::value;
-      switch (eq) {
-        case EQ_UX: return fused_x_launch<EQ_UX, SV>(s, G, io, so, st);
-        case EQ_VX: return fused_x_launch<EQ_VX, SV>(s, G, io, so, st);
-        case EQ_PX: return fused_x_launch<EQ_PX, SV>(s, G, io, so, st);
-        default: return fused_x_launch<EQ_TX, SV>(s, G, io, so, st);
-      }
+      IXB_EQ_SWITCH(return fused_launch<E_, SV>(s, G, io, so, st))
     };
     if (solver == IXB_SOLVER_EXACT) e = fx(std::integral_constant<int, IXB_SOLVER_EXACT>{});
     else if (solver == SOLVER_MIXED) e = fx(std::integral_constant<int, SOLVER_MIXED>{});

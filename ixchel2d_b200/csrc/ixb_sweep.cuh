@@ -252,20 +252,22 @@ cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& G, const Swe
 }
 
 // ---------------------------------------------------------------------------
-// Fused x-sweep: one CTA per x-line (TL = 1) assembles the line's rows
-// straight into the chunk layout of the line solve in shared memory (a warp
-// takes 32 consecutive cells of the line: coalesced field reads), solves
-// and writes the line, then finishes the b_o norm (p'-x) and the pass norm
-// with its loop test.  One launch per sweep instead of two, and no staging
-// of the rows through global memory.
+// Fused sweep: a CTA assembles the rows of its TL lines straight into the
+// chunk layout of the line solve in shared memory, solves and writes the
+// lines, then finishes the b_o norm (p'-x) and the pass norm with its loop
+// test.  One launch per sweep instead of two, and no staging of the rows
+// through global memory.  x-lines: consecutive threads take consecutive
+// cells of a line; y-lines: consecutive threads take the TL adjacent lines
+// of a row, so the field reads stay coalesced.
 // ---------------------------------------------------------------------------
 template <int EQ, int SOLVER, int TL, int G, int M>
 __global__ void __launch_bounds__(TL * G)
-    fused_x_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n, const int line_lo,
-                   const int line_hi, const int nfull) {
+    fused_sweep_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n,
+                       const int line_lo, const int line_hi, const int nfull) {
   IXB_PDL_ENTRY();
   using ST = SweepTypes<SOLVER, EQ>;
   using S = typename ST::S;
+  constexpr bool X = EqIsX<EQ>::value;
   constexpr int NT = TL * G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S* sm = reinterpret_cast<S*>(smem_raw);
@@ -279,8 +281,9 @@ __global__ void __launch_bounds__(TL * G)
 #pragma unroll
   for (int it = 0; it < (M > 0 ? M : m); ++it) {  // with M > 0 a thread's M cells are assembled together
     const int idx = threadIdx.x + it * NT;
-    const int l = TL == 1 ? 0 : idx / npad;
-    const int r = idx - l * npad;
+    int l, r;
+    if (X) { l = TL == 1 ? 0 : idx / npad; r = idx - l * npad; }
+    else { l = idx % TL; r = idx / TL; }
     const int L = L0 + l;
     const bool valid = L >= line_lo && L <= line_hi && r < n;
     Row<double> row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
@@ -294,7 +297,7 @@ __global__ void __launch_bounds__(TL * G)
   }
   __syncthreads();
   const double acc =
-      solve_lines<S, true, ST::DC, SOLVER == IXB_SOLVER_EXACT, TL, G, M>(sm, so, n, line_lo, line_hi, nfull, L0);
+      solve_lines<S, X, ST::DC, SOLVER == IXB_SOLVER_EXACT, TL, G, M>(sm, so, n, line_lo, line_hi, nfull, L0);
   if (io.nrm1.partials) finish_norm(io.nrm1, block_sum(acc_bo));
   if (so.nrm0.partials) {
     const bool last = finish_norm(so.nrm0, block_sum(acc));
@@ -316,21 +319,25 @@ cudaError_t fused_go(const SweepShape& s, const Geo<double>& G, const SweepIO<do
   return launch_k(K, s.grid, s.tl * s.g, s.smem, st, G, io, so, s.n, s.line_lo, s.line_hi, s.nfull);
 }
 
-// Launches the fused form of x-sweep EQ for one-line shapes (TL = 1, 128 or
-// 256 threads); cudaErrorNotSupported for any other shape (the caller then
+// Launches the fused form of sweep EQ for the shapes of IXB_FUSED_X_SHAPES /
+// IXB_FUSED_Y_SHAPES; any other shape: cudaErrorNotSupported (the caller
 // runs the two-kernel sweep).
 template <int EQ, int SOLVER>
-cudaError_t fused_x_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
-                           cudaStream_t st) {
-  static_assert(EqIsX<EQ>::value, "x-sweeps only");
-  if (s.tl != 1 || (s.g != 128 && s.g != 256)) return cudaErrorNotSupported;
+cudaError_t fused_launch(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
+                         cudaStream_t st) {
   constexpr bool EXACT = SOLVER == IXB_SOLVER_EXACT;
-  if (s.g == 128) {
-    if (!EXACT && s.m == 3) return fused_go<fused_x_kernel<EQ, SOLVER, 1, 128, 3>>(s, G, io, so, st);
-    return fused_go<fused_x_kernel<EQ, SOLVER, 1, 128, 0>>(s, G, io, so, st);
+#define IXB_FUSED_(TL_, G_)                                                                     \
+  if (s.tl == TL_ && s.g == G_) {                                                               \
+    if (!EXACT && s.m == 3) return fused_go<fused_sweep_kernel<EQ, SOLVER, TL_, G_, 3>>(s, G, io, so, st); \
+    return fused_go<fused_sweep_kernel<EQ, SOLVER, TL_, G_, 0>>(s, G, io, so, st);                \
   }
-  if (!EXACT && s.m == 3) return fused_go<fused_x_kernel<EQ, SOLVER, 1, 256, 3>>(s, G, io, so, st);
-  return fused_go<fused_x_kernel<EQ, SOLVER, 1, 256, 0>>(s, G, io, so, st);
+  if constexpr (EqIsX<EQ>::value) {
+    IXB_FUSED_X_SHAPES(IXB_FUSED_)
+  } else {
+    IXB_FUSED_Y_SHAPES(IXB_FUSED_)
+  }
+#undef IXB_FUSED_
+  return cudaErrorNotSupported;
 }
 
 }  // namespace ixb

@@ -4,6 +4,6 @@
 namespace ixb {
 template cudaError_t assemble_launch<EQ_TX, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&,
                                                               const SweepIO<double>&, const StageBuf&, cudaStream_t);
-template cudaError_t fused_x_launch<EQ_TX, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
-                                                     const SolveIO&, cudaStream_t);
+template cudaError_t fused_launch<EQ_TX, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
+                                                   const SolveIO&, cudaStream_t);
 }  // namespace ixb

@@ -4,4 +4,6 @@
 namespace ixb {
 template cudaError_t assemble_launch<EQ_TY, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&,
                                                               const SweepIO<double>&, const StageBuf&, cudaStream_t);
+template cudaError_t fused_launch<EQ_TY, IXB_SOLVER_EXACT>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
+                                                   const SolveIO&, cudaStream_t);
 }  // namespace ixb

@@ -6,6 +6,6 @@ template cudaError_t assemble_launch<EQ_UX, IXB_SOLVER_HYBRID>(const SweepShape&
                                                                const SweepIO<double>&, const StageBuf&, cudaStream_t);
 template cudaError_t assemble_batch_launch<EQ_UX, IXB_SOLVER_HYBRID>(const void*, const int2*, int, const int*, const BatchNorm&,
                                                            cudaStream_t);
-template cudaError_t fused_x_launch<EQ_UX, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
-                                                     const SolveIO&, cudaStream_t);
+template cudaError_t fused_launch<EQ_UX, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
+                                                   const SolveIO&, cudaStream_t);
 }  // namespace ixb

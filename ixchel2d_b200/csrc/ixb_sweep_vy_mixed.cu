@@ -6,4 +6,6 @@ template cudaError_t assemble_launch<EQ_VY, SOLVER_MIXED>(const SweepShape&, con
                                                           const SweepIO<double>&, const StageBuf&, cudaStream_t);
 template cudaError_t assemble_batch_launch<EQ_VY, SOLVER_MIXED>(const void*, const int2*, int, const int*, const BatchNorm&,
                                                            cudaStream_t);
+template cudaError_t fused_launch<EQ_VY, SOLVER_MIXED>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
+                                                   const SolveIO&, cudaStream_t);
 }  // namespace ixb

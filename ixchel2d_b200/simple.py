@@ -137,6 +137,12 @@ class Simple2D:
     def set_sweep_shape(self, sweep: int, lines_per_cta: int = 0, threads_per_line: int = 0):
         F.check(F.lib.ixb_set_sweep_shape(self.h, sweep, lines_per_cta, threads_per_line), "ixb_set_sweep_shape")
 
+    def iteration_launches(self) -> int:
+        """Kernels one outer iteration launches with the current shapes (one inner pass per loop)."""
+        k = C.c_int()
+        F.check(F.lib.ixb_iteration_launches(self.h, C.byref(k)), "ixb_iteration_launches")
+        return k.value
+
     def autotune(self, reps: int = 5, flush_bytes: int = 0) -> dict:
         """Pick the fastest launch shape of every sweep; returns {sweep: (lines_per_cta, threads_per_line, ms)}."""
         chosen = (C.c_int * 16)()

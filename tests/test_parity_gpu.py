@@ -128,6 +128,20 @@ def test_every_launch_shape_keeps_parity(shape):
         assert relerr(gs[k], os_[k]) < HYBRID_TOL, (k, relerr(gs[k], os_[k]))
 
 
+def test_iteration_launch_count():
+    if os.environ.get("IXB_SPLIT") == "1":
+        pytest.skip("fused sweeps switched off")
+    g = Simple2D.from_case(cases.lid_driven_mixed(45, 29))
+    for k in range(8):
+        g.set_sweep_shape(k, 1, 128)  # x-sweeps fused, y-sweeps two kernels
+    assert g.iteration_launches() == 4 * 1 + 4 * 2 + 3
+    for k in range(8):
+        g.set_sweep_shape(k, 4, 64)  # y-sweeps fused, x-sweeps two kernels
+    assert g.iteration_launches() == 4 * 2 + 4 * 1 + 3
+    g.set_sweep_shape(1, 1, 256)
+    assert g.iteration_launches() == 3 * 2 + 5 * 1 + 3
+
+
 def test_autotune_then_parity():
     case = cases.natural_cavity(40, 36, Ra=1e5)
     g, o = _pair(case)
