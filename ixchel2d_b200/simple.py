@@ -70,9 +70,18 @@ class Simple2D:
                 raise ValueError(f"{k}: shape {a.shape} != {self._shapes[k]}")
         F.check(F.lib.ixb_upload_state(self.h, *map(F.dptr, arrs)), "ixb_upload_state")
 
-    def download(self) -> dict:
-        out = {k: np.zeros(s, order="F") for k, s in self._shapes.items()}
+    def download(self, out: dict | None = None) -> dict:
+        """The seven state arrays; with `out`, written into its arrays (float64,
+        Fortran-ordered, the reference's shapes; e.g. views of pinned memory,
+        which the copies then reach directly) instead of new ones."""
         keys = ("u", "v", "p", "T", "u_ant", "v_ant", "T_ant")
+        if out is None:
+            out = {k: np.empty(s, order="F") for k, s in self._shapes.items()}
+        else:
+            for k in keys:
+                a = out[k]
+                if a.dtype != np.float64 or not a.flags.f_contiguous or a.shape != self._shapes[k]:
+                    raise ValueError(f"{k}: needs a float64 Fortran-ordered array of shape {self._shapes[k]}")
         F.check(F.lib.ixb_download_state(self.h, *[F.dptr(out[k]) for k in keys]), "ixb_download_state")
         return out
 
