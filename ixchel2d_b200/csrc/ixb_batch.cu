@@ -61,6 +61,7 @@ struct ixb_batch {
   int2* asm_items[EQ_COUNT] = {};
   int asm_n[EQ_COUNT] = {};
   SolveInst* sol_inst[EQ_COUNT] = {};
+  FusedInst* fus_inst[EQ_COUNT] = {};  // the same instances for the fused form (same work items)
   int2* sol_items[EQ_COUNT] = {};
   int sol_n[EQ_COUNT] = {};
   size_t sol_smem[EQ_COUNT] = {};
@@ -110,6 +111,7 @@ void dfree(T*& p) {
 void free_tables(ixb_batch* b) {
   for (int e = 0; e < EQ_COUNT; ++e) {
     dfree(b->asm_inst[e]); dfree(b->asm_items[e]); dfree(b->sol_inst[e]); dfree(b->sol_items[e]);
+    dfree(b->fus_inst[e]);
   }
   dfree(b->cell_inst); dfree(b->corr_items); dfree(b->res_items);
   for (auto& p : b->partials) dfree(p);
@@ -185,6 +187,42 @@ cudaError_t launch_asm_eq(ixb_batch* b, int eq, const BatchNorm& bn) {
   }
 }
 
+template <int SOLVER>
+cudaError_t launch_fused_eq(ixb_batch* b, int eq, const BatchNorm& an, const BatchNorm& sn) {
+  const int tl = b->tl[eq], g = b->g[eq];
+  const size_t sm = b->sol_smem[eq];
+  const FusedInst* in = b->fus_inst[eq];
+  const int2* it = b->sol_items[eq];
+  const int n = b->sol_n[eq];
+  switch (eq) {
+    case EQ_UY: return fused_batch_launch<EQ_UY, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+    case EQ_UX: return fused_batch_launch<EQ_UX, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+    case EQ_VY: return fused_batch_launch<EQ_VY, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+    case EQ_VX: return fused_batch_launch<EQ_VX, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+    case EQ_PY: return fused_batch_launch<EQ_PY, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+    case EQ_PX: return fused_batch_launch<EQ_PX, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+    case EQ_TY: return fused_batch_launch<EQ_TY, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+    default: return fused_batch_launch<EQ_TX, SOLVER>(tl, g, sm, in, it, n, b->active, an, sn, b->stream);
+  }
+}
+
+// One sweep of every active instance: one fused launch where the shape has
+// a fused form, else the assembly launch and the line-solve launch.  an:
+// the b_o norm (p'-x), sn: the pass norm.
+cudaError_t sweep_batch(ixb_batch* b, int eq, const BatchNorm& an, const BatchNorm& sn) {
+  const int form = form_of(b);
+  if (fused_enabled() && fused_shape(eq, b->tl[eq], b->g[eq])) {
+    const cudaError_t e = form == SOLVER_MIXED ? launch_fused_eq<SOLVER_MIXED>(b, eq, an, sn)
+                                               : launch_fused_eq<IXB_SOLVER_HYBRID>(b, eq, an, sn);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  cudaError_t e = form == SOLVER_MIXED ? launch_asm_eq<SOLVER_MIXED>(b, eq, an) : launch_asm_eq<IXB_SOLVER_HYBRID>(b, eq, an);
+  if (e != cudaSuccess) return e;
+  const bool dc = form == SOLVER_MIXED && eq != EQ_PY && eq != EQ_PX;
+  return solve_batch_launch(form, (eq & 1) != 0, dc, b->tl[eq], b->g[eq], b->sol_smem[eq], b->sol_inst[eq],
+                            b->sol_items[eq], b->sol_n[eq], b->active, sn, b->stream);
+}
+
 BatchNorm norm_of(ixb_batch* b, int k) {
   return BatchNorm{b->partials[k], b->counters + (size_t)k * b->count, b->results + (size_t)k * b->count};
 }
@@ -250,6 +288,9 @@ int build_tables(ixb_batch* b) {
       smem = std::max(smem, s.smem);
     }
     BCK(upload(&b->sol_inst[eq], sv));
+    std::vector<FusedInst> fv(b->count);
+    for (int i = 0; i < b->count; ++i) fv[i] = FusedInst{handle_geo(b->h[i]), io[eq][i], sv[i]};
+    BCK(upload(&b->fus_inst[eq], fv));
     BCK(upload(&b->sol_items[eq], sitems));
     b->sol_n[eq] = (int)sitems.size();
     b->sol_smem[eq] = smem;
@@ -289,11 +330,8 @@ int body(ixb_batch* b) {
   const BatchNorm none{nullptr, nullptr, nullptr};
   for (int eq = 0; eq < EQ_COUNT; ++eq) {
     const BatchNorm an = eq == EQ_PX ? norm_of(b, 2) : none;
-    BCK(form == SOLVER_MIXED ? launch_asm_eq<SOLVER_MIXED>(b, eq, an) : launch_asm_eq<IXB_SOLVER_HYBRID>(b, eq, an));
     const BatchNorm sn = eq == EQ_VX ? norm_of(b, 0) : eq == EQ_PX ? norm_of(b, 1) : eq == EQ_TX ? norm_of(b, 3) : none;
-    const bool dc = form == SOLVER_MIXED && eq != EQ_PY && eq != EQ_PX;
-    BCK(solve_batch_launch(form, (eq & 1) != 0, dc, b->tl[eq], b->g[eq], b->sol_smem[eq], b->sol_inst[eq],
-                           b->sol_items[eq], b->sol_n[eq], b->active, sn, b->stream));
+    BCK(sweep_batch(b, eq, an, sn));
     if (eq == EQ_PX) BCK(correct_batch_launch(b->cell_inst, b->corr_items, b->ncorr, b->active, 1, b->stream));
   }
   BCK(residual_batch_launch(b->cell_inst, b->res_items, b->nres, b->active, norm_of(b, 4), 1, b->stream));
@@ -512,14 +550,7 @@ int ixb_batch_autotune(ixb_batch* b, int reps, int* chosen, double* ms) {
       b->tl[eq] = shapes[k][0];
       b->g[eq] = shapes[k][1];
       if ((st = build_tables(b)) != IXB_OK) break;
-      const bool dc = form == SOLVER_MIXED && eq != EQ_PY && eq != EQ_PX;
-      auto once = [&]() -> cudaError_t {
-        cudaError_t e = form == SOLVER_MIXED ? launch_asm_eq<SOLVER_MIXED>(b, eq, none)
-                                             : launch_asm_eq<IXB_SOLVER_HYBRID>(b, eq, none);
-        if (e != cudaSuccess) return e;
-        return solve_batch_launch(form, (eq & 1) != 0, dc, b->tl[eq], b->g[eq], b->sol_smem[eq], b->sol_inst[eq],
-                                  b->sol_items[eq], b->sol_n[eq], b->active, none, b->stream);
-      };
+      auto once = [&]() -> cudaError_t { return sweep_batch(b, eq, none, none); };
       cudaError_t e = once();
       if (e == cudaErrorInvalidValue) { cudaGetLastError(); continue; }  // shape cannot run here
       if (e != cudaSuccess) { b->last_cuda = e; st = IXB_ECUDA; break; }

@@ -185,6 +185,16 @@ struct SolveInst {
   int n, line_lo, line_hi, nfull;
   int first, count;  // its work items in the launch's item list
 };
+// one instance of a batched fused sweep: its assembly view and its line solve
+struct FusedInst {
+  Geo<double> G;
+  SweepIO<double> io;
+  SolveInst s;
+};
+template <int EQ, int SOLVER>
+cudaError_t fused_batch_launch(int tl, int g, size_t smem, const FusedInst* inst, const int2* items, int nitems,
+                               const int* active, const BatchNorm& bn_asm, const BatchNorm& bn_sol,
+                               cudaStream_t st);
 // form: IXB_SOLVER_HYBRID, IXB_SOLVER_EXACT or SOLVER_MIXED; x: line along
 // ii; dc: the staged right-hand sides are binary64 residuals whose solution
 // is added to `in`

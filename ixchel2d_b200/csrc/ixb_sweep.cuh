@@ -260,24 +260,20 @@ cudaError_t assemble_launch(const SweepShape& s, const Geo<double>& G, const Swe
 // cells of a line; y-lines: consecutive threads take the TL adjacent lines
 // of a row, so the field reads stay coalesced.
 // ---------------------------------------------------------------------------
+// Rows of lines L0 .. L0+TL-1 of sweep EQ assembled into the chunk layout of
+// solve_lines (m rows per chunk at pitch mp); identity rows pad each line to
+// G*m rows.  Returns nothing; acc_bo collects the b_o norm (p'-x).
 template <int EQ, int SOLVER, int TL, int G, int M>
-__global__ void __launch_bounds__(TL * G)
-    fused_sweep_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n,
-                       const int line_lo, const int line_hi, const int nfull) {
-  IXB_PDL_ENTRY();
-  using ST = SweepTypes<SOLVER, EQ>;
-  using S = typename ST::S;
+__device__ __forceinline__ void fused_assemble(typename SweepTypes<SOLVER, EQ>::S* sm, const Geo<double>& G_,
+                                               const SweepIO<double>& io, const int m, const int mp, const int n,
+                                               const int line_lo, const int line_hi, const int L0,
+                                               double& acc_bo) {
+  using S = typename SweepTypes<SOLVER, EQ>::S;
   constexpr bool X = EqIsX<EQ>::value;
   constexpr int NT = TL * G;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S* sm = reinterpret_cast<S*>(smem_raw);
-  const int m = M > 0 ? M : so.m;
-  const int mp = M > 0 ? (M | 1) : so.mp;
   const int npad = G * m;
   const int LS = (int)line_smem_elems(G, mp);
   const int arr = G * mp;
-  const int L0 = 1 + blockIdx.x * TL;
-  double acc_bo = 0.0;
 #pragma unroll
   for (int it = 0; it < (M > 0 ? M : m); ++it) {  // with M > 0 a thread's M cells are assembled together
     const int idx = threadIdx.x + it * NT;
@@ -287,7 +283,7 @@ __global__ void __launch_bounds__(TL * G)
     const int L = L0 + l;
     const bool valid = L >= line_lo && L <= line_hi && r < n;
     Row<double> row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
-    if (!valid) row = Row<double>{0.0, 1.0, 0.0, 0.0};  // identity rows pad the line to G*m rows
+    if (!valid) row = Row<double>{0.0, 1.0, 0.0, 0.0};
     const int ch = r / m;
     const int off = l * LS + ch * mp + (r - ch * m);
     sm[off] = S(row.a);
@@ -295,13 +291,58 @@ __global__ void __launch_bounds__(TL * G)
     sm[off + 2 * arr] = S(row.c);
     sm[off + 3 * arr] = S(row.d);
   }
+}
+
+template <int EQ, int SOLVER, int TL, int G, int M>
+__global__ void __launch_bounds__(TL * G)
+    fused_sweep_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n,
+                       const int line_lo, const int line_hi, const int nfull) {
+  IXB_PDL_ENTRY();
+  using ST = SweepTypes<SOLVER, EQ>;
+  using S = typename ST::S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);
+  const int m = M > 0 ? M : so.m;
+  const int mp = M > 0 ? (M | 1) : so.mp;
+  const int L0 = 1 + blockIdx.x * TL;
+  double acc_bo = 0.0;
+  fused_assemble<EQ, SOLVER, TL, G, M>(sm, G_, io, m, mp, n, line_lo, line_hi, L0, acc_bo);
   __syncthreads();
-  const double acc =
-      solve_lines<S, X, ST::DC, SOLVER == IXB_SOLVER_EXACT, TL, G, M>(sm, so, n, line_lo, line_hi, nfull, L0);
+  const double acc = solve_lines<S, EqIsX<EQ>::value, ST::DC, SOLVER == IXB_SOLVER_EXACT, TL, G, M>(
+      sm, so, n, line_lo, line_hi, nfull, L0);
   if (io.nrm1.partials) finish_norm(io.nrm1, block_sum(acc_bo));
   if (so.nrm0.partials) {
     const bool last = finish_norm(so.nrm0, block_sum(acc));
     if (last && so.ctl.ctl && threadIdx.x == 0) ctl_inner_step(so.ctl.ctl, so.ctl.norms, so.ctl.which, so.ctl.cond);
+  }
+}
+
+// Batched fused sweep: work item i = (instance, line group) of items[i]; a
+// CTA walks the items grid-stride, skipping instances that no longer
+// iterate; the b_o norm (p'-x) and the pass norm are reduced per instance.
+template <int EQ, int SOLVER, int TL, int G>
+__global__ void __launch_bounds__(TL * G)
+    fused_batch_kernel(const FusedInst* __restrict__ inst, const int2* __restrict__ items, const int nitems,
+                       const int* __restrict__ active, const BatchNorm bn_asm, const BatchNorm bn_sol) {
+  IXB_PDL_ENTRY();
+  using ST = SweepTypes<SOLVER, EQ>;
+  using S = typename ST::S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 wi = items[it];
+    if (!active[wi.x]) continue;  // uniform across the CTA
+    const FusedInst& d = inst[wi.x];
+    const int L0 = 1 + wi.y * TL;
+    double acc_bo = 0.0;
+    fused_assemble<EQ, SOLVER, TL, G, 0>(sm, d.G, d.io, d.s.io.m, d.s.io.mp, d.s.n, d.s.line_lo, d.s.line_hi, L0,
+                                         acc_bo);
+    __syncthreads();
+    const double acc = solve_lines<S, EqIsX<EQ>::value, ST::DC, false, TL, G, 0>(sm, d.s.io, d.s.n, d.s.line_lo,
+                                                                                d.s.line_hi, d.s.nfull, L0);
+    if (bn_asm.partials) finish_item_norm(bn_asm, wi.x, d.s.first, d.s.count, it, block_sum(acc_bo));
+    if (bn_sol.partials) finish_item_norm(bn_sol, wi.x, d.s.first, d.s.count, it, block_sum(acc));
+    __syncthreads();  // the next item reuses the shared memory
   }
 }
 
@@ -337,6 +378,34 @@ cudaError_t fused_launch(const SweepShape& s, const Geo<double>& G, const SweepI
     IXB_FUSED_Y_SHAPES(IXB_FUSED_)
   }
 #undef IXB_FUSED_
+  return cudaErrorNotSupported;
+}
+
+// Launches the batched fused form of sweep EQ with one shape (TL x G) for
+// every instance; cudaErrorNotSupported for shapes outside IXB_FUSED_*_SHAPES.
+template <int EQ, int SOLVER>
+cudaError_t fused_batch_launch(int tl, int g, size_t smem, const FusedInst* inst, const int2* items, int nitems,
+                               const int* active, const BatchNorm& bn_asm, const BatchNorm& bn_sol,
+                               cudaStream_t st) {
+  auto go = [&](auto k, int nt) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, dev = 0, nsm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, nt, smem)) != cudaSuccess) return e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidValue;
+    const int grid = std::max(1, std::min(nitems, per_sm * nsm));
+    return launch_k(k, grid, nt, smem, st, inst, items, nitems, active, bn_asm, bn_sol);
+  };
+#define IXB_FBATCH_(TL_, G_) \
+  if (tl == TL_ && g == G_) return go(fused_batch_kernel<EQ, SOLVER, TL_, G_>, TL_ * G_);
+  if constexpr (EqIsX<EQ>::value) {
+    IXB_FUSED_X_SHAPES(IXB_FBATCH_)
+  } else {
+    IXB_FUSED_Y_SHAPES(IXB_FBATCH_)
+  }
+#undef IXB_FBATCH_
   return cudaErrorNotSupported;
 }
 

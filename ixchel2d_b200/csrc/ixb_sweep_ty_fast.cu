@@ -8,4 +8,6 @@ template cudaError_t assemble_batch_launch<EQ_TY, IXB_SOLVER_HYBRID>(const void*
                                                            cudaStream_t);
 template cudaError_t fused_launch<EQ_TY, IXB_SOLVER_HYBRID>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
                                                    const SolveIO&, cudaStream_t);
+template cudaError_t fused_batch_launch<EQ_TY, IXB_SOLVER_HYBRID>(int, int, size_t, const FusedInst*, const int2*, int, const int*,
+                                                         const BatchNorm&, const BatchNorm&, cudaStream_t);
 }  // namespace ixb

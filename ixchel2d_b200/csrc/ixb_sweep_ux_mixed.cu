@@ -8,4 +8,6 @@ template cudaError_t assemble_batch_launch<EQ_UX, SOLVER_MIXED>(const void*, con
                                                            cudaStream_t);
 template cudaError_t fused_launch<EQ_UX, SOLVER_MIXED>(const SweepShape&, const Geo<double>&, const SweepIO<double>&,
                                                    const SolveIO&, cudaStream_t);
+template cudaError_t fused_batch_launch<EQ_UX, SOLVER_MIXED>(int, int, size_t, const FusedInst*, const int2*, int, const int*,
+                                                         const BatchNorm&, const BatchNorm&, cudaStream_t);
 }  // namespace ixb
