@@ -660,14 +660,18 @@ def run_profile_adi():
 
 def run_profile_batch():
     """Profiling driver: 64 natural-convection cavities (side 64..512, Ra
-    1e3..1e6, seed 1234), refined form, default shapes, two batched outer
-    iterations (run with IXB_NO_GRAPH=1 so that ncu sees the kernels)."""
+    1e3..1e6, seed 1234), refined form, two batched outer iterations (run
+    with IXB_NO_GRAPH=1 so that ncu sees the kernels).  Shapes: y-sweeps
+    2 x 64 (two kernels), x-sweeps 1 x 128 (fused), the batch autotuner's
+    usual choices for the x-sweeps."""
     from ixchel2d_b200 import Batch, cases
     rng = np.random.default_rng(1234)
     sides = rng.integers(64, 513, 64)
     ras = 10.0 ** rng.uniform(3.0, 6.0, 64)
     bt = Batch.from_cases([cases.natural_cavity(int(a), int(a), Ra=float(r), T0=0.5) for a, r in zip(sides, ras)],
                           conv_paso=0.0)
+    for k in range(8):
+        bt.set_sweep_shape(k, 1 if k % 2 else 2, 128 if k % 2 else 64)
     bt.iterate(2)
     bt.close()
 

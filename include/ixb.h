@@ -177,8 +177,8 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
 int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads_per_line);
 /* Kernels one outer iteration launches with the current launch shapes (one
  * inner pass per loop): one per sweep whose shape runs assembly and line
- * solve as one kernel (x-sweeps with one line per CTA; y-sweeps with 2, 4 or
- * 8 lines per CTA), two per other sweep, plus the p' preset, the p/u/v
+ * solve as one kernel (x-sweeps with one line per CTA; y-sweeps with 4 or 8
+ * lines per CTA), two per other sweep, plus the p' preset, the p/u/v
  * correction and the u residual.  IXB_SPLIT=1 in the environment keeps every
  * sweep at two kernels. */
 int ixb_iteration_launches(ixb_handle* h, int* launches);

@@ -162,10 +162,12 @@ struct SolveIO {
   int m, mp;            // chunk rows per thread, padded pitch
 };
 // Launch shapes (lines per CTA, threads per line) of the fused sweeps:
-// x-sweeps one line per CTA; y-sweeps several adjacent lines per CTA, so
-// that a warp's field reads span adjacent lines.
+// x-sweeps one line per CTA; y-sweeps 4 or 8 adjacent lines per CTA, so
+// that a warp's field reads span adjacent lines (with 2 lines a warp reads
+// 16 separate 16-byte pieces and the fused y-sweep measured twice as slow
+// as its two kernels).
 #define IXB_FUSED_X_SHAPES(X_) X_(1, 128) X_(1, 256)
-#define IXB_FUSED_Y_SHAPES(X_) X_(2, 64) X_(2, 128) X_(4, 32) X_(4, 64) X_(8, 32)
+#define IXB_FUSED_Y_SHAPES(X_) X_(4, 32) X_(4, 64) X_(8, 32)
 inline bool fused_shape(int eq, int tl, int g) {
   bool hit = false;
 #define IXB_HIT_(TL_, G_) hit = hit || (tl == TL_ && g == G_);
