@@ -79,7 +79,6 @@ int ensure_tables(ixb_handle* h) {
   return IXB_OK;
 }
 
-const int kShapes[7][2] = {{1, 128}, {1, 256}, {2, 64}, {2, 128}, {4, 32}, {4, 64}, {8, 32}};
 
 // Default launch shape of a sweep: the fewest waves of CTAs (every CTA
 // resident at once when possible), then the shortest chunks, then the
@@ -87,8 +86,8 @@ const int kShapes[7][2] = {{1, 128}, {1, 256}, {2, 64}, {2, 128}, {4, 32}, {4, 6
 void pick_shape(ixb_handle* h, int eq) {
   int best = -1;
   long long best_key = 0;
-  for (int k = 0; k < 7; ++k) {
-    SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), kShapes[k][0], kShapes[k][1]);
+  for (int k = 0; k < kNumShapes; ++k) {
+    SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), kShapeList[k][0], kShapeList[k][1]);
     const int occ = sweep_occupancy(eq, solver_form(h), s);
     if (occ <= 0) continue;
     const long long waves = (s.grid + (long long)occ * h->nsm - 1) / ((long long)occ * h->nsm);
@@ -96,8 +95,8 @@ void pick_shape(ixb_handle* h, int eq) {
     if (best < 0 || key < best_key) { best = k; best_key = key; }
   }
   if (best < 0) best = 1;
-  h->shape_tl[eq] = kShapes[best][0];
-  h->shape_g[eq] = kShapes[best][1];
+  h->shape_tl[eq] = kShapeList[best][0];
+  h->shape_g[eq] = kShapeList[best][1];
 }
 
 // Inputs and outputs of sweep `eq` at the handle's current buffer parity;
@@ -848,9 +847,9 @@ int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads
     return IXB_OK;
   }
   int k = 0;
-  for (; k < 7; ++k)
-    if (kShapes[k][0] == lines_per_cta && kShapes[k][1] == threads_per_line) break;
-  if (k == 7) return IXB_EINVAL;
+  for (; k < kNumShapes; ++k)
+    if (kShapeList[k][0] == lines_per_cta && kShapeList[k][1] == threads_per_line) break;
+  if (k == kNumShapes) return IXB_EINVAL;
   SweepShape s = sweep_shape(sweep, h->mi, h->nj, real_bytes(h), lines_per_cta, threads_per_line);
   if (sweep_occupancy(sweep, solver_form(h), s) <= 0) return IXB_EINVAL;
   h->shape_tl[sweep] = lines_per_cta;
@@ -881,8 +880,8 @@ int ixb_autotune(ixb_handle* h, int reps, size_t flush_bytes, int* chosen, doubl
   for (int eq = 0; eq < EQ_COUNT && st == IXB_OK; ++eq) {
     double best = 1e30;
     int best_k = -1;
-    for (int k = 0; k < 7 && st == IXB_OK; ++k) {
-      if (ixb_set_sweep_shape(h, eq, kShapes[k][0], kShapes[k][1]) != IXB_OK) continue;
+    for (int k = 0; k < kNumShapes && st == IXB_OK; ++k) {
+      if (ixb_set_sweep_shape(h, eq, kShapeList[k][0], kShapeList[k][1]) != IXB_OK) continue;
       st = sweep(h, eq, nullptr, false);  // warm-up
       double total = 0.0;
       for (int r = 0; r < reps && st == IXB_OK; ++r) {
@@ -903,9 +902,9 @@ int ixb_autotune(ixb_handle* h, int reps, size_t flush_bytes, int* chosen, doubl
     }
     if (st != IXB_OK) break;
     if (best_k < 0) { st = IXB_ECUDA; break; }
-    h->shape_tl[eq] = kShapes[best_k][0];
-    h->shape_g[eq] = kShapes[best_k][1];
-    if (chosen) { chosen[2 * eq] = kShapes[best_k][0]; chosen[2 * eq + 1] = kShapes[best_k][1]; }
+    h->shape_tl[eq] = kShapeList[best_k][0];
+    h->shape_g[eq] = kShapeList[best_k][1];
+    if (chosen) { chosen[2 * eq] = kShapeList[best_k][0]; chosen[2 * eq + 1] = kShapeList[best_k][1]; }
     if (ms) ms[eq] = best;
   }
   for (int k = 0; k < nsave; ++k)

@@ -504,7 +504,7 @@ int ixb_batch_instance(ixb_batch* b, int i, ixb_handle** h) {
 
 int ixb_batch_set_sweep_shape(ixb_batch* b, int sweep, int lines_per_cta, int threads_per_line) {
   if (!b || sweep < 0 || sweep >= EQ_COUNT) return IXB_EINVAL;
-  static const int shapes[7][2] = {{1, 128}, {1, 256}, {2, 64}, {2, 128}, {4, 32}, {4, 64}, {8, 32}};
+  const auto& shapes = kShapeList;
   bool ok = lines_per_cta == 0;
   for (auto& s : shapes) ok |= (s[0] == lines_per_cta && s[1] == threads_per_line);
   if (!ok) return IXB_EINVAL;
@@ -516,7 +516,7 @@ int ixb_batch_set_sweep_shape(ixb_batch* b, int sweep, int lines_per_cta, int th
 
 int ixb_batch_autotune(ixb_batch* b, int reps, int* chosen, double* ms) {
   if (!b || reps < 1) return IXB_EINVAL;
-  static const int shapes[7][2] = {{1, 128}, {1, 256}, {2, 64}, {2, 128}, {4, 32}, {4, 64}, {8, 32}};
+  const auto& shapes = kShapeList;
   for (ixb_handle* h : b->h) BCK(cudaStreamSynchronize(h->stream));
   // every buffer a sweep may write, saved and restored around the trials
   std::vector<std::pair<double*, double*>> saved;
@@ -546,7 +546,7 @@ int ixb_batch_autotune(ixb_batch* b, int reps, int* chosen, double* ms) {
   for (int eq = 0; eq < EQ_COUNT && st == IXB_OK; ++eq) {
     double best = 1e300;
     int bk = -1;
-    for (int k = 0; k < 7 && st == IXB_OK; ++k) {
+    for (int k = 0; k < kNumShapes && st == IXB_OK; ++k) {
       b->tl[eq] = shapes[k][0];
       b->g[eq] = shapes[k][1];
       if ((st = build_tables(b)) != IXB_OK) break;

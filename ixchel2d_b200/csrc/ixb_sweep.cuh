@@ -282,8 +282,9 @@ __device__ __forceinline__ void fused_assemble(typename SweepTypes<SOLVER, EQ>::
     else { l = idx % TL; r = idx / TL; }
     const int L = L0 + l;
     const bool valid = L >= line_lo && L <= line_hi && r < n;
-    Row<double> row = staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, valid, acc_bo);
-    if (!valid) row = Row<double>{0.0, 1.0, 0.0, 0.0};
+    // padding rows and unsolved lines: identity rows, nothing to assemble
+    const Row<double> row = valid ? staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, true, acc_bo)
+                                  : Row<double>{0.0, 1.0, 0.0, 0.0};
     const int ch = r / m;
     const int off = l * LS + ch * mp + (r - ch * m);
     sm[off] = S(row.a);
