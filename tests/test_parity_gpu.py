@@ -142,6 +142,47 @@ def test_iteration_launch_count():
     assert g.iteration_launches() == 3 * 2 + 5 * 1 + 3
 
 
+_SPLIT_CHILD = """
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from ixchel2d_b200 import Simple2D, cases
+from ixchel2d_b200 import _ffi as F
+from oracle import oracle as O
+from tests.conftest import relerr
+STATE = ("u", "v", "p", "T", "u_ant", "v_ant", "T_ant")
+case = cases.lid_driven_mixed(45, 29)
+for solver, iters in ((F.SOLVER_EXACT, 40), (F.SOLVER_HYBRID, 200)):
+    for shape in ((1, 128), (1, 256)):
+        g = Simple2D.from_case(case, solver=solver)
+        o = O.OracleCase(case, solver=solver)
+        for k in range(8):
+            g.set_sweep_shape(k, *shape)
+        assert g.iteration_launches() == 19, g.iteration_launches()
+        g.iterations(iters)
+        o.iterations(iters)
+        gs, os_ = g.download(), o.get_state()
+        for k in STATE:
+            if solver == F.SOLVER_EXACT:
+                assert np.array_equal(gs[k], os_[k]), (k, shape)
+            else:
+                assert relerr(gs[k], os_[k]) < 1e-10, (k, shape, relerr(gs[k], os_[k]))
+print("ok")
+"""
+
+
+def test_two_kernel_form_keeps_parity():
+    # IXB_SPLIT=1 (read once per process) keeps every sweep at two kernels,
+    # assembly and line solve: parity of that form for the one-line x shapes
+    # that otherwise run fused, in a child process
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _SPLIT_CHILD, root], env={**os.environ, "IXB_SPLIT": "1"},
+                       capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]
+
+
 def test_autotune_then_parity():
     case = cases.natural_cavity(40, 36, Ra=1e5)
     g, o = _pair(case)
