@@ -6,7 +6,9 @@
 ! region of :356-389 / :1277) by the calls shown in INTEGRATION.md.
 !
 ! The derived types mirror the C structs field by field (bind(C)); arrays
-! keep the reference's Fortran shapes and are passed by reference.
+! keep the reference's Fortran shapes and are passed by reference.  Every
+! function of ixb.h has an interface here; the batched line solves take
+! device addresses (type(c_ptr), e.g. from an OpenACC host_data region).
 !
 module ixb
   use iso_c_binding
@@ -210,6 +212,158 @@ module ixb
        integer(c_int), value :: i
        type(ixb_report), intent(out) :: rep
      end function ixb_batch_report
+     ! ---- library, handle and diagnostics ----
+     integer(c_int) function ixb_version() bind(C, name="ixb_version")
+       import :: c_int
+     end function ixb_version
+
+     type(c_ptr) function ixb_strerror(status) bind(C, name="ixb_strerror")  ! a C string (c_f_pointer to read)
+       import :: c_int, c_ptr
+       integer(c_int), value :: status
+     end function ixb_strerror
+
+     integer(c_int) function ixb_device_count() bind(C, name="ixb_device_count")
+       import :: c_int
+     end function ixb_device_count
+
+     integer(c_int) function ixb_set_stream(h, stream) bind(C, name="ixb_set_stream")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, stream          ! stream: a cudaStream_t
+     end function ixb_set_stream
+
+     integer(c_int) function ixb_download_aux(h, au, av, b_o, resu, corr_pres) bind(C, name="ixb_download_aux")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: au(*), av(*), b_o(*), resu(*), corr_pres(*)
+     end function ixb_download_aux
+
+     integer(c_int) function ixb_set_work(h, corr_pres, au, av) bind(C, name="ixb_set_work")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(in) :: corr_pres(*), au(*), av(*)
+     end function ixb_set_work
+
+     integer(c_int) function ixb_roll(h) bind(C, name="ixb_roll")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function ixb_roll
+
+     integer(c_int) function ixb_phase(h, which) bind(C, name="ixb_phase")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: which
+     end function ixb_phase
+
+     integer(c_int) function ixb_time_phases(h, reps, flush_bytes, ms) bind(C, name="ixb_time_phases")
+       import :: c_int, c_ptr, c_size_t, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: reps
+       integer(c_size_t), value :: flush_bytes
+       real(c_double), intent(out) :: ms(*)
+     end function ixb_time_phases
+
+     ! ---- launch shapes ----
+     integer(c_int) function ixb_set_sweep_shape(h, sweep, lines_per_cta, threads_per_line) &
+          bind(C, name="ixb_set_sweep_shape")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: sweep, lines_per_cta, threads_per_line
+     end function ixb_set_sweep_shape
+
+     integer(c_int) function ixb_iteration_launches(h, launches) bind(C, name="ixb_iteration_launches")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), intent(out) :: launches
+     end function ixb_iteration_launches
+
+     integer(c_int) function ixb_autotune(h, reps, flush_bytes, chosen, ms) bind(C, name="ixb_autotune")
+       import :: c_int, c_ptr, c_size_t, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: reps
+       integer(c_size_t), value :: flush_bytes
+       integer(c_int), intent(out) :: chosen(16)
+       real(c_double), intent(out) :: ms(8)
+     end function ixb_autotune
+
+     integer(c_int) function ixb_batch_set_sweep_shape(b, sweep, lines_per_cta, threads_per_line) &
+          bind(C, name="ixb_batch_set_sweep_shape")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: b
+       integer(c_int), value :: sweep, lines_per_cta, threads_per_line
+     end function ixb_batch_set_sweep_shape
+
+     integer(c_int) function ixb_batch_autotune(b, reps, chosen, ms) bind(C, name="ixb_batch_autotune")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: b
+       integer(c_int), value :: reps
+       integer(c_int), intent(out) :: chosen(16)
+       real(c_double), intent(out) :: ms(8)
+     end function ixb_batch_autotune
+
+     ! ---- batched line solves on DEVICE arrays (a..x: device addresses) ----
+     integer(c_int) function ixb_tridiag_f64(a, b, c, d, x, n, nsys, layout, solver, stream) &
+          bind(C, name="ixb_tridiag_f64")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: a, b, c, d, x, stream
+       integer(c_int), value :: n, nsys, layout, solver
+     end function ixb_tridiag_f64
+
+     integer(c_int) function ixb_tridiag_f32(a, b, c, d, x, n, nsys, layout, solver, stream) &
+          bind(C, name="ixb_tridiag_f32")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: a, b, c, d, x, stream
+       integer(c_int), value :: n, nsys, layout, solver
+     end function ixb_tridiag_f32
+
+     integer(c_int) function ixb_tridiag_f64_noalloc(a, b, c, d, x, n, nsys, layout, solver, stream) &
+          bind(C, name="ixb_tridiag_f64_noalloc")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: a, b, c, d, x, stream
+       integer(c_int), value :: n, nsys, layout, solver
+     end function ixb_tridiag_f64_noalloc
+
+     integer(c_int) function ixb_tridiag_status() bind(C, name="ixb_tridiag_status")
+       import :: c_int
+     end function ixb_tridiag_status
+
+     ! ---- energy equation with the flow held fixed, and its adjoint ----
+     integer(c_int) function ixb_energy_iterations(h, n) bind(C, name="ixb_energy_iterations")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: n
+     end function ixb_energy_iterations
+
+     integer(c_int) function ixb_adjoint_energy(h, K, j0, j1, grad) bind(C, name="ixb_adjoint_energy")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: K, j0, j1
+       real(c_double), intent(out) :: grad(*)
+     end function ixb_adjoint_energy
+
+     integer(c_int) function ixb_set_bc_values(h, var, side, values) bind(C, name="ixb_set_bc_values")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: var, side
+       real(c_double), intent(in) :: values(*)
+     end function ixb_set_bc_values
+
+     ! ---- host-side inputs ----
+     integer(c_int) function ixb_mesh_axis(mkind, n, length, param, centre, nodes) bind(C, name="ixb_mesh_axis")
+       import :: c_int, c_double
+       integer(c_int), value :: mkind, n
+       real(c_double), value :: length, param, centre
+       real(c_double), intent(out) :: nodes(*)
+     end function ixb_mesh_axis
+
+     integer(c_int) function ixb_bc_locate(side, ndivis, x1, btype, bvalue, xx, mm, yy, nn, out) &
+          bind(C, name="ixb_bc_locate")
+       import :: c_int, c_double, ixb_bc_side
+       integer(c_int), value :: side, ndivis, mm, nn
+       real(c_double), intent(in) :: x1(*), bvalue(*), xx(*), yy(*)
+       integer(c_int), intent(in) :: btype(*)
+       type(ixb_bc_side), intent(out) :: out
+     end function ixb_bc_locate
+
   end interface
 
 end module ixb
