@@ -29,6 +29,12 @@ def test_every_declared_symbol_is_exported_and_bound():
     assert set(names) == bound
 
 
+def test_fortran_module_binds_every_declared_function():
+    txt = (ROOT / "include" / "mod_ixb.f90").read_text()
+    bound = set(re.findall(r'bind\(C,\s*name="(ixb_\w+)"\)', txt))
+    assert bound == set(_declared())
+
+
 def test_strerror_and_version():
     assert F.lib.ixb_version() >= 100
     for s in range(9):
