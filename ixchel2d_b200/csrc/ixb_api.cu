@@ -447,6 +447,14 @@ int xfer_state(ixb_handle* h, const std::array<double*, 7>& pad, const std::arra
     ++s.n;
   }
   if (s.n == 0) return IXB_OK;
+  if (!h->xfer) {  // allocated on the first transfer (7 host-shaped arrays)
+    CK(cudaStreamSynchronize(h->stream));
+    if (cudaMalloc(&h->xfer, (size_t)7 * (mi + 1) * (nj + 1) * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      h->xfer = nullptr;
+      return IXB_ENOMEM;
+    }
+  }
   const dim3 grid(148 * 2, s.n);
   if (upload) {
     for (int k = 0, q = 0; k < 7; ++k) {
@@ -549,8 +557,6 @@ int ixb_create(int mi, int nj, int prec_mode, ixb_handle** out) {
     if (cudaMalloc(f, fb) != cudaSuccess) return fail(IXB_ENOMEM);
     if (cudaMemset(*f, 0, fb) != cudaSuccess) return fail(IXB_ECUDA);
   }
-  if (cudaMalloc(&h->xfer, (size_t)7 * (mi + 1) * (nj + 1) * sizeof(double)) != cudaSuccess)
-    return fail(IXB_ENOMEM);
   // au = av = 1e40 (main.f90:309-310)
   {
     std::vector<double> big(h->fsz, 1.e40);

@@ -76,7 +76,7 @@ struct ixb_handle {
   int shape_g[ixb::EQ_COUNT] = {};
   int nsm = 148;
   // adjoint workspace (ixb_adjoint_energy), allocated on first use
-  double* xfer = nullptr;  // seven host-shaped (column-major, unpadded) state arrays: the state transfers' staging
+  double* xfer = nullptr;  // seven host-shaped (column-major, unpadded) state arrays: the state transfers' staging, allocated on the first transfer
   double* adj_pool = nullptr;
   size_t adj_size = 0;
 };
