@@ -169,7 +169,7 @@ int ixb_phase(ixb_handle* h, int which);
 int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
 /* Launch shape of one sweep (0..7 = u-y, u-x, v-y, v-x, p'-y, p'-x, T-y,
  * T-x): lines per CTA and threads per line, one of (1,128) (1,256) (1,512)
- * (2,64) (2,128) (4,32) (4,64) (8,32); each thread eliminates a chunk of
+ * (2,64) (2,128) (4,32) (4,64) (8,32) (16,16); each thread eliminates a chunk of
  * max(3, ceil(n/threads_per_line)) rows.  lines_per_cta = 0 restores the
  * default (the fewest waves of resident CTAs, then the shortest chunks).
  * No reference counterpart: the reference runs one sequential tridiagonal
@@ -177,8 +177,8 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
 int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads_per_line);
 /* Kernels one outer iteration launches with the current launch shapes (one
  * inner pass per loop): one per sweep whose shape runs assembly and line
- * solve as one kernel (x-sweeps with one line per CTA; y-sweeps with 4 or 8
- * lines per CTA), two per other sweep, plus the p' preset, the p/u/v
+ * solve as one kernel (x-sweeps with one line per CTA; y-sweeps with 4, 8 or
+ * 16 lines per CTA), two per other sweep, plus the p' preset, the p/u/v
  * correction and the u residual.  IXB_SPLIT=1 in the environment keeps every
  * sweep at two kernels. */
 int ixb_iteration_launches(ixb_handle* h, int* launches);
