@@ -415,8 +415,12 @@ def adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, warm=500, fd_nodes=8):
     cavity n x n, Ra, after `warm` SIMPLE iterations; hot-wall profile of
     `nodes` piecewise-linear nodes, value 1 + U(-0.05, 0.05) (seed 1234);
     objective the hot-wall Nusselt number after K passes of the T sweeps.
-    Gradient by the adjoint against central differences (h = 1e-6) of the
-    same GPU forward on fd_nodes of the nodes."""
+    Gradient by the adjoint against central differences of the same GPU
+    forward on fd_nodes of the nodes, with h = 1e-6 and with h = 1e-2: with
+    the flow held fixed the objective is affine in the nodes, so central
+    differences are exact for any step and the small step only adds the
+    forward's rounding divided by h.  A linearity check compares
+    J(theta + d) - J(theta) with the adjoint's g . d."""
     from ixchel2d_b200 import Simple2D, cases
     from ixchel2d_b200.adjoint import HotWallNusselt
     case = cases.natural_cavity(n, n, Ra=Ra, T0=0.5)
@@ -434,19 +438,27 @@ def adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, warm=500, fd_nodes=8):
     nu = J.value(theta)
     t_fwd = time.perf_counter() - t0
     pick = np.linspace(0, nodes - 1, fd_nodes).astype(int)
-    h = 1e-6
-    fd = np.zeros(fd_nodes)
-    for q, k in enumerate(pick):
-        e = np.zeros(nodes)
-        e[k] = h
-        fd[q] = (J.value(theta + e) - J.value(theta - e)) / (2 * h)
+    fds = {}
+    for h in (1e-6, 1e-2):
+        fd = np.zeros(fd_nodes)
+        for q, k in enumerate(pick):
+            e = np.zeros(nodes)
+            e[k] = h
+            fd[q] = (J.value(theta + e) - J.value(theta - e)) / (2 * h)
+        fds[h] = fd
+    d = rng.uniform(-0.01, 0.01, nodes)
+    dj = J.value(theta + d) - nu
     sim.close()
+    fd = fds[1e-6]
     return {"case": f"natural_cavity_{n}x{n}_Ra{Ra:g}", "flow": f"held fixed after {warm} SIMPLE iterations",
             "nodes": nodes, "K": K, "nu_hot_wall": nu,
             "adjoint_s": t_adj, "forward_s": t_fwd, "fd_all_nodes_s_estimate": 2 * nodes * t_fwd,
             "fd_nodes_checked": fd_nodes,
             "max_rel_err_vs_fd": float(np.max(np.abs(g[pick] - fd) / np.maximum(np.abs(fd), 1e-300))),
-            "normwise_rel_err_vs_fd": float(np.linalg.norm(g[pick] - fd) / np.linalg.norm(fd))}
+            "normwise_rel_err_vs_fd": float(np.linalg.norm(g[pick] - fd) / np.linalg.norm(fd)),
+            "max_rel_err_vs_fd_h1e-2": float(np.max(np.abs(g[pick] - fds[1e-2]) /
+                                                 np.maximum(np.abs(fds[1e-2]), 1e-300))),
+            "linearity_rel_err": float(abs(dj - g @ d) / abs(dj))}
 
 
 def make_sim(case, prec, stream, shapes):
