@@ -688,6 +688,20 @@ def run_profile_batch():
     bt.close()
 
 
+def run_profile_adjoint():
+    """Profiling driver: the energy adjoint on the 256 x 256 cavity (Ra 1e5)
+    after 50 SIMPLE iterations, 128 hot-wall nodes, K = 2 passes (one launch
+    of each adjoint kernel per sweep)."""
+    from ixchel2d_b200 import Simple2D, cases
+    from ixchel2d_b200.adjoint import HotWallNusselt
+    case = cases.natural_cavity(256, 256, Ra=1e5, T0=0.5)
+    sim = Simple2D.from_case(case)
+    sim.iterations(50)
+    J = HotWallNusselt(sim, sim.download(), case.yp, 128, 2, 2, 254)
+    J.gradient(np.ones(128))
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -701,6 +715,7 @@ def main():
     ap.add_argument("--save-shapes", help="write the autotuned sweep launch shapes to this JSON file")
     ap.add_argument("--profile-adi", action="store_true", help="run the line-solve profiling driver")
     ap.add_argument("--profile-batch", action="store_true", help="run the batched-cavities profiling driver")
+    ap.add_argument("--profile-adjoint", action="store_true", help="run the energy-adjoint profiling driver")
     args = ap.parse_args()
     if args.profile_phases:
         run_profile_phases(args.prec, args.shapes)
@@ -710,6 +725,9 @@ def main():
         return
     if args.profile_batch:
         run_profile_batch()
+        return
+    if args.profile_adjoint:
+        run_profile_adjoint()
         return
     if args.warmup < 3:
         args.warmup = 3
