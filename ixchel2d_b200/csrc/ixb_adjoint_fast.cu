@@ -209,11 +209,25 @@ extern "C" int ixb_adjoint_energy(ixb_handle* h, int K, int j0, int j1, double* 
     ACK(cudaGetLastError());
     return IXB_OK;
   };
-  // K passes of (T-y, T-x), reversed: T-x first
-  for (int k = 0; k < K; ++k) {
-    int r = reverse(sx, lam, lam2);
+  // K passes of (T-y, T-x), reversed: T-x first.  A WHILE graph runs them
+  // kLoopUnroll at a time (rebuilt when the handle or its workspace
+  // changes); the remaining K mod kLoopUnroll are plain launches
+  const std::function<int()> pass = [&]() -> int {
+    const int r1 = reverse(sx, lam, lam2);
+    return r1 != IXB_OK ? r1 : reverse(sy, lam2, lam);
+  };
+  if (K >= kLoopUnroll) {
+    if (h->agraph_dirty || !h->agraph_exec || h->agraph_pool != h->adj_pool) {
+      const int r = handle_build_loop_graph(h, pass, kLoopUnroll, &h->agraph, &h->agraph_exec);
+      if (r != IXB_OK) return r;
+      h->agraph_dirty = false;
+      h->agraph_pool = h->adj_pool;
+    }
+    const int r = handle_run_loop_graph(h, h->agraph_exec, K / kLoopUnroll);
     if (r != IXB_OK) return r;
-    r = reverse(sy, lam2, lam);
+  }
+  for (int k = 0; k < K % kLoopUnroll; ++k) {
+    const int r = pass();
     if (r != IXB_OK) return r;
   }
   std::vector<double> g(nj + 2);

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <array>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -255,6 +256,12 @@ __global__ void ctl_begin_kernel(Ctl* c, cudaGraphConditionalHandle outer) {
   c->n_simple = c->n_momen = c->n_pres = c->n_ener = 0;
 }
 
+// Counter of a K-pass WHILE loop: closes the loop after the pass that
+// brings `left` to zero.
+__global__ void loop_count_kernel(int* left, cudaGraphConditionalHandle cond) {
+  if (--*left <= 0) cudaGraphSetConditional(cond, 0u);
+}
+
 // Add a WHILE node to `g` after `dep` and return its body graph.
 int add_while(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, cudaGraphConditionalHandle cond,
               cudaGraph_t* body, cudaGraphNode_t* node) {
@@ -394,6 +401,11 @@ int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
 void free_all(ixb_handle* h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->egraph_exec) cudaGraphExecDestroy(h->egraph_exec);
+  if (h->egraph) cudaGraphDestroy(h->egraph);
+  if (h->agraph_exec) cudaGraphExecDestroy(h->agraph_exec);
+  if (h->agraph) cudaGraphDestroy(h->agraph);
+  if (h->loop_left) cudaFree(h->loop_left);
   double** bufs[] = {&h->u[0], &h->u[1], &h->v[0], &h->v[1], &h->T[0], &h->T[1], &h->pc[0], &h->pc[1],
                      &h->p, &h->u_ant, &h->v_ant, &h->T_ant, &h->au, &h->av, &h->b_o, &h->resu, &h->zero,
                      &h->fcon[0], &h->fcon[1], &h->fcon[2], &h->flin[0], &h->flin[1], &h->flin[2],
@@ -616,7 +628,7 @@ int ixb_set_stream(ixb_handle* h, void* stream) {
   if (h->own_stream) cudaStreamDestroy(h->stream);
   h->stream = (cudaStream_t)stream;
   h->own_stream = false;
-  h->graph_dirty = true;
+  h->graph_dirty = h->egraph_dirty = h->agraph_dirty = true;
   return IXB_OK;
 }
 
@@ -664,7 +676,7 @@ int ixb_set_params(ixb_handle* h, const ixb_params* p) {
     for (int k = 0; k < EQ_COUNT; ++k) h->shape_tl[k] = h->shape_g[k] = 0;
   h->prm = *p;
   h->has_params = true;
-  h->graph_dirty = true;
+  h->graph_dirty = h->egraph_dirty = h->agraph_dirty = true;
   return IXB_OK;
 }
 
@@ -718,7 +730,7 @@ int ixb_set_sources(ixb_handle* h, int var, const double* fcon, const double* fl
     TRY(put2d(h, *pc[k], src[k], rows, cols));
   }
   CK(cudaStreamSynchronize(h->stream));
-  h->graph_dirty = true;
+  h->graph_dirty = h->egraph_dirty = h->agraph_dirty = true;
   return IXB_OK;
 }
 
@@ -900,7 +912,7 @@ int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads
   if (!h || sweep < 0 || sweep >= EQ_COUNT) return IXB_EINVAL;
   if (lines_per_cta == 0) {  // back to the default choice
     h->shape_tl[sweep] = h->shape_g[sweep] = 0;
-    h->graph_dirty = true;
+    h->graph_dirty = h->egraph_dirty = h->agraph_dirty = true;
     return IXB_OK;
   }
   int k = 0;
@@ -911,7 +923,7 @@ int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads
   if (sweep_occupancy(sweep, solver_form(h), s) <= 0) return IXB_EINVAL;
   h->shape_tl[sweep] = lines_per_cta;
   h->shape_g[sweep] = threads_per_line;
-  h->graph_dirty = true;
+  h->graph_dirty = h->egraph_dirty = h->agraph_dirty = true;
   return IXB_OK;
 }
 
@@ -972,7 +984,7 @@ int ixb_autotune(ixb_handle* h, int reps, size_t flush_bytes, int* chosen, doubl
   if (e1) cudaEventDestroy(e1);
   if (flush) cudaFree(flush);
   cudaFree(save);
-  h->graph_dirty = true;
+  h->graph_dirty = h->egraph_dirty = h->agraph_dirty = true;
   return st;
 }
 
@@ -995,10 +1007,19 @@ static int nusselt(ixb_handle* h, int vertical, int k0, int k1, double* nu0, dou
 int ixb_energy_iterations(ixb_handle* h, int n) {
   if (!h || n < 0) return IXB_EINVAL;
   TRY(ready(h));
-  for (int k = 0; k < n; ++k) {
+  if (n == 0) return IXB_OK;
+  // one pass, T-y then T-x (buffer parity back to 0); kLoopUnroll of them
+  // form the body of a WHILE loop, the rest run as plain launches
+  const std::function<int()> pass = [h]() -> int {
     TRY(sweep(h, EQ_TY, nullptr, false));
-    TRY(sweep(h, EQ_TX, nullptr, false));
+    return sweep(h, EQ_TX, nullptr, false);
+  };
+  if (h->egraph_dirty || !h->egraph_exec) {
+    TRY(handle_build_loop_graph(h, pass, kLoopUnroll, &h->egraph, &h->egraph_exec));
+    h->egraph_dirty = false;
   }
+  if (n >= kLoopUnroll) TRY(handle_run_loop_graph(h, h->egraph_exec, n / kLoopUnroll));
+  for (int k = 0; k < n % kLoopUnroll; ++k) TRY(pass());
   CK(cudaStreamSynchronize(h->stream));
   return IXB_OK;
 }
@@ -1048,6 +1069,34 @@ int ixb_tridiag_status(void) {
 }  // extern "C"
 
 namespace ixb {
+int handle_build_loop_graph(ixb_handle* h, const std::function<int()>& pass, int unroll, cudaGraph_t* graph,
+                            cudaGraphExec_t* exec) {
+  if (*exec) { cudaGraphExecDestroy(*exec); *exec = nullptr; }
+  if (*graph) { cudaGraphDestroy(*graph); *graph = nullptr; }
+  if (!h->loop_left && cudaMalloc(&h->loop_left, sizeof(int)) != cudaSuccess) return IXB_ENOMEM;
+  TRY(normalize_parity(h));
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  *graph = g;
+  cudaGraphConditionalHandle c;
+  CK(cudaGraphConditionalHandleCreate(&c, g, 1, cudaGraphCondAssignDefault));
+  cudaGraph_t body;
+  cudaGraphNode_t wnode, last;
+  TRY(add_while(h, g, nullptr, c, &body, &wnode));
+  TRY(capture_into(h, body, nullptr, [&]() -> int {
+    for (int u = 0; u < unroll; ++u) TRY(pass());
+    loop_count_kernel<<<1, 1, 0, h->stream>>>(h->loop_left, c);
+    return cudaGetLastError() == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &last));
+  CK(cudaGraphInstantiate(exec, g, 0));
+  return IXB_OK;
+}
+int handle_run_loop_graph(ixb_handle* h, cudaGraphExec_t exec, int passes) {
+  TRY(normalize_parity(h));
+  CK(cudaMemcpyAsync(h->loop_left, &passes, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaGraphLaunch(exec, h->stream));
+  return IXB_OK;
+}
 Geo<double> handle_geo(const ixb_handle* h) { return make_geo(h); }
 int handle_solver_form(const ixb_handle* h) { return solver_form(h); }
 int handle_ready(ixb_handle* h) { return ready(h); }

@@ -2,6 +2,7 @@
 // CUDA stream), shared by the single-instance driver (ixb_api.cu) and the
 // batched driver (ixb_batch.cu).  Not part of the public ABI.
 #pragma once
+#include <functional>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -67,6 +68,14 @@ struct ixb_handle {
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   bool graph_dirty = true;
+  // K passes of the energy sweeps (ixb_energy_iterations) and of the energy
+  // adjoint's reversed sweeps (ixb_adjoint_energy): WHILE graphs whose
+  // counter kernel closes the loop after `loop_left` passes
+  cudaGraphExec_t egraph_exec = nullptr, agraph_exec = nullptr;
+  cudaGraph_t egraph = nullptr, agraph = nullptr;
+  bool egraph_dirty = true, agraph_dirty = true;
+  const double* agraph_pool = nullptr;  // adj_pool the adjoint graph was built on
+  int* loop_left = nullptr;
   // params and flags
   ixb_params prm{};
   bool has_mesh = false, has_params = false, has_bc[3] = {false, false, false};
@@ -87,6 +96,14 @@ Geo<double> handle_geo(const ixb_handle* h);
 int handle_solver_form(const ixb_handle* h);
 int handle_ready(ixb_handle* h);  // mesh, params and boundary tables set; mesh tables built
 // inputs/outputs of sweep `eq` at the current buffer parity (flips it), no norms
+// WHILE graph whose body runs `pass` (launches on the handle's stream that
+// leave buffer parity unchanged) `unroll` times, then a counter: built once,
+// run by handle_run_loop_graph(h, exec, iterations) (stream-ordered,
+// iterations >= 1; unroll * iterations passes)
+constexpr int kLoopUnroll = 10;
+int handle_build_loop_graph(ixb_handle* h, const std::function<int()>& pass, int unroll, cudaGraph_t* graph,
+                            cudaGraphExec_t* exec);
+int handle_run_loop_graph(ixb_handle* h, cudaGraphExec_t exec, int iterations);
 SweepIO<double> handle_sweep_io(ixb_handle* h, int eq, const double* prev);
 int handle_real_bytes(const ixb_handle* h);  // element size of the staged rows
 }  // namespace ixb
