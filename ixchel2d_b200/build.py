@@ -1,7 +1,9 @@
 """Build libixb.so in-tree for sm_100a with nvcc.
 
 Run ``python -m ixchel2d_b200.build`` (or call :func:`build`).  Objects go to
-``ixchel2d_b200/_build/``; the shared library to ``ixchel2d_b200/libixb.so``.
+``ixchel2d_b200/_build/``; the shared library to ``ixchel2d_b200/libixb.so``
+and the case driver (PROGRAM IXCHEL2D on the library) to
+``ixchel2d_b200/ixchel2d_gpu``.
 Rebuilds only what changed (any header change rebuilds every object).
 """
 from __future__ import annotations
@@ -17,6 +19,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libixb.so"
+DRIVER = PKG / "ixchel2d_gpu"
 INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -93,7 +96,25 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> Path:
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_driver()
     return LIB
+
+
+def build_driver() -> Path:
+    """Link the ixchel2d_gpu case driver against libixb.so (found next to it
+    at run time through an $ORIGIN rpath)."""
+    srcs = [CSRC / "driver" / "ixchel2d_gpu.cpp", CSRC / "ixb_listdir.cpp"]
+    deps = srcs + [LIB, CSRC / "ixb_listdir.h", INCLUDE / "ixb.h"]
+    if DRIVER.exists() and DRIVER.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return DRIVER
+    tmp = DRIVER.with_name(DRIVER.name + ".tmp")
+    cmd = [HOST_CXX, *CXXFLAGS, "-o", str(tmp), *map(str, srcs), "-L", str(PKG), "-lixb",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, DRIVER)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -24,39 +24,6 @@
 
 namespace {
 
-// Fortran Dw.d output of x with w = 23, d = 15: "0.ddddddddddddddd" mantissa,
-// exponent "D+ee" (|e| <= 99) or "+eee" (the D dropped for |e| > 99),
-// right-justified.  The 15 digits are those of the correctly rounded
-// %.14E conversion.
-std::string fmt_d23_15(double x) {
-  char buf[64];
-  std::string mant, exps;
-  if (x == 0.0 || !std::isfinite(x)) {
-    if (!std::isfinite(x)) {
-      std::snprintf(buf, sizeof buf, "%23s", std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity"));
-      return buf;
-    }
-    mant = "0.000000000000000";
-    exps = "D+00";
-  } else {
-    std::snprintf(buf, sizeof buf, "%.14E", std::fabs(x));  // d.ddddddddddddddE+xx
-    const char* e = std::strchr(buf, 'E');
-    const int ex = std::atoi(e + 1) + 1;
-    std::string digits;
-    digits.push_back(buf[0]);
-    digits.append(buf + 2, (size_t)(e - (buf + 2)));
-    mant = "0." + digits;
-    const int ax = ex < 0 ? -ex : ex;
-    char eb[16];
-    if (ax <= 99) std::snprintf(eb, sizeof eb, "D%c%02d", ex < 0 ? '-' : '+', ax);
-    else std::snprintf(eb, sizeof eb, "%c%03d", ex < 0 ? '-' : '+', ax);
-    exps = eb;
-  }
-  std::string s = (x < 0 ? "-" : "") + mant + exps;
-  if (s.size() < 23) s.insert(0, 23 - s.size(), ' ');
-  return s;
-}
-
 double round_d23_15(double x) {
   char buf[64];
   std::snprintf(buf, sizeof buf, "%.14E", x);
@@ -64,6 +31,8 @@ double round_d23_15(double x) {
 }
 
 }  // namespace
+
+using ixb::fmt_d23_15;
 
 extern "C" {
 

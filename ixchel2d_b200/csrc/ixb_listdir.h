@@ -1,4 +1,5 @@
-// ixb_listdir.h -- Fortran list-directed record reader (host only).
+// ixb_listdir.h -- Fortran list-directed record reader and Dw.d output for
+// the reference's text files (host only).
 #pragma once
 #include <cstdio>
 #include <string>
@@ -25,5 +26,7 @@ bool parse_int(const std::string& t, int* out);
 bool parse_logical(const std::string& t, int* out);
 std::string fortran_char(const std::string& t, size_t len);
 int bc_type_code(const std::string& tipo4);
+// x as Fortran D23.15 writes it (right-justified in 23 columns)
+std::string fmt_d23_15(double x);
 
 }  // namespace ixb
