@@ -496,7 +496,7 @@ int main(int argc, char** argv) {
 
   int itera = 0;
   double nusselt0 = 0.0, nusselt1 = 0.0, maxbo = 0.0, residuo = 0.0;
-  int64_t simple_total = 0, limit_hits = 0;
+  int64_t simple_total = 0, limit_hits = 0, momen_total = 0, pres_total = 0, ener_total = 0;
   const auto t0 = std::chrono::steady_clock::now();
   for (int ll = 1; ll <= P.itermax / P.paq_itera; ++ll) {
     for (int kk = 1; kk <= P.paq_itera; ++kk) {
@@ -507,6 +507,9 @@ int main(int argc, char** argv) {
       maxbo = rep.maxbo;
       residuo = rep.residuo;
       simple_total += rep.n_simple;
+      momen_total += rep.n_momen;
+      pres_total += rep.n_pres;
+      ener_total += rep.n_ener;
       if (rep.exit_code == 2) ++limit_hits;
       ++itera;
       if (say && itera % 500 == 0)
@@ -606,8 +609,11 @@ int main(int argc, char** argv) {
   }
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   ck(ixb_destroy(h), "ixb_destroy");
-  if (say)
-    std::printf(" pasos de tiempo=%d, iteraciones SIMPLE=%lld (limite alcanzado en %lld pasos), %.3f s\n", itera,
-                (long long)simple_total, (long long)limit_hits, secs);
+  // run summary (also under --quiet): time steps, SIMPLE iterations, the
+  // inner passes of the momentum / pressure-correction / energy loops, seconds
+  std::printf(" pasos de tiempo=%d, iteraciones SIMPLE=%lld (limite alcanzado en %lld pasos), "
+              "pases internos momento/presion/energia=%lld/%lld/%lld, %.3f s\n",
+              itera, (long long)simple_total, (long long)limit_hits, (long long)momen_total, (long long)pres_total,
+              (long long)ener_total, secs);
   return 0;
 }
