@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 #include "ixb_internal.h"
@@ -338,52 +339,63 @@ cudaError_t stream_solve(const R* a, const R* b, const R* c, const R* d, R* x, i
 
 // ---------------------------------------------------------------------------
 // Interleaved systems (row i of system s at i*nsys + s), hybrid solver.
-// A group of W adjacent systems occupies W*sizeof(R) = 128 contiguous bytes
-// of every row: whole 128-byte segments, the narrowest access that streams
-// from HBM at full rate (32-byte segments, 4 binary64 systems, stream at
-// under 40 % of it).  A thread-block cluster of Q CTAs (one per SM) solves
-// one group at a time, CTA q holding rows q*256 .. q*256+255 of all W
-// systems: thread t owns rows k*16 .. k*16+15 (k = t / W) of system
-// w = t % W.  Each group arrives as four 2-D tiles (a, b, c, d; box W x 256
-// rows, copied by the tensor engine without multicast) in shared memory
-// while the CTA is still solving the previous group from registers.  Every
-// thread eliminates its 16 rows (modified Thomas) to two rows coupled to the
-// neighbouring chunks.  The 32Q reduced rows of system w are solved in
-// cluster rank w % Q (its owner) by one warp (Thomas-PCR on 32 lanes): every
-// CTA stages its reduced rows in the owners' layout and sends each owner its
-// runs by bulk shared-to-shared copies that complete on the owner's mbarrier.
-// After a cluster barrier every thread reads its two solutions back and
-// back-substitutes into a solution tile that the tensor engine stores.  The
-// reduced rows are double-buffered across groups.  Every wait on a copy is
-// bounded (g_tri_timeout, as above).
+// A group of W adjacent systems occupies SEG = W*sizeof(R) contiguous bytes
+// of every row: 128-byte segments stream from HBM at full rate, 64-byte ones
+// a little below it and 32-byte ones (4 binary64 systems) at under 40 % of
+// it.  A thread-block cluster of Q CTAs (one per SM) solves one group at a
+// time, CTA q holding rows q*ROWS .. q*ROWS+ROWS-1 of all W systems: thread
+// t owns rows k*16 .. k*16+15 (k = t / W) of system w = t % W.  Each group
+// arrives as four tiles (a, b, c, d; boxes of W x 256 rows, copied by the
+// tensor engine without multicast) in shared memory while the CTA is still
+// solving the previous group from registers.  Every thread eliminates its
+// 16 rows (modified Thomas) to two rows coupled to the neighbouring chunks.
+// The reduced rows of system w are solved in cluster rank w % Q (its owner)
+// by one warp (Thomas-PCR on 32 lanes): every CTA stages its reduced rows in
+// the owners' layout and sends each owner its runs by bulk shared-to-shared
+// copies that complete on the owner's mbarrier.  After a cluster barrier
+// every thread reads its two solutions back and back-substitutes into a
+// solution tile that the tensor engine stores.  The reduced rows are
+// double-buffered across groups.  Every wait on a copy is bounded
+// (g_tri_timeout, as above).  (SEG, ROWS) = (128, 256) for lines of up to
+// 2048 rows; (64, 512) above, which halves W and so the cluster size that
+// holds a 4096-row group (8 instead of 16 CTAs: more clusters fit the GPU).
 // ---------------------------------------------------------------------------
 namespace {
 
 namespace cg = cooperative_groups;
 
-constexpr int kStrRows = 256;            // rows per CTA (one 2-D tile box)
-constexpr int kStrM = 16;                // rows per thread
-constexpr int kStrC = kStrRows / kStrM;  // chunks per CTA per system
+constexpr int kStrM = 16;    // rows per thread
+constexpr int kStrBox = 256;  // rows per 2-D tile box (the tensor-copy limit)
 
-template <class R>
+// A configuration: SEG bytes of every row per group (W = SEG / sizeof(R)
+// systems) and ROWS rows per CTA, so that a cluster of Q CTAs covers
+// Q * ROWS rows.  (128, 256): W = 16 / 32, clusters of up to 16 CTAs;
+// (64, 512): W = 8 / 16, clusters of up to 8 (n <= 4096 in both).
+template <class R, int SEG, int ROWS>
 struct StridedCfg {
-  static constexpr int W = 128 / (int)sizeof(R);  // systems per group: 16 (binary64) or 32 (binary32)
-  static constexpr int T = W * kStrC;             // threads per CTA: 256 or 512
-  static constexpr int TILE = W * kStrRows;       // elements per tile
+  static constexpr int W = SEG / (int)sizeof(R);  // systems per group
+  static constexpr int C = ROWS / kStrM;          // chunks per CTA per system
+  static constexpr int T = W * C;                 // threads per CTA
+  static constexpr int TILE = W * ROWS;           // elements per tile
+  static constexpr int BOXES = ROWS / kStrBox;    // tile boxes per array
+  // The 2*C*Q reduced rows of a system are 32 lane chunks of m = C*Q/16
+  // rows, at pitch m + 2 (even, so that a chunk's two reduced rows are one
+  // aligned pair).  The owner of a system solves m rows per lane, so m is
+  // 4, 8 or 16 (warp_unit_solve): Q <= QMAX.
+  static constexpr int QMAX = (256 / C < W ? 256 / C : W) < 16 ? (256 / C < W ? 256 / C : W) : 16;
   // one set of gathered reduced rows: a | c | d of the W / Q owned systems,
-  // 32 lane chunks of Q rows at pitch Q + 2 each (even, so that a chunk's
-  // two reduced rows are one aligned pair): at most 48 W rows (Q = 4)
-  static constexpr int SETA = 48 * W;
-  // a CTA's rows for one owned system of one owner are one run of
-  // (32 / Q) lane chunks: at most 48 elements (Q = 4); W runs per array
-  static constexpr int RUN = 48;
+  // W * (2C + 64 / Q) elements per array, at most W * (2C + 16) (Q = 4)
+  static constexpr int SETA = W * (2 * C + 16);
+  // a CTA's rows for one owned system of one owner are one run of (32 / Q)
+  // lane chunks: 2C + 64 / Q elements, at most 2C + 16 (Q = 4); W runs per array
+  static constexpr int RUN = 2 * C + 16;
 };
 
 // shared memory (bytes): 4 input tiles, the solution tile, 2 sets of
 // gathered reduced rows, the outgoing runs, 3 mbarriers (tiles, 2 sets)
-template <class R>
+template <class R, int SEG, int ROWS>
 __host__ __device__ constexpr size_t strided_smem_bytes() {
-  using SC = StridedCfg<R>;
+  using SC = StridedCfg<R, SEG, ROWS>;
   return ((size_t)5 * SC::TILE + 2 * 3 * (size_t)SC::SETA + 3 * (size_t)SC::W * SC::RUN) * sizeof(R) + 32;
 }
 
@@ -511,14 +523,14 @@ struct Pair2<double> { using type = double2; };
 template <>
 struct Pair2<float> { using type = float2; };
 
-template <class R>
-__global__ void __launch_bounds__(StridedCfg<R>::T, 1)
+template <class R, int SEG, int ROWS>
+__global__ void __launch_bounds__(StridedCfg<R, SEG, ROWS>::T, 1)
     tri_strided_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                        const __grid_constant__ CUtensorMap mapC, const __grid_constant__ CUtensorMap mapD,
                        const __grid_constant__ CUtensorMap mapX, int n, int nsys) {
-  using SC = StridedCfg<R>;
+  using SC = StridedCfg<R, SEG, ROWS>;
   using P2 = typename Pair2<R>::type;
-  constexpr int W = SC::W, T = SC::T, M = kStrM;
+  constexpr int W = SC::W, T = SC::T, M = kStrM, CH = SC::C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);  // a | b | c | d, [row][system] each
   R* xt = tile + 4 * SC::TILE;               // solution tile
@@ -527,36 +539,41 @@ __global__ void __launch_bounds__(StridedCfg<R>::T, 1)
   uint64_t* bar = reinterpret_cast<uint64_t*>(outr + 3 * W * SC::RUN);  // tiles
   uint64_t* rbar = bar + 1;                                            // reduced rows of set 0, 1
   cg::cluster_group cluster = cg::this_cluster();
-  const int Q = (int)cluster.num_blocks();  // 4, 8 or 16
+  const int Q = (int)cluster.num_blocks();  // 4 .. SC::QMAX, a power of two
   const int rank = (int)cluster.block_rank();
   const int S = W / Q;                       // systems each CTA owns
-  const int pitch = Q + 2;                   // lane chunks of Q reduced rows, padded
+  const int m = CH * Q / 16;                 // reduced rows per lane chunk: 4, 8 or 16
+  const int pitch = m + 2;                   // lane chunks of m reduced rows, padded
   const int sysP = 32 * pitch;               // one owned system in a set array
   const int run = (32 / Q) * pitch;          // this CTA's part of one owned system
   const int tid = threadIdx.x;
   const int w = tid % W, k = tid / W;
   const int owner = w % Q, slot = w / Q;  // system w's reduced rows: rank `owner`, slot `slot`
-  const int row0 = rank * kStrRows + k * M;
+  const int row0 = rank * ROWS + k * M;
   const int nclusters = gridDim.x / Q;
   const int cl = blockIdx.x / Q;
   const int ngroups = (nsys + W - 1) / W;
-  const bool stores = rank * kStrRows < n;  // CTAs wholly past the last row store nothing
+  const bool stores = rank * ROWS < n;  // CTAs wholly past the last row store nothing
   // this chunk's reduced rows 2i, 2i+1 (i = rank*C + k): their pair in the
-  // run for system w and in the owner's set (Q and 2i are even: one lane
+  // run for system w and in the owner's set (m and 2i are even: one lane
   // chunk, even position)
-  const int i2 = 2 * (rank * kStrC + k);
-  const int q_run = ((2 * k) / Q) * pitch + (2 * k) % Q;
-  const int p_e = slot * sysP + (i2 / Q) * pitch + i2 % Q;
+  const int i2 = 2 * (rank * CH + k);
+  const int q_run = ((2 * k) / m) * pitch + (2 * k) % m;
+  const int p_e = slot * sysP + (i2 / m) * pitch + i2 % m;
   // bytes an owner receives per group: Q senders x S systems x 3 arrays x run
   const unsigned recv_bytes = (unsigned)(3 * W * run * sizeof(R));
   constexpr unsigned kTileBytes = (unsigned)(SC::TILE * sizeof(R));
   auto issue = [&](int g) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of the tiles precede the copies
     mbar_expect_tx(bar, 4 * kTileBytes);
-    tile_load_2d(tile, &mapA, g * W, rank * kStrRows, bar);
-    tile_load_2d(tile + SC::TILE, &mapB, g * W, rank * kStrRows, bar);
-    tile_load_2d(tile + 2 * SC::TILE, &mapC, g * W, rank * kStrRows, bar);
-    tile_load_2d(tile + 3 * SC::TILE, &mapD, g * W, rank * kStrRows, bar);
+#pragma unroll
+    for (int bx = 0; bx < SC::BOXES; ++bx) {
+      const int y = rank * ROWS + bx * kStrBox, o = bx * kStrBox * W;
+      tile_load_2d(tile + o, &mapA, g * W, y, bar);
+      tile_load_2d(tile + SC::TILE + o, &mapB, g * W, y, bar);
+      tile_load_2d(tile + 2 * SC::TILE + o, &mapC, g * W, y, bar);
+      tile_load_2d(tile + 3 * SC::TILE + o, &mapD, g * W, y, bar);
+    }
   };
   if (tid == 0) {
     mbar_init(bar);
@@ -660,7 +677,7 @@ __global__ void __launch_bounds__(StridedCfg<R>::T, 1)
         R* sa = scr + o;
         R* sc = scr + SC::SETA + o;
         R* sd = scr + 2 * SC::SETA + o;
-        switch (Q) {
+        switch (m) {
           case 4: warp_unit_solve<R, 4>(A, Cc, D, sa, sc, sd, pitch); break;
           case 8: warp_unit_solve<R, 8>(A, Cc, D, sa, sc, sd, pitch); break;
           default: warp_unit_solve<R, 16>(A, Cc, D, sa, sc, sd, pitch); break;
@@ -677,7 +694,11 @@ __global__ void __launch_bounds__(StridedCfg<R>::T, 1)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor engine
     __syncthreads();
     // rows past n and systems past nsys fall outside the map and are not written
-    if (tid == 0 && !failed && stores) tile_store_2d(&mapX, g * W, rank * kStrRows, xt);
+    if (tid == 0 && !failed && stores) {
+#pragma unroll
+      for (int bx = 0; bx < SC::BOXES; ++bx)
+        if (rank * ROWS + bx * kStrBox < n) tile_store_2d(&mapX, g * W, rank * ROWS + bx * kStrBox, xt + bx * kStrBox * W);
+    }
   }
   if (tid == 0) {
     if (failed) {
@@ -709,15 +730,15 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// [n rows][nsys systems] in tiles of W systems x 256 rows; rows and systems
+// [n rows][nsys systems] in boxes of W systems x 256 rows; rows and systems
 // past the ends read as zeros and are not written
 template <class R>
-bool strided_map(CUtensorMap* map, const R* p, int n, int nsys) {
+bool strided_map(CUtensorMap* map, const R* p, int n, int nsys, int W) {
   const EncodeTiledFn fn = encode_tiled();
   if (!fn) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)nsys, (cuuint64_t)n};
   const cuuint64_t strides[1] = {(cuuint64_t)nsys * sizeof(R)};
-  const cuuint32_t box[2] = {(cuuint32_t)StridedCfg<R>::W, (cuuint32_t)kStrRows};
+  const cuuint32_t box[2] = {(cuuint32_t)W, (cuuint32_t)kStrBox};
   const cuuint32_t estr[2] = {1, 1};
   const CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   return fn(map, dt, 2, const_cast<R*>(p), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -725,24 +746,21 @@ bool strided_map(CUtensorMap* map, const R* p, int n, int nsys) {
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// cudaErrorInvalidValue: outside the kernel's range (n > 16*256 rows, a row
-// pitch or base address the tensor copies cannot take, or no room for a
-// cluster of Q CTAs); the caller then uses the general interleaved kernel
-template <class R>
-cudaError_t strided_solve(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
-  using SC = StridedCfg<R>;
-  if (n < 1 || n > 16 * kStrRows || nsys < 1) return cudaErrorInvalidValue;
-  const uintptr_t all = (uintptr_t)a | (uintptr_t)b | (uintptr_t)c | (uintptr_t)d | (uintptr_t)x;
-  if ((all & 15) != 0 || ((size_t)nsys * sizeof(R)) % 16 != 0) return cudaErrorInvalidValue;
+// cudaErrorInvalidValue: outside the configuration's range (n above
+// QMAX * ROWS rows, or no room for a cluster of Q CTAs)
+template <class R, int SEG, int ROWS>
+cudaError_t strided_launch(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
+  using SC = StridedCfg<R, SEG, ROWS>;
   int Q = 4;  // CTAs per cluster: a power of two >= 4 (W / Q systems of 32 lane chunks on each owner)
-  while (Q * kStrRows < n) Q <<= 1;
+  while (Q * ROWS < n) Q <<= 1;
+  if (Q > SC::QMAX) return cudaErrorInvalidValue;
   CUtensorMap maps[5];
-  if (!strided_map(&maps[0], a, n, nsys) || !strided_map(&maps[1], b, n, nsys) ||
-      !strided_map(&maps[2], c, n, nsys) || !strided_map(&maps[3], d, n, nsys) ||
-      !strided_map(&maps[4], static_cast<const R*>(x), n, nsys))
+  if (!strided_map(&maps[0], a, n, nsys, SC::W) || !strided_map(&maps[1], b, n, nsys, SC::W) ||
+      !strided_map(&maps[2], c, n, nsys, SC::W) || !strided_map(&maps[3], d, n, nsys, SC::W) ||
+      !strided_map(&maps[4], static_cast<const R*>(x), n, nsys, SC::W))
     return cudaErrorInvalidValue;
-  auto k = tri_strided_kernel<R>;
-  const size_t smem = strided_smem_bytes<R>();
+  auto k = tri_strided_kernel<R, SEG, ROWS>;
+  const size_t smem = strided_smem_bytes<R, SEG, ROWS>();
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if (Q > 8 && (e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
@@ -769,6 +787,34 @@ cudaError_t strided_solve(const R* a, const R* b, const R* c, const R* d, R* x, 
   e = cudaLaunchKernelEx(&cfg, k, maps[0], maps[1], maps[2], maps[3], maps[4], n, nsys);
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
+}
+
+// IXB_STRIDED_SEG=64 or 128 forces one configuration; otherwise lines of
+// more than 2048 rows use 64-byte segments with 512-row CTAs (clusters of
+// 8 instead of 16, so more of them fit the GPU at once), shorter lines
+// 128-byte segments with 256-row CTAs (less padding).
+int strided_seg_choice() {
+  static const int v = [] {
+    const char* e = std::getenv("IXB_STRIDED_SEG");
+    return e ? std::atoi(e) : 0;
+  }();
+  return v;
+}
+
+// cudaErrorInvalidValue: outside the kernels' range (n > 4096 rows, a row
+// pitch or base address the tensor copies cannot take, or no room for a
+// cluster); the caller then uses the general interleaved kernel
+template <class R>
+cudaError_t strided_solve(const R* a, const R* b, const R* c, const R* d, R* x, int n, int nsys, cudaStream_t st) {
+  if (n < 1 || n > 16 * kStrBox || nsys < 1) return cudaErrorInvalidValue;
+  const uintptr_t all = (uintptr_t)a | (uintptr_t)b | (uintptr_t)c | (uintptr_t)d | (uintptr_t)x;
+  if ((all & 15) != 0 || ((size_t)nsys * sizeof(R)) % 16 != 0) return cudaErrorInvalidValue;
+  const int seg = strided_seg_choice();
+  if (seg == 64 || (seg != 128 && n > 8 * kStrBox)) {
+    const cudaError_t e = strided_launch<R, 64, 512>(a, b, c, d, x, n, nsys, st);
+    if (e != cudaErrorInvalidValue) return e;
+  }
+  return strided_launch<R, 128, 256>(a, b, c, d, x, n, nsys, st);
 }
 
 }  // namespace

@@ -183,6 +183,47 @@ def test_two_kernel_form_keeps_parity():
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]
 
 
+_STRIDED_CHILD = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np
+import torch
+from ixchel2d_b200 import _ffi as F
+from oracle import oracle as O
+from tests.conftest import relerr
+for n, nsys in ((5, 16), (48, 64), (300, 48), (700, 64), (1025, 36), (2048, 128), (2049, 16), (3000, 100),
+                (4096, 512)):
+    rng = np.random.default_rng(n + 3 * nsys)
+    a = rng.uniform(-1, 0, (nsys, n)); c = rng.uniform(-1, 0, (nsys, n))
+    b = np.abs(a) + np.abs(c) + rng.uniform(0.1, 1, (nsys, n)); d = rng.uniform(-1, 1, (nsys, n))
+    ref = O.tridiagonal_batch(a, b, c, d)
+    for tdt, fn, tol in ((torch.float64, F.lib.ixb_tridiag_f64, 1e-12), (torch.float32, F.lib.ixb_tridiag_f32, 2e-5)):
+        A, B, Cc, D = (torch.tensor(np.ascontiguousarray(v.T), dtype=tdt, device="cuda") for v in (a, b, c, d))
+        X = torch.full_like(D, float("nan"))
+        st = fn(A.data_ptr(), B.data_ptr(), Cc.data_ptr(), D.data_ptr(), X.data_ptr(), n, nsys, 1, F.SOLVER_HYBRID,
+                torch.cuda.current_stream().cuda_stream)
+        assert st == F.OK, (n, nsys, st)
+        torch.cuda.synchronize()
+        e = relerr(X.cpu().numpy().astype(np.float64).T, ref)
+        assert e < tol, (n, nsys, str(tdt), e)
+        assert F.lib.ixb_tridiag_status() == F.OK, (n, nsys)
+print("ok")
+"""
+
+
+@pytest.mark.parametrize("seg", ["64", "128"])
+def test_strided_configurations_keep_parity(seg):
+    # IXB_STRIDED_SEG (read once per process) forces one interleaved cluster
+    # configuration for every size: 64-byte segments with 512-row CTAs, or
+    # 128-byte segments with 256-row CTAs; every row is written (X starts as NaN)
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _STRIDED_CHILD, root], env={**os.environ, "IXB_STRIDED_SEG": seg},
+                       capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]
+
+
 def test_autotune_then_parity():
     case = cases.natural_cavity(40, 36, Ra=1e5)
     g, o = _pair(case)
