@@ -169,7 +169,8 @@ int ixb_phase(ixb_handle* h, int which);
 int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
 /* Launch shape of one sweep (0..7 = u-y, u-x, v-y, v-x, p'-y, p'-x, T-y,
  * T-x): lines per CTA and threads per line, one of (1,128) (1,256) (1,512)
- * (2,64) (2,128) (4,32) (4,64) (8,32) (16,16); each thread eliminates a chunk of
+ * (2,64) (2,128) (4,32) (4,64) (4,128) (8,32) (8,64) (8,128) (16,16)
+ * (16,32); each thread eliminates a chunk of
  * max(3, ceil(n/threads_per_line)) rows.  lines_per_cta = 0 restores the
  * default (the fewest waves of resident CTAs, then the shortest chunks).
  * No reference counterpart: the reference runs one sequential tridiagonal
