@@ -83,8 +83,8 @@ int ensure_tables(ixb_handle* h) {
 
 
 // Default launch shape of a sweep: the fewest waves of CTAs (every CTA
-// resident at once when possible), then the shortest chunks, then the
-// larger CTA.
+// resident at once when possible), then the shortest chunks, then the most
+// SMs busy (CTAs up to the SM count), then the larger CTA.
 void pick_shape(ixb_handle* h, int eq) {
   int best = -1;
   long long best_key = 0;
@@ -93,7 +93,8 @@ void pick_shape(ixb_handle* h, int eq) {
     const int occ = sweep_occupancy(eq, solver_form(h), s);
     if (occ <= 0) continue;
     const long long waves = (s.grid + (long long)occ * h->nsm - 1) / ((long long)occ * h->nsm);
-    const long long key = waves * 1000000LL + (long long)s.m * 1000 + (256 - s.nt);
+    const long long busy = std::min<long long>(s.grid, h->nsm);
+    const long long key = waves * 1000000000LL + (long long)s.m * 1000000 + (h->nsm - busy) * 1000 + (1024 - s.nt);
     if (best < 0 || key < best_key) { best = k; best_key = key; }
   }
   if (best < 0) best = 1;
