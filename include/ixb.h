@@ -259,6 +259,18 @@ int ixb_tridiag_f64_noalloc(const double* a, const double* b, const double* c, c
 int ixb_energy_iterations(ixb_handle* h, int n);
 int ixb_adjoint_energy(ixb_handle* h, int K, int j0, int j1, double* grad);
 int ixb_set_bc_values(ixb_handle* h, int var, int side, const double* values);
+/* The same gradient through K outer SIMPLE iterations (ixb_simple_iterations
+ * from the current state) whose flow evolves but does not depend on the
+ * temperature: Ri = Riy = 0 (forced convection), else IXB_EINVAL.  Then T
+ * after K iterations is a composition of affine T passes, those of iteration
+ * k with the coefficients of that iteration's velocities, and the gradient is
+ * exact.  The call runs the K iterations, checkpointing the seven state
+ * fields every C iterations (device memory for K/C + 1 checkpoints and C
+ * velocity pairs), then reverses them segment by segment, recomputing each
+ * segment from its checkpoint; it leaves the state after the K iterations
+ * and, if nu0 is not NULL, stores nu0 of ixb_nusselt_x(h, j0, j1) there.
+ * Binary64 form (IXB_PREC_FP64) for the exact gradient. */
+int ixb_adjoint_energy_coupled(ixb_handle* h, int K, int C, int j0, int j1, double* grad, double* nu0);
 
 /* ---- batched cavities: many instances, one launch per phase ----
  * No counterpart in the reference, which runs one case per process.  A

@@ -340,6 +340,15 @@ module ixb
        real(c_double), intent(out) :: grad(*)
      end function ixb_adjoint_energy
 
+     integer(c_int) function ixb_adjoint_energy_coupled(h, K, C, j0, j1, grad, nu0) &
+          bind(C, name="ixb_adjoint_energy_coupled")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: K, C, j0, j1
+       real(c_double), intent(out) :: grad(*)
+       real(c_double), intent(out) :: nu0
+     end function ixb_adjoint_energy_coupled
+
      integer(c_int) function ixb_set_bc_values(h, var, side, values) bind(C, name="ixb_set_bc_values")
        import :: c_int, c_ptr, c_double
        type(c_ptr), value :: h

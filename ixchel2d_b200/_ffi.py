@@ -102,6 +102,7 @@ SIGNATURES = [
     ("ixb_batch_report", C.c_int, [_vp, C.c_int, C.POINTER(Report)]),
     ("ixb_energy_iterations", C.c_int, [_vp, C.c_int]),
     ("ixb_adjoint_energy", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp]),
+    ("ixb_adjoint_energy_coupled", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),
     ("ixb_set_bc_values", C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     ("ixb_mesh_axis", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _vp]),
     ("ixb_staggered_mesh", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,

@@ -170,6 +170,16 @@ class Simple2D:
         F.check(F.lib.ixb_adjoint_energy(self.h, K, j0, j1, F.dptr(g)), "ixb_adjoint_energy")
         return g
 
+    def adjoint_energy_coupled(self, K: int, ckpt: int, j0: int, j1: int):
+        """(grad, nu0) after K outer iterations from the current state, for a flow that does not depend on T
+        (Ri = Riy = 0): grad[jj-1] = d nu0 / d (side-a value of T x-line jj); checkpoints every ckpt iterations.
+        Leaves the state after the K iterations."""
+        g = np.zeros(self.nj + 1)
+        nu = C.c_double()
+        F.check(F.lib.ixb_adjoint_energy_coupled(self.h, K, ckpt, j0, j1, F.dptr(g), C.byref(nu)),
+                "ixb_adjoint_energy_coupled")
+        return g, nu.value
+
     def set_bc_values(self, var: int, side: int, values):
         v = np.ascontiguousarray(values, dtype=np.float64)
         F.check(F.lib.ixb_set_bc_values(self.h, var, side, F.dptr(v)), "ixb_set_bc_values")

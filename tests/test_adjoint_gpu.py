@@ -75,3 +75,89 @@ def test_adjoint_leaves_the_state_unchanged_and_torch_wrapper():
     nu.backward()
     assert np.allclose(theta.grad.numpy(), J.gradient(np.ones(8)))
     assert abs(nu.item() - J.value(np.ones(8))) < 1e-12
+
+
+# ---------------------------------------------------------------------------
+# energy adjoint through K outer iterations of an evolving flow that does not
+# depend on T (Ri = Riy = 0), with checkpoints every C iterations
+# ---------------------------------------------------------------------------
+MI_F, NJ_F = 40, 32
+
+
+def _forced_case():
+    """Lid-driven forced convection (mixed mode, Ri = 0): lid u = 1 on side d,
+    no-slip elsewhere; T = profile on side a, T = 0 on side c, sides b and d
+    adiabatic; zero flow and T = 0.5 to start.  The T loop runs 1 to 5
+    passes per outer iteration (conv_t = 1e-4, iter_ecuaci_max = 3)."""
+    xu, yv, xp, yp = cases.staggered_mesh(MI_F, NJ_F)
+    prm = cases.default_params(**cases.nondim("mixta", 100.0, 0.71, 0.0))
+    prm.update(conv_t=1e-4, iter_ecuaci_max=3)
+    z = [(cases.ALL, F.BC_DIRI, 0.0)]
+    bc = {0: cases.bc_table((xu, yp), {0: z, 1: z, 2: z, 3: [(cases.ALL, F.BC_DIRI, 1.0)]}),
+          1: cases.bc_table((xp, yv), {0: z, 1: z, 2: z, 3: z}),
+          2: cases.bc_table((xp, yp), {0: [(cases.ALL, F.BC_DIRI, 1.0)], 1: [(cases.ALL, F.BC_NEUM, 0.0)],
+                                       2: [(cases.ALL, F.BC_DIRI, 0.0)], 3: [(cases.ALL, F.BC_NEUM, 0.0)]})}
+    return cases.Case(MI_F, NJ_F, xu, yv, xp, yp, prm, bc, cases.zero_state(MI_F, NJ_F, 0.5))
+
+
+def _profile():
+    jj = np.arange(NJ_F + 1)
+    return 1.0 + 0.05 * np.sin(0.7 * jj)
+
+
+def _forward(case, values, K, j0, j1):
+    sim = Simple2D.from_case(case)
+    sim.set_bc_values(2, 0, values)
+    sim.iterations(K)
+    nu = sim.nusselt_x(j0, j1)[0]
+    st = sim.download()
+    sim.close()
+    return nu, st
+
+
+def test_coupled_adjoint_matches_central_differences():
+    case = _forced_case()
+    K, j0, j1 = 60, 2, NJ_F - 2
+    vals = _profile()
+    sim = Simple2D.from_case(case)
+    sim.set_bc_values(2, 0, vals)
+    g, nu = sim.adjoint_energy_coupled(K, 16, j0, j1)
+    end = sim.download()
+    sim.close()
+    # the call leaves the state and objective of a plain K-iteration run
+    nu_ref, st_ref = _forward(case, vals, K, j0, j1)
+    assert abs(nu - nu_ref) <= 1e-13 * abs(nu_ref), (nu, nu_ref)
+    for k in ("u", "v", "p", "T"):
+        assert np.max(np.abs(end[k] - st_ref[k])) <= 1e-13 * max(np.max(np.abs(st_ref[k])), 1e-300), k
+    # the flow does not depend on T, so nu is affine in the wall values:
+    # central differences with a large step are exact
+    H = 1e-2
+    for L in (3, NJ_F // 2, NJ_F - 3, NJ_F - 1):
+        e = np.zeros(NJ_F + 1)
+        e[L - 1] = H
+        fd = (_forward(case, vals + e, K, j0, j1)[0] - _forward(case, vals - e, K, j0, j1)[0]) / (2 * H)
+        assert abs(g[L - 1] - fd) <= 1e-8 * max(abs(fd), 1e-3), (L, g[L - 1], fd)
+    assert np.max(np.abs(g)) > 1e-3
+
+
+def test_coupled_adjoint_is_independent_of_the_checkpoint_interval():
+    case = _forced_case()
+    K, j0, j1 = 45, 2, NJ_F - 2
+    out = []
+    for ckpt in (1, 16, 45):
+        sim = Simple2D.from_case(case)
+        sim.set_bc_values(2, 0, _profile())
+        out.append(sim.adjoint_energy_coupled(K, ckpt, j0, j1))
+        sim.close()
+    for g, nu in out[1:]:
+        assert np.array_equal(g, out[0][0]) and nu == out[0][1]
+
+
+def test_coupled_adjoint_refuses_buoyant_flow():
+    case = cases.natural_cavity(24, 24, Ra=1e4, T0=0.5)  # Riy = -1: the flow depends on T
+    sim = Simple2D.from_case(case)
+    with pytest.raises(Exception):
+        sim.adjoint_energy_coupled(10, 5, 2, 20)
+    g = np.zeros(25)
+    assert F.lib.ixb_adjoint_energy_coupled(sim.h, 10, 5, 2, 20, F.dptr(g), None) == F.EINVAL
+    sim.close()
