@@ -461,6 +461,49 @@ def adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, warm=500, fd_nodes=8):
             "linearity_rel_err": float(abs(dj - g @ d) / abs(dj))}
 
 
+def coupled_adjoint_bench(n=256, Re=100.0, nodes=128, K=500, C=50, fd_nodes=8):
+    """Energy adjoint through K outer SIMPLE iterations of an evolving flow
+    that does not depend on T, with checkpoints every C iterations:
+    lid-driven forced convection n x n (Re, Ri = 0), from zero flow and
+    T = 0.5; hot-wall profile of `nodes` piecewise-linear nodes, value
+    1 + U(-0.05, 0.05) (seed 1234); objective the hot-wall Nusselt number
+    after the K iterations.  The T loop runs up to 5 passes per iteration
+    (conv_t = 1e-4, iter_ecuaci_max = 3).  Gradient against central
+    differences of the same GPU forward on fd_nodes nodes, h = 1e-6 and
+    h = 1e-2 (the objective is affine in the nodes: exact for any step)."""
+    from ixchel2d_b200 import Simple2D, cases
+    from ixchel2d_b200.adjoint import HotWallNusseltCoupled
+    case = cases.lid_driven_forced(n, n, Re=Re, conv_t=1e-4, iter_ecuaci_max=3)
+    sim = Simple2D.from_case(case)
+    J = HotWallNusseltCoupled(sim, case.state, case.yp, nodes, K, 2, n - 2, ckpt=C)
+    rng = np.random.default_rng(1234)
+    theta = 1.0 + rng.uniform(-0.05, 0.05, nodes)
+    J.gradient(theta)  # warm
+    t0 = time.perf_counter()
+    g = J.gradient(theta)
+    t_adj = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    nu = J.value(theta)
+    t_fwd = time.perf_counter() - t0
+    pick = np.linspace(0, nodes - 1, fd_nodes).astype(int)
+    fds = {}
+    for h in (1e-6, 1e-2):
+        fd = np.zeros(fd_nodes)
+        for q, k in enumerate(pick):
+            e = np.zeros(nodes)
+            e[k] = h
+            fd[q] = (J.value(theta + e) - J.value(theta - e)) / (2 * h)
+        fds[h] = fd
+    sim.close()
+    rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+    return {"case": case.name, "flow": "evolving over the K iterations from rest (Ri = Riy = 0)",
+            "nodes": nodes, "K": K, "C": C, "nu_hot_wall": nu, "adjoint_s": t_adj, "forward_s": t_fwd,
+            "fd_all_nodes_s_estimate": 2 * nodes * t_fwd, "fd_nodes_checked": fd_nodes,
+            "max_rel_err_vs_fd": rel(g[pick], fds[1e-6]),
+            "normwise_rel_err_vs_fd": float(np.linalg.norm(g[pick] - fds[1e-6]) / np.linalg.norm(fds[1e-6])),
+            "max_rel_err_vs_fd_h1e-2": rel(g[pick], fds[1e-2])}
+
+
 def make_sim(case, prec, stream, shapes):
     from ixchel2d_b200 import Simple2D
     sim = Simple2D.from_case(case, prec=prec)
@@ -575,6 +618,7 @@ def run_ours(args):
     batched = batched_bench(stream)
     # ---- energy adjoint (flow held fixed) ----
     adjoint = adjoint_bench()
+    adjoint_coupled = coupled_adjoint_bench()
 
     cells = case.cells
     dom = int(np.argmax(phase_ms))
@@ -613,6 +657,7 @@ def run_ours(args):
             "adi_line_solve": adi,
             "batched_cavities": batched,
             "energy_adjoint": adjoint,
+            "energy_adjoint_coupled": adjoint_coupled,
             "sweep_shapes": {n: {SWEEPS[int(k)]: list(v[:2]) for k, v in sh.items()} for n, sh in shapes.items()},
             "iteration_alg_bytes": iter_bytes,
             "cpu_baseline": None if cpu_val is None else {

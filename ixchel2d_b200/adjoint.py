@@ -1,8 +1,10 @@
 """Gradient of the hot-wall Nusselt number with respect to a piecewise-linear
-hot-wall temperature profile, with the flow held fixed: a thin
-torch.autograd.Function over ixb_energy_iterations (forward) and
-ixb_adjoint_energy (backward), used to check the adjoint against finite
-differences."""
+hot-wall temperature profile: with the flow held fixed (HotWallNusselt, over
+ixb_energy_iterations and ixb_adjoint_energy), or through K outer SIMPLE
+iterations of a flow that does not depend on T (HotWallNusseltCoupled, over
+ixb_simple_iterations and ixb_adjoint_energy_coupled).  as_torch() wraps
+either in a thin torch.autograd.Function, used to check the adjoint against
+finite differences."""
 from __future__ import annotations
 
 import numpy as np
@@ -62,3 +64,28 @@ class HotWallNusselt:
                 return g * torch.tensor(grad, dtype=theta.dtype, device=theta.device)
 
         return _Fn.apply
+
+
+class HotWallNusseltCoupled(HotWallNusselt):
+    """J(theta) = nu0 of ixb_nusselt_x(j0, j1) after K outer SIMPLE
+    iterations from `state` (the flow evolves with them but does not depend
+    on T: Ri = Riy = 0), with the side-a T boundary values set to P theta.
+    The gradient comes from ixb_adjoint_energy_coupled with checkpoints every
+    `ckpt` iterations."""
+
+    def __init__(self, sim: Simple2D, state: dict, yp: np.ndarray, nodes: int, K: int, j0: int, j1: int,
+                 ckpt: int = 50):
+        super().__init__(sim, state, yp, nodes, K, j0, j1)
+        self.ckpt = ckpt
+
+    def value(self, theta: np.ndarray) -> float:
+        self.sim.set_bc_values(F.VAR_T, 0, self.P @ np.asarray(theta, dtype=np.float64))
+        self.sim.upload(self.state)
+        self.sim.iterations(self.K)
+        return self.sim.nusselt_x(self.j0, self.j1)[0]
+
+    def gradient(self, theta: np.ndarray) -> np.ndarray:
+        self.sim.set_bc_values(F.VAR_T, 0, self.P @ np.asarray(theta, dtype=np.float64))
+        self.sim.upload(self.state)
+        g, _ = self.sim.adjoint_energy_coupled(self.K, self.ckpt, self.j0, self.j1)
+        return self.P.T @ g

@@ -213,3 +213,23 @@ def lid_driven_mixed(mi: int = 701, nj: int = 301, Re: float = 100.0, Ri: float 
                                3: [(ALL, BC_DIRI, 0.0)]}),
     }
     return Case(mi, nj, xu, yv, xp, yp, prm, bc, zero_state(mi, nj, 0.0), name=f"lid_driven_mixed_{mi}x{nj}_Re{Re:g}")
+
+
+def lid_driven_forced(mi: int = 256, nj: int = 256, Re: float = 100.0, Pr: float = 0.71, T0: float = 0.5,
+                      **param_kw) -> Case:
+    """Lid-driven forced convection ('mixta' with Ri = 0, so Ri = Riy = 0 and
+    the flow does not depend on T) on a uniform mesh: lid u = 1 on side d,
+    no-slip elsewhere; T = 1 on side a (the hot wall; per-line values by
+    ixb_set_bc_values), T = 0 on side c, sides b and d adiabatic; zero flow
+    and uniform T0 to start."""
+    xu, yv, xp, yp = staggered_mesh(mi, nj, "unif", "unif")
+    prm = default_params(**nondim("mixta", Re, Pr, 0.0))
+    prm.update(param_kw)
+    z = [(ALL, BC_DIRI, 0.0)]
+    bc = {
+        0: bc_table((xu, yp), {0: z, 1: z, 2: z, 3: [(ALL, BC_DIRI, 1.0)]}),
+        1: bc_table((xp, yv), {0: z, 1: z, 2: z, 3: z}),
+        2: bc_table((xp, yp), {0: [(ALL, BC_DIRI, 1.0)], 1: [(ALL, BC_NEUM, 0.0)], 2: [(ALL, BC_DIRI, 0.0)],
+                               3: [(ALL, BC_NEUM, 0.0)]}),
+    }
+    return Case(mi, nj, xu, yv, xp, yp, prm, bc, zero_state(mi, nj, T0), name=f"lid_driven_forced_{mi}x{nj}_Re{Re:g}")

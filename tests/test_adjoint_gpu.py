@@ -85,19 +85,9 @@ MI_F, NJ_F = 40, 32
 
 
 def _forced_case():
-    """Lid-driven forced convection (mixed mode, Ri = 0): lid u = 1 on side d,
-    no-slip elsewhere; T = profile on side a, T = 0 on side c, sides b and d
-    adiabatic; zero flow and T = 0.5 to start.  The T loop runs 1 to 5
+    """Lid-driven forced convection (Ri = Riy = 0); the T loop runs 1 to 5
     passes per outer iteration (conv_t = 1e-4, iter_ecuaci_max = 3)."""
-    xu, yv, xp, yp = cases.staggered_mesh(MI_F, NJ_F)
-    prm = cases.default_params(**cases.nondim("mixta", 100.0, 0.71, 0.0))
-    prm.update(conv_t=1e-4, iter_ecuaci_max=3)
-    z = [(cases.ALL, F.BC_DIRI, 0.0)]
-    bc = {0: cases.bc_table((xu, yp), {0: z, 1: z, 2: z, 3: [(cases.ALL, F.BC_DIRI, 1.0)]}),
-          1: cases.bc_table((xp, yv), {0: z, 1: z, 2: z, 3: z}),
-          2: cases.bc_table((xp, yp), {0: [(cases.ALL, F.BC_DIRI, 1.0)], 1: [(cases.ALL, F.BC_NEUM, 0.0)],
-                                       2: [(cases.ALL, F.BC_DIRI, 0.0)], 3: [(cases.ALL, F.BC_NEUM, 0.0)]})}
-    return cases.Case(MI_F, NJ_F, xu, yv, xp, yp, prm, bc, cases.zero_state(MI_F, NJ_F, 0.5))
+    return cases.lid_driven_forced(MI_F, NJ_F, Re=100.0, conv_t=1e-4, iter_ecuaci_max=3)
 
 
 def _profile():
@@ -160,4 +150,20 @@ def test_coupled_adjoint_refuses_buoyant_flow():
         sim.adjoint_energy_coupled(10, 5, 2, 20)
     g = np.zeros(25)
     assert F.lib.ixb_adjoint_energy_coupled(sim.h, 10, 5, 2, 20, F.dptr(g), None) == F.EINVAL
+    sim.close()
+
+
+def test_coupled_autograd_function_matches_adjoint():
+    import torch
+    from ixchel2d_b200.adjoint import HotWallNusseltCoupled
+    case = _forced_case()
+    sim = Simple2D.from_case(case)
+    nodes, K = 12, 30
+    J = HotWallNusseltCoupled(sim, case.state, case.yp, nodes, K, 2, NJ_F - 2, ckpt=8)
+    theta = torch.tensor(1.0 + 0.02 * np.cos(np.arange(nodes)), dtype=torch.float64, requires_grad=True)
+    y = J.as_torch()(theta)
+    y.backward()
+    g = J.gradient(theta.detach().numpy())
+    assert np.allclose(theta.grad.numpy(), g, rtol=0, atol=1e-14 * np.max(np.abs(g)))
+    assert float(y) == J.value(theta.detach().numpy())
     sim.close()
