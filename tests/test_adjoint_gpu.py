@@ -165,5 +165,5 @@ def test_coupled_autograd_function_matches_adjoint():
     y.backward()
     g = J.gradient(theta.detach().numpy())
     assert np.allclose(theta.grad.numpy(), g, rtol=0, atol=1e-14 * np.max(np.abs(g)))
-    assert float(y) == J.value(theta.detach().numpy())
+    assert float(y.detach()) == J.value(theta.detach().numpy())
     sim.close()
