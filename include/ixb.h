@@ -179,9 +179,10 @@ int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads
 /* Kernels one outer iteration launches with the current launch shapes (one
  * inner pass per loop): one per sweep whose shape runs assembly and line
  * solve as one kernel (x-sweeps with one line per CTA; y-sweeps with 4, 8 or
- * 16 lines per CTA), two per other sweep, plus the p' preset, the p/u/v
- * correction and the u residual.  IXB_SPLIT=1 in the environment keeps every
- * sweep at two kernels. */
+ * 16 lines per CTA), two per other sweep, plus the p/u/v correction and the
+ * u residual, and the p' reset when the loop is host-driven
+ * (IXB_NO_GRAPH=1) or IXB_DOWHILE=0.  IXB_SPLIT=1 in the environment keeps
+ * every sweep at two kernels. */
 int ixb_iteration_launches(ixb_handle* h, int* launches);
 /* Autotuner for the launch shapes: for every sweep, times each candidate
  * shape `reps` times on the current state (a scratch buffer of flush_bytes

@@ -142,12 +142,19 @@ SweepIO<double> sweep_io(ixb_handle* h, int eq, const double* prev, bool with_no
   return io;
 }
 
-// Launch one sweep reading field buffers `cur` and writing `cur^1`.
-int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm, const CtlRef& ctl = CtlRef{}) {
+// Launch one sweep reading field buffers `cur` and writing `cur^1`; with
+// zero_input the swept field is read as zeros (the handle's zero field),
+// whatever its current buffer holds.
+int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm, const CtlRef& ctl = CtlRef{},
+          bool zero_input = false) {
   Geo<double> G = make_geo(h);
   if (h->shape_tl[eq] == 0) pick_shape(h, eq);
   SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), h->shape_tl[eq], h->shape_g[eq]);
-  const SweepIO<double> io = sweep_io(h, eq, prev, with_norm);
+  SweepIO<double> io = sweep_io(h, eq, prev, with_norm);
+  if (zero_input) {
+    io.in = h->zero;
+    if (eq == EQ_PY || eq == EQ_PX) io.pc = h->zero;
+  }
   const StageBuf stage{h->stage, h->stage_stride, h->stage_P};
   CK(launch_sweep_f64(eq, solver_form(h), s, G, io, stage, h->stream, ctl));
   return IXB_OK;
@@ -376,11 +383,24 @@ int build_graph(ixb_handle* h) {
     return capture_into(h, b, nullptr, pass, &last);
   };
   TRY(inner_loop(nullptr, c_mom, mom_pass));
-  TRY(capture_into(h, outer_body, &wn, [&]() {
-    return launch_preset_f64(h->pc[h->cpc], h->fsz, CtlRef{h->ctl_d, nrm, c_pres, 0, 0}, h->stream) == cudaSuccess
-               ? IXB_OK : IXB_ECUDA;
-  }, &last));
-  TRY(inner_loop(&last, c_pres, pres_pass));
+  if (dw) {
+    // p' starts every pressure loop from zero (main.f90:752-758): the first
+    // pass's y-sweep reads the zero field and its norm compares with zero,
+    // so no reset kernel is needed; its exit test opens the WHILE node
+    TRY(capture_into(h, outer_body, &wn, [&]() -> int {
+      TRY(sweep(h, EQ_PY, nullptr, false, CtlRef{}, true));
+      TRY(sweep(h, EQ_PX, h->zero, true, CtlRef{h->ctl_d, nrm, c_pres, 0, 1}));
+      return IXB_OK;
+    }, &last));
+    TRY(add_while(h, outer_body, &last, c_pres, &b, &wn));
+    TRY(capture_into(h, b, nullptr, pres_pass, &last));
+  } else {
+    TRY(capture_into(h, outer_body, &wn, [&]() {
+      return launch_preset_f64(h->pc[h->cpc], h->fsz, CtlRef{h->ctl_d, nrm, c_pres, 0, 0}, h->stream) == cudaSuccess
+                 ? IXB_OK : IXB_ECUDA;
+    }, &last));
+    TRY(inner_loop(&last, c_pres, pres_pass));
+  }
   TRY(capture_into(h, outer_body, &wn, [&]() { return correct(h, CtlRef{h->ctl_d, nrm, c_ener, 0, 0}); }, &last));
   TRY(inner_loop(&last, c_ener, ener_pass));
   TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
@@ -926,7 +946,9 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms) {
 
 int ixb_iteration_launches(ixb_handle* h, int* launches) {
   if (!h || !launches) return IXB_EINVAL;
-  int k = 3;  // p' preset, p/u/v correction, u residual
+  // p/u/v correction, u residual, and the p' reset kernel unless the graph
+  // runs the inner loops in do-while form (whose first pressure pass reads zeros)
+  int k = (h->use_graph && do_while_loops()) ? 2 : 3;
   for (int eq = 0; eq < EQ_COUNT; ++eq) {
     if (h->shape_tl[eq] == 0) pick_shape(h, eq);
     k += (fused_enabled() && fused_shape(eq, h->shape_tl[eq], h->shape_g[eq])) ? 1 : 2;
