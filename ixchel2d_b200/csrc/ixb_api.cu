@@ -320,18 +320,21 @@ bool do_while_loops() {
   return v;
 }
 
-int build_graph(ixb_handle* h) {
-  if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
-  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+// The SIMPLE loop as one graph: a WHILE node over `unroll` outer passes.
+// unroll > 1 serves fixed counts that are multiples of it (every pass's
+// outer test counts; the last one of the body decides whether it repeats).
+int build_graph(ixb_handle* h, int unroll, cudaGraph_t* graph, cudaGraphExec_t* exec) {
+  if (*exec) { cudaGraphExecDestroy(*exec); *exec = nullptr; }
+  if (*graph) { cudaGraphDestroy(*graph); *graph = nullptr; }
   // the graph bakes buffer parity 0 into its kernel arguments
   const int cu = h->cu, cv = h->cv, cT = h->cT, cpc = h->cpc;
   h->cu = h->cv = h->cT = h->cpc = 0;
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
-  h->graph = g;
+  *graph = g;
   // a conditional handle belongs to the graph that holds its node: the
-  // outer handle to g, the three inner ones to the outer loop's body
-  cudaGraphConditionalHandle c_outer, c_mom, c_pres, c_ener;
+  // outer handle to g, the inner ones to the outer loop's body
+  cudaGraphConditionalHandle c_outer;
   CK(cudaGraphConditionalHandleCreate(&c_outer, g, 1, cudaGraphCondAssignDefault));
   cudaGraphNode_t n_begin, n_outer;
   TRY(capture_into(h, g, nullptr, [&]() {
@@ -339,75 +342,95 @@ int build_graph(ixb_handle* h) {
   }, &n_begin));
   cudaGraph_t outer_body;
   TRY(add_while(h, g, &n_begin, c_outer, &outer_body, &n_outer));
-  CK(cudaGraphConditionalHandleCreate(&c_mom, outer_body, 1, cudaGraphCondAssignDefault));
-  CK(cudaGraphConditionalHandleCreate(&c_pres, outer_body, 1, 0));
-  CK(cudaGraphConditionalHandleCreate(&c_ener, outer_body, 1, 0));
-  // outer body: WHILE(mom) -> p' reset + gate(pres) -> WHILE(pres) -> correct + gate(ener)
-  //             -> WHILE(ener) -> residual + outer test.  The kernel that finishes a loop's norm
-  //             applies its exit test (ixb_ctl.cuh); the momentum loop is opened by the outer
-  //             test of the previous pass and, for the first pass, by the handle's default.
   cudaGraphNode_t last = nullptr, wn;
   cudaGraph_t b;
   const double* nrm = h->norms;
-  const auto mom_pass = [&]() -> int {
-    TRY(sweep(h, EQ_UY, nullptr, false));
-    TRY(sweep(h, EQ_UX, nullptr, false));
-    const double* v_start = h->v[h->cv];
-    TRY(sweep(h, EQ_VY, nullptr, false));
-    TRY(sweep(h, EQ_VX, v_start, true, CtlRef{h->ctl_d, nrm, c_mom, 0, 0}));
-    return IXB_OK;
-  };
-  const auto pres_pass = [&]() -> int {
-    const double* pc_start = h->pc[h->cpc];
-    TRY(sweep(h, EQ_PY, nullptr, false));
-    TRY(sweep(h, EQ_PX, pc_start, true, CtlRef{h->ctl_d, nrm, c_pres, 0, 1}));
-    return IXB_OK;
-  };
-  const auto ener_pass = [&]() -> int {
-    const double* t_start = h->T[h->cT];
-    TRY(sweep(h, EQ_TY, nullptr, false));
-    TRY(sweep(h, EQ_TX, t_start, true, CtlRef{h->ctl_d, nrm, c_ener, 0, 2}));
-    return IXB_OK;
-  };
-  const bool dw = do_while_loops();
-  // one inner loop: WHILE(pass), or (do-while form) the first pass in the
-  // outer body and a WHILE node for the further passes, whose condition the
-  // first pass's exit test sets
-  const auto inner_loop = [&](cudaGraphNode_t* dep, cudaGraphConditionalHandle cond, const auto& pass) -> int {
-    if (dw) {
-      TRY(capture_into(h, outer_body, dep, pass, &last));
-      TRY(add_while(h, outer_body, &last, cond, &b, &wn));
-    } else {
-      TRY(add_while(h, outer_body, dep, cond, &b, &wn));
-    }
-    return capture_into(h, b, nullptr, pass, &last);
-  };
-  TRY(inner_loop(nullptr, c_mom, mom_pass));
-  if (dw) {
-    // p' starts every pressure loop from zero (main.f90:752-758): the first
-    // pass's y-sweep reads the zero field and its norm compares with zero,
-    // so no reset kernel is needed; its exit test opens the WHILE node
-    TRY(capture_into(h, outer_body, &wn, [&]() -> int {
-      TRY(sweep(h, EQ_PY, nullptr, false, CtlRef{}, true));
-      TRY(sweep(h, EQ_PX, h->zero, true, CtlRef{h->ctl_d, nrm, c_pres, 0, 1}));
+  for (int pass_no = 0; pass_no < unroll; ++pass_no) {
+    cudaGraphConditionalHandle c_mom, c_pres, c_ener;
+    CK(cudaGraphConditionalHandleCreate(&c_mom, outer_body, 1, cudaGraphCondAssignDefault));
+    CK(cudaGraphConditionalHandleCreate(&c_pres, outer_body, 1, 0));
+    CK(cudaGraphConditionalHandleCreate(&c_ener, outer_body, 1, 0));
+    // outer pass: WHILE(mom) -> p' reset + gate(pres) -> WHILE(pres) -> correct + gate(ener)
+    //             -> WHILE(ener) -> residual + outer test.  The kernel that finishes a loop's norm
+    //             applies its exit test (ixb_ctl.cuh); the momentum loop is opened by the outer
+    //             test of the previous pass and, for the first pass, by the handle's default.
+    const auto mom_pass = [&]() -> int {
+      TRY(sweep(h, EQ_UY, nullptr, false));
+      TRY(sweep(h, EQ_UX, nullptr, false));
+      const double* v_start = h->v[h->cv];
+      TRY(sweep(h, EQ_VY, nullptr, false));
+      TRY(sweep(h, EQ_VX, v_start, true, CtlRef{h->ctl_d, nrm, c_mom, 0, 0}));
       return IXB_OK;
-    }, &last));
-    TRY(add_while(h, outer_body, &last, c_pres, &b, &wn));
-    TRY(capture_into(h, b, nullptr, pres_pass, &last));
-  } else {
-    TRY(capture_into(h, outer_body, &wn, [&]() {
-      return launch_preset_f64(h->pc[h->cpc], h->fsz, CtlRef{h->ctl_d, nrm, c_pres, 0, 0}, h->stream) == cudaSuccess
-                 ? IXB_OK : IXB_ECUDA;
-    }, &last));
-    TRY(inner_loop(&last, c_pres, pres_pass));
+    };
+    const auto pres_pass = [&]() -> int {
+      const double* pc_start = h->pc[h->cpc];
+      TRY(sweep(h, EQ_PY, nullptr, false));
+      TRY(sweep(h, EQ_PX, pc_start, true, CtlRef{h->ctl_d, nrm, c_pres, 0, 1}));
+      return IXB_OK;
+    };
+    const auto ener_pass = [&]() -> int {
+      const double* t_start = h->T[h->cT];
+      TRY(sweep(h, EQ_TY, nullptr, false));
+      TRY(sweep(h, EQ_TX, t_start, true, CtlRef{h->ctl_d, nrm, c_ener, 0, 2}));
+      return IXB_OK;
+    };
+    const bool dw = do_while_loops();
+    // one inner loop: WHILE(pass), or (do-while form) the first pass in the
+    // outer body and a WHILE node for the further passes, whose condition the
+    // first pass's exit test sets
+    const auto inner_loop = [&](cudaGraphNode_t* dep, cudaGraphConditionalHandle cond, const auto& pass) -> int {
+      if (dw) {
+        TRY(capture_into(h, outer_body, dep, pass, &last));
+        TRY(add_while(h, outer_body, &last, cond, &b, &wn));
+      } else {
+        TRY(add_while(h, outer_body, dep, cond, &b, &wn));
+      }
+      return capture_into(h, b, nullptr, pass, &last);
+    };
+    TRY(inner_loop(pass_no == 0 ? nullptr : &last, c_mom, mom_pass));
+    if (dw) {
+      // p' starts every pressure loop from zero (main.f90:752-758): the first
+      // pass's y-sweep reads the zero field and its norm compares with zero,
+      // so no reset kernel is needed; its exit test opens the WHILE node
+      TRY(capture_into(h, outer_body, &wn, [&]() -> int {
+        TRY(sweep(h, EQ_PY, nullptr, false, CtlRef{}, true));
+        TRY(sweep(h, EQ_PX, h->zero, true, CtlRef{h->ctl_d, nrm, c_pres, 0, 1}));
+        return IXB_OK;
+      }, &last));
+      TRY(add_while(h, outer_body, &last, c_pres, &b, &wn));
+      TRY(capture_into(h, b, nullptr, pres_pass, &last));
+    } else {
+      TRY(capture_into(h, outer_body, &wn, [&]() {
+        return launch_preset_f64(h->pc[h->cpc], h->fsz, CtlRef{h->ctl_d, nrm, c_pres, 0, 0}, h->stream) == cudaSuccess
+                   ? IXB_OK : IXB_ECUDA;
+      }, &last));
+      TRY(inner_loop(&last, c_pres, pres_pass));
+    }
+    TRY(capture_into(h, outer_body, &wn, [&]() { return correct(h, CtlRef{h->ctl_d, nrm, c_ener, 0, 0}); }, &last));
+    TRY(inner_loop(&last, c_ener, ener_pass));
+    TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
+                     &last));
   }
-  TRY(capture_into(h, outer_body, &wn, [&]() { return correct(h, CtlRef{h->ctl_d, nrm, c_ener, 0, 0}); }, &last));
-  TRY(inner_loop(&last, c_ener, ener_pass));
-  TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
-                   &last));
-  CK(cudaGraphInstantiate(&h->graph_exec, g, 0));
+  CK(cudaGraphInstantiate(exec, g, 0));
   h->cu = cu; h->cv = cv; h->cT = cT; h->cpc = cpc;
-  h->graph_dirty = false;
+  return IXB_OK;
+}
+
+// The graph for `unroll` outer passes per body (1 or kOuterUnroll), built
+// or rebuilt when stale.
+int ensure_graph(ixb_handle* h, int unroll, cudaGraphExec_t* exec) {
+  if (h->graph_dirty) {
+    h->graph_stale[0] = h->graph_stale[1] = true;
+    h->graph_dirty = false;
+  }
+  const int k = unroll > 1 ? 1 : 0;
+  cudaGraph_t* g = k ? &h->graph_u : &h->graph;
+  cudaGraphExec_t* e = k ? &h->graph_u_exec : &h->graph_exec;
+  if (h->graph_stale[k] || !*e) {
+    TRY(build_graph(h, unroll, g, e));
+    h->graph_stale[k] = false;
+  }
+  *exec = *e;
   return IXB_OK;
 }
 
@@ -421,8 +444,9 @@ int normalize_parity(ixb_handle* h) {
   return IXB_OK;
 }
 
-int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
-  if (h->graph_dirty || !h->graph_exec) TRY(build_graph(h));
+int run_graph_once(ixb_handle* h, int unroll, int fixed_count, ixb_report* rep) {
+  cudaGraphExec_t exec = nullptr;
+  TRY(ensure_graph(h, unroll, &exec));
   TRY(normalize_parity(h));
   Ctl* c = h->ctl_h;
   std::memset(c, 0, sizeof(Ctl));
@@ -433,7 +457,7 @@ int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
   c->iter_ecuaci = h->iter_ecuaci;
   c->iter_simple = h->iter_simple;
   CK(cudaMemcpyAsync(h->ctl_d, c, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
-  CK(cudaGraphLaunch(h->graph_exec, h->stream));
+  CK(cudaGraphLaunch(exec, h->stream));
   CK(cudaMemcpyAsync(c, h->ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   rep->maxbo = c->maxbo; rep->residuo = c->residuo;
@@ -445,9 +469,30 @@ int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
   return c->status;
 }
 
+// The SIMPLE loop on the device: a fixed count of at least kOuterUnroll runs
+// its multiple of kOuterUnroll through the unrolled graph (one WHILE body
+// launch per kOuterUnroll passes) and the rest through the plain one; the
+// reported counts add up, the rest is the last call's.
+int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
+  if (fixed_count < kOuterUnroll) return run_graph_once(h, 1, fixed_count, rep);
+  const int head = fixed_count / kOuterUnroll * kOuterUnroll, rest = fixed_count - head;
+  const int st = run_graph_once(h, kOuterUnroll, head, rep);
+  if (st != IXB_OK || rest == 0) return st;
+  ixb_report r2{};
+  const int st2 = run_graph_once(h, 1, rest, &r2);
+  r2.n_simple += rep->n_simple;
+  r2.n_momen += rep->n_momen;
+  r2.n_pres += rep->n_pres;
+  r2.n_ener += rep->n_ener;
+  *rep = r2;
+  return st2;
+}
+
 void free_all(ixb_handle* h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->graph_u_exec) cudaGraphExecDestroy(h->graph_u_exec);
+  if (h->graph_u) cudaGraphDestroy(h->graph_u);
   if (h->egraph_exec) cudaGraphExecDestroy(h->egraph_exec);
   if (h->egraph) cudaGraphDestroy(h->egraph);
   if (h->agraph_exec) cudaGraphExecDestroy(h->agraph_exec);

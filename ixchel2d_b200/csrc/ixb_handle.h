@@ -67,7 +67,12 @@ struct ixb_handle {
   ixb::Ctl* ctl_h = nullptr;  // pinned
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
-  bool graph_dirty = true;
+  bool graph_dirty = true;  // set by every change that invalidates the SIMPLE graphs
+  // the same loop with kOuterUnroll outer passes per WHILE body, for fixed
+  // counts (ixb_simple_iterations); stale flags of [0] graph, [1] graph_u
+  cudaGraphExec_t graph_u_exec = nullptr;
+  cudaGraph_t graph_u = nullptr;
+  bool graph_stale[2] = {true, true};
   // K passes of the energy sweeps (ixb_energy_iterations) and of the energy
   // adjoint's reversed sweeps (ixb_adjoint_energy): WHILE graphs whose
   // counter kernel closes the loop after `loop_left` passes
@@ -101,6 +106,8 @@ int handle_ready(ixb_handle* h);  // mesh, params and boundary tables set; mesh 
 // run by handle_run_loop_graph(h, exec, iterations) (stream-ordered,
 // iterations >= 1; unroll * iterations passes)
 constexpr int kLoopUnroll = 10;
+// outer SIMPLE passes per WHILE body in the fixed-count graph
+constexpr int kOuterUnroll = 4;
 int handle_build_loop_graph(ixb_handle* h, const std::function<int()>& pass, int unroll, cudaGraph_t* graph,
                             cudaGraphExec_t* exec);
 int handle_run_loop_graph(ixb_handle* h, cudaGraphExec_t exec, int iterations);

@@ -272,6 +272,22 @@ def test_loop_exit_logic_matches_oracle():
         assert np.array_equal(gs[k], os_[k]), k
 
 
+@pytest.mark.parametrize("n", [4, 7, 9])
+def test_fixed_counts_through_the_unrolled_graph(n):
+    # counts of 4 or more run their multiple of 4 with four outer passes per
+    # WHILE body and the rest in the plain graph: the same fields as n
+    # single calls, and the counts add up
+    case = cases.natural_cavity(20, 16, Ra=1e5)
+    a, b = _pair(case, solver=F.SOLVER_EXACT)[0], Simple2D.from_case(case, solver=F.SOLVER_EXACT)
+    rep = a.iterations(n)
+    for _ in range(n):
+        b.iterations(1)
+    assert rep["n_simple"] == n and rep["n_momen"] == n and rep["n_pres"] == n and rep["n_ener"] == n, rep
+    sa, sb = a.download(), b.download()
+    for k in STATE:
+        assert np.array_equal(sa[k], sb[k]), k
+
+
 def test_time_steps_with_roll():
     case = cases.natural_cavity(16, 16, Ra=1e4, dt=0.5, iter_simple_max=3)
     g, o = _pair(case, solver=F.SOLVER_EXACT)
