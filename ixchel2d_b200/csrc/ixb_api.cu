@@ -469,23 +469,14 @@ int run_graph_once(ixb_handle* h, int unroll, int fixed_count, ixb_report* rep) 
   return c->status;
 }
 
-// The SIMPLE loop on the device: a fixed count of at least kOuterUnroll runs
-// its multiple of kOuterUnroll through the unrolled graph (one WHILE body
-// launch per kOuterUnroll passes) and the rest through the plain one; the
-// reported counts add up, the rest is the last call's.
+// The SIMPLE loop on the device: a fixed count that is a positive multiple
+// of kOuterUnroll runs through the unrolled graph (one WHILE body launch per
+// kOuterUnroll passes), anything else through the plain one.  (Splitting
+// other counts into the two graphs costs a second launch and host sync per
+// call, more than the unrolling saves on small grids.)
 int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
-  if (fixed_count < kOuterUnroll) return run_graph_once(h, 1, fixed_count, rep);
-  const int head = fixed_count / kOuterUnroll * kOuterUnroll, rest = fixed_count - head;
-  const int st = run_graph_once(h, kOuterUnroll, head, rep);
-  if (st != IXB_OK || rest == 0) return st;
-  ixb_report r2{};
-  const int st2 = run_graph_once(h, 1, rest, &r2);
-  r2.n_simple += rep->n_simple;
-  r2.n_momen += rep->n_momen;
-  r2.n_pres += rep->n_pres;
-  r2.n_ener += rep->n_ener;
-  *rep = r2;
-  return st2;
+  const bool unrolled = fixed_count > 0 && fixed_count % kOuterUnroll == 0;
+  return run_graph_once(h, unrolled ? kOuterUnroll : 1, fixed_count, rep);
 }
 
 void free_all(ixb_handle* h) {

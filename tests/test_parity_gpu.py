@@ -272,11 +272,10 @@ def test_loop_exit_logic_matches_oracle():
         assert np.array_equal(gs[k], os_[k]), k
 
 
-@pytest.mark.parametrize("n", [4, 7, 9])
+@pytest.mark.parametrize("n", [4, 7, 12])
 def test_fixed_counts_through_the_unrolled_graph(n):
-    # counts of 4 or more run their multiple of 4 with four outer passes per
-    # WHILE body and the rest in the plain graph: the same fields as n
-    # single calls, and the counts add up
+    # multiples of 4 run with four outer passes per WHILE body, other counts
+    # in the plain graph: the same fields as n single calls, and the counts
     case = cases.natural_cavity(20, 16, Ra=1e5)
     a, b = _pair(case, solver=F.SOLVER_EXACT)[0], Simple2D.from_case(case, solver=F.SOLVER_EXACT)
     rep = a.iterations(n)
