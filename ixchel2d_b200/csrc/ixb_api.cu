@@ -3,10 +3,12 @@
 //
 // The outer iteration (source/main.f90:395-1217) runs as one CUDA graph per
 // handle: the reference's three inner loops and the outer loop are WHILE
-// conditional nodes whose conditions are set on the device by tiny control
-// kernels that apply the reference's exit tests, so a whole SIMPLE loop is
-// one graph launch with no host round trip.  The same sequence can also be
-// driven from the host (one sync per inner pass) for debugging.
+// conditional nodes whose conditions are set on the device by the kernels
+// that finish each norm, applying the reference's exit tests, so a whole
+// SIMPLE loop is one graph launch with no host round trip.  Fixed counts
+// that are multiples of four use a second graph with four outer passes per
+// WHILE body.  The same sequence can also be driven from the host (one sync
+// per inner pass) for debugging.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -350,10 +352,13 @@ int build_graph(ixb_handle* h, int unroll, cudaGraph_t* graph, cudaGraphExec_t* 
     CK(cudaGraphConditionalHandleCreate(&c_mom, outer_body, 1, cudaGraphCondAssignDefault));
     CK(cudaGraphConditionalHandleCreate(&c_pres, outer_body, 1, 0));
     CK(cudaGraphConditionalHandleCreate(&c_ener, outer_body, 1, 0));
-    // outer pass: WHILE(mom) -> p' reset + gate(pres) -> WHILE(pres) -> correct + gate(ener)
-    //             -> WHILE(ener) -> residual + outer test.  The kernel that finishes a loop's norm
-    //             applies its exit test (ixb_ctl.cuh); the momentum loop is opened by the outer
-    //             test of the previous pass and, for the first pass, by the handle's default.
+    // outer pass: momentum loop -> pressure loop -> correct + gate(ener) -> energy loop
+    //             -> residual + outer test.  Do-while form (the default): each loop is its
+    //             first pass, then a WHILE node for further passes; the pressure loop's first
+    //             pass reads p' as zero.  Otherwise: WHILE(mom) -> p' reset + gate(pres) ->
+    //             WHILE(pres) -> ... with the momentum loop opened by the outer test of the
+    //             previous pass and, for the first pass, by the handle's default.  The kernel
+    //             that finishes a loop's norm applies its exit test (ixb_ctl.cuh).
     const auto mom_pass = [&]() -> int {
       TRY(sweep(h, EQ_UY, nullptr, false));
       TRY(sweep(h, EQ_UX, nullptr, false));
