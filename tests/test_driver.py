@@ -254,3 +254,17 @@ def test_driver_refined_run_keeps_nusselt(tmp_path, has_gpu, oracle_run):
     assert np.max(np.abs(got[:, 1:3] - want[:, 1:3])) < 1e-6
     assert np.max(np.abs(got[:, 3] - want[:, 3])) < 1e-6
     assert not (tmp_path / names["out_u"]).exists()
+
+
+def test_reynolds_tag_overflows_like_the_reference(tmp_path):
+    """entero_caracter writes each of its five digits with I1, so a ten-
+    thousands digit above 9 prints '*' (Re = ceiling(sqrt(1e12)) = 1e6)."""
+    assert CF.entero_caracter(1_000_000) == "*0000"
+    assert CF.entero_caracter(99_999) == "99999"
+    rec = CF.reynolds_tag("natural", 1e12)
+    assert rec == "*0000"
+    _case_dir(tmp_path, Ra=1e12, make_folder=False)
+    r, kv = _check(tmp_path, "--mkdir")
+    assert r.returncode == 0, r.stderr
+    assert kv["Rec"] == rec and kv["folder"] == f"n00012m00016R{rec}"
+    assert kv["nusselt_file"] == f"nuss_sim_n00012m00016_R{rec}.dat"
