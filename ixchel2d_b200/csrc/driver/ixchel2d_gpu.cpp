@@ -75,7 +75,7 @@ struct Options {
   int prec = IXB_PREC_FP64;
   int solver = IXB_SOLVER_HYBRID;
   int cuerpo = -1;  // definir_cuerpo option; -1 = 'sincu', the reference's choice (main.f90:327)
-  bool autotune = false, check = false, mkdir = false, quiet = false;
+  bool autotune = true, check = false, mkdir = false, quiet = false;
 };
 
 [[noreturn]] void die(int code, const std::string& msg) {
@@ -247,15 +247,17 @@ void parse_args(int argc, char** argv, Options* o) {
       else if (v == "chime") o->cuerpo = IXB_BODY_CHIME;
       else die(2, "--cuerpo takes sincu, trian, cuadr or chime");
     } else if (a == "--autotune") o->autotune = true;
+    else if (a == "--no-autotune") o->autotune = false;
     else if (a == "--check") o->check = true;
     else if (a == "--mkdir") o->mkdir = true;
     else if (a == "--quiet") o->quiet = true;
     else if (a == "-h" || a == "--help") {
       std::printf(
           "usage: ixchel2d_gpu [CASE_DIR] [--mi M --nj N] [--prec fp64|refined] [--solver hybrid|exact]\n"
-          "                    [--cuerpo sincu|trian|cuadr|chime] [--autotune] [--mkdir] [--check] [--quiet]\n"
+          "                    [--cuerpo sincu|trian|cuadr|chime] [--no-autotune] [--mkdir] [--check] [--quiet]\n"
           "Runs the Ixchel2D case in CASE_DIR (default: the current folder) on the GPU.\n"
-          "--check reads every input, prints what it found and exits without using the GPU.\n");
+          "--check reads every input, prints what it found and exits without using the GPU.\n"
+          "The launch shapes of the line sweeps are autotuned on the initial state (--no-autotune: defaults).\n");
       std::exit(0);
     } else if (!a.empty() && a[0] == '-') die(2, "unknown option " + a);
     else o->dir = a;
