@@ -84,10 +84,29 @@ int ensure_tables(ixb_handle* h) {
 }
 
 
-// Default launch shape of a sweep: the fewest waves of CTAs (every CTA
-// resident at once when possible), then the shortest chunks, then the most
-// SMs busy (CTAs up to the SM count), then the larger CTA.
+// Default launch shape of a sweep, from per-shape timings of every sweep on
+// 64x64, 256x256 and 701x301 grids in both precision forms: x-lines one per
+// CTA with 256 threads for lines of more than 384 rows, else 128; y-lines in
+// the fused form with 4 adjacent lines per CTA (8 once there are 4 lines per
+// SM) and 128 threads per line for lines of 160 rows or more, else 64.
+// Those shapes were within about 5 % of the best (at worst 15 %, binary64
+// y-sweeps at 701x301), where the rule below was 20-50 % behind.  When the
+// shape cannot be resident: the fewest waves of CTAs, then the shortest
+// chunks, then the most SMs busy (CTAs up to the SM count), then the larger CTA.
 void pick_shape(ixb_handle* h, int eq) {
+  {
+    const bool x = (eq & 1) != 0;
+    SweepShape probe = sweep_shape(eq, h->mi, h->nj, real_bytes(h), 1, 128);
+    const int lines = probe.nfull, n = probe.n;
+    const int tl = x ? 1 : (lines >= 4 * h->nsm ? 8 : 4);
+    const int g = x ? (n > 384 ? 256 : 128) : (n >= 160 ? 128 : 64);
+    const SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), tl, g);
+    if (sweep_occupancy(eq, solver_form(h), s) > 0) {
+      h->shape_tl[eq] = tl;
+      h->shape_g[eq] = g;
+      return;
+    }
+  }
   int best = -1;
   long long best_key = 0;
   for (int k = 0; k < kNumShapes; ++k) {
