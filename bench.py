@@ -54,10 +54,23 @@ SWEEPS = ["u-y", "u-x", "v-y", "v-x", "p'-y", "p'-x", "T-y", "T-x"]
 METRIC = "Mcell-iter/s (SIMPLE outer iteration, p-cells): FP32+FP64-refined vs FP64"
 
 
-def workload_config():
+def workload_config(world: int = 1):
+    """The `config` object of both arms (identical keys and values)."""
     return {"workload": f"lid_driven_mixed_{MI}x{NJ}_Re100_Ri1_Pr0.71_tanh1.2", "mi": MI, "nj": NJ,
             "p_cells": (MI + 1) * (NJ + 1), "outer_iters_per_step": ITERS, "inner_passes": 1,
-            "l2": "flushed (256 MiB write) before every timed step and kernel launch"}
+            "l2": "flushed (256 MiB write) before every timed step and kernel launch",
+            "parallelism": f"replicas{world}"}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 def make_case():
@@ -208,29 +221,34 @@ def run_reference(args):
         if pg:
             pg.destroy_process_group()
         return
-    case = make_case()
+    case = make_case()  # built without mapping libixb.so (cases.py loads no library for this case)
     from oracle import oracle as O
     O.set_threads(os.cpu_count() or 1)
     o = O.OracleCase(case, conv_u=1e30, conv_p=1e30, conv_t=1e30)
-    # each step is a bounded sample of the workload: 2 outer iterations
-    sample_iters = 2
+    # each step is the same workload as the GPU arm's step: ITERS outer iterations of the full case
+    o.iterations(2)
     for _ in range(args.warmup):
-        o.iterations(sample_iters)
+        o.iterations(ITERS)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        o.iterations(sample_iters)
+        o.iterations(ITERS)
         times.append(time.perf_counter() - t0)
     tot = sum(times)
-    value = case.cells * sample_iters * args.steps / tot / 1e6
+    value = case.cells * ITERS * args.steps / tot / 1e6
+    loaded = sorted({ln.split()[-1] for ln in Path("/proc/self/maps").read_text().splitlines()
+                     if ln.endswith(".so") and ("oracle" in ln or "ixchel2d_b200" in ln)})
     line = {
         "impl": "reference", "metric": METRIC, "value": value,
         "unit": "Mcell-iter/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "config": workload_config(),
-        "cpu_baseline": {"value": value, "unit": "Mcell-iter/s", "cores": O.max_threads(), "kind": "port",
-                         "sample": f"{sample_iters} outer iterations of the full 701x301 case per step"},
+        "dtype": "f64", "data": "synthetic", "config": workload_config(world),
+        "cpu_baseline": {"value": value, "unit": "Mcell-iter/s", "cores": O.max_threads(), "cpu_model": cpu_model(),
+                         "kind": "port",
+                         "sample": f"{ITERS} outer iterations of the full {MI}x{NJ} case per step, "
+                                   f"{args.steps} steps after {args.warmup} warm-up steps"},
         "e2e": {"value": value, "unit": "Mcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "libraries_mapped": loaded,
         "note": "reference is Fortran+OpenACC (nvfortran-only build); its C++ restatement (oracle/) is timed",
     }
     print(json.dumps(line), flush=True)
@@ -637,7 +655,7 @@ def run_ours(args):
             "metric": METRIC, "value": rate["refined"], "unit": "Mcell-iter/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["refined"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic", "config": {**workload_config(), "parallelism": f"replicas{world}"},
+            "data": "synthetic", "config": workload_config(world),
             "fp64": {"value": rate["fp64"], "unit": "Mcell-iter/s", "ms_per_step": ms["fp64"] / args.steps,
                      "dtype": "f64"},
             "refined_over_fp64": rate["refined"] / rate["fp64"],
@@ -661,7 +679,7 @@ def run_ours(args):
             "sweep_shapes": {n: {SWEEPS[int(k)]: list(v[:2]) for k, v in sh.items()} for n, sh in shapes.items()},
             "iteration_alg_bytes": iter_bytes,
             "cpu_baseline": None if cpu_val is None else {
-                "value": cpu_val, "unit": "Mcell-iter/s", "cores": cpu_cores, "kind": "port",
+                "value": cpu_val, "unit": "Mcell-iter/s", "cores": cpu_cores, "cpu_model": cpu_model(), "kind": "port",
                 "sample": f"{cpu_iters} outer iterations of the same 701x301 case ({cpu_s:.1f} s)"},
             "gpu_launches": sum((per_iter[n] * ITERS + 1) * args.steps for n in modes),
             "kernels_per_outer_iteration": per_iter,

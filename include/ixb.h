@@ -233,9 +233,12 @@ int ixb_tridiag_status(void);
  *   library's device image (one per GPU that loads the library, held until
  *   the process exits): n*nsys must not exceed IXB_NOALLOC_MAX_ELEMS, larger
  *   calls return IXB_EINVAL without launching anything.
- * - The first layout-1 call on a device looks up the array's device address
- *   (cudaGetSymbolAddress) with that device current; make that first call
- *   before any stream capture on the device.
+ * - A layout-1 call outside stream capture looks up the array's device
+ *   address (cudaGetSymbolAddress) with that device current, so a context
+ *   re-created after cudaDeviceReset is picked up; a call on a capturing
+ *   stream reuses the address of the last uncaptured call on that device.
+ *   Make a first uncaptured layout-1 call on a device before capturing one
+ *   (otherwise the captured call returns IXB_ECUDA).
  * - Every call shares the one array; nothing in it needs to start at zero
  *   (each element is written before it is read), but calls whose kernels
  *   overlap on the GPU (different streams, or different host threads) race

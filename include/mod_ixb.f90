@@ -3,7 +3,9 @@
 ! Ixchel2D Fortran driver.  A maintainer adds this module to
 ! source/CMakeLists.txt's SOURCE_FILES, links libixb.so, and replaces the
 ! ALGORITMO_SIMPLE body of source/main.f90:395-1217 (and the !$acc data
-! region of :356-389 / :1277) by the calls shown in INTEGRATION.md.
+! region of :356-389 / :1277) by ixb_* calls: create the handle, set the
+! mesh, parameters and boundary tables, upload the state, call ixb_step per
+! time step, download for the writers, destroy the handle.
 !
 ! The derived types mirror the C structs field by field (bind(C)); arrays
 ! keep the reference's Fortran shapes and are passed by reference.  Every

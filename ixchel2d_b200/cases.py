@@ -20,8 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._ffi import BC_DIRI, BC_NEUM, BCSide, check, dptr, lib
-import ctypes as C
+from ._types import BC_DIRI, BC_NEUM, BCSide
 
 
 def d23_15(x: np.ndarray) -> np.ndarray:
@@ -72,18 +71,37 @@ def staggered_mesh(mi: int, nj: int, xkind="unif", ykind="unif", ao=1.0, bo=1.0,
     return d23_15(xu), d23_15(yv), d23_15(xp), d23_15(yp)
 
 
+def locate(coord: np.ndarray, x1s, size: int) -> list[int]:
+    """Segment index list of one side, the rule of lectura_cond_frontera
+    (source/mod_cond_frontera.f90:125-149): the first segment starts at node 2,
+    segment k ends before the first node whose coordinate exceeds its x1
+    (size+1 when none does), and the last segment ends at node size-1."""
+    idx = [2]
+    for x1 in x1s:
+        kk = 1
+        while kk <= size and not (coord[kk - 1] > x1):
+            kk += 1
+        idx.append(kk)
+    idx[len(x1s)] = size - 1
+    return idx
+
+
 def bc_side(side: int, segments: list[tuple[float, int, float]], xx: np.ndarray, yy: np.ndarray) -> BCSide:
     """One side of a boundary table: segments are (x1, type, value) in file
-    order; indices by ixb_bc_locate (lectura_cond_frontera's rule)."""
+    order; sides a and c (0, 2) run along the y-coordinates, b and d (1, 3)
+    along x.  The same table ixb_bc_locate builds, computed here so that a
+    case can be built without mapping the library."""
+    if not 0 <= side <= 3 or len(segments) > 15:
+        raise ValueError("side must be 0..3 and a side holds at most 15 segments")
+    coord = np.asarray(yy if side in (0, 2) else xx, dtype=np.float64)
     out = BCSide()
-    nd = len(segments)
-    x1 = (C.c_double * max(nd, 1))(*[s[0] for s in segments])
-    ty = (C.c_int * max(nd, 1))(*[s[1] for s in segments])
-    va = (C.c_double * max(nd, 1))(*[s[2] for s in segments])
-    xx = np.ascontiguousarray(xx, dtype=np.float64)
-    yy = np.ascontiguousarray(yy, dtype=np.float64)
-    check(lib.ixb_bc_locate(side, nd, x1, ty, va, dptr(xx), xx.size, dptr(yy), yy.size, C.byref(out)),
-          "ixb_bc_locate")
+    out.side = side
+    out.ndivis = len(segments)
+    for k, (_, ty, va) in enumerate(segments):
+        out.type[k] = int(ty)
+        out.value[k] = float(va)
+    for k, ix in enumerate(locate(coord, [float(s[0]) for s in segments], coord.size)):
+        out.index[k] = ix
     return out
 
 
@@ -132,6 +150,7 @@ def add_body(case: Case, shape: int, prm=None, flags: int = 0, t_value: float = 
             arrs[var] = (np.array(f, dtype=np.float64, order="F"), np.array(l, dtype=np.float64, order="F"))
         else:
             arrs[var] = (np.zeros(sh[var], order="F"), np.zeros(sh[var], order="F"))
+    from ._ffi import check, dptr, lib  # the masks come from the library's ixb_body_sources
     p = None if prm is None else np.ascontiguousarray(prm, dtype=np.float64)
     xp = np.ascontiguousarray(case.xp, dtype=np.float64)
     yp = np.ascontiguousarray(case.yp, dtype=np.float64)

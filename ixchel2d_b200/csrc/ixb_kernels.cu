@@ -2,6 +2,7 @@
 // (p/u/v correction, u residual, Nusselt number, mesh-constant tables), the
 // launch shape of the sweeps and their dispatch to the per-equation
 // translation units.
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -282,16 +283,22 @@ bool pdl_enabled() {
   return on;
 }
 
+// The shared-memory opt-in is a per-device function attribute, so it is set
+// once per device (under a lock: handles may be created from several threads).
 cudaError_t sweep_set_smem_limits() {
-  static int done = 0;
-  if (done) return cudaSuccess;
+  constexpr int kMaxDev = 64;
+  static bool done[kMaxDev] = {};
+  static std::mutex mu;
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return cudaSuccess;
   e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
   e = solve_set_smem_limits(optin - 1024);  // room for the static reduction buffers
-  if (e == cudaSuccess) done = 1;
+  if (e == cudaSuccess) done[dev] = true;
   return e;
 }
 

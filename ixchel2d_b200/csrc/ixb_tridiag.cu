@@ -920,18 +920,27 @@ std::mutex g_noalloc_mutex;
 
 // Device address of the scratch array for the current device.  In host code
 // the name g_noalloc_scratch denotes a host-side shadow, not device memory,
-// so the address is looked up once per device with that device current.
-cudaError_t noalloc_scratch(double** out) {
+// so the address is looked up with that device current.  Outside stream
+// capture it is looked up on every call (a context destroyed and re-created,
+// e.g. after cudaDeviceReset, reloads the module at another address); while
+// `st` is capturing, the address of the last uncaptured call on this device
+// is used, so the first call on a device must come before any capture.
+cudaError_t noalloc_scratch(cudaStream_t st, double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_noalloc_ptr[dev] = static_cast<double*>(p);
+  } else if (!g_noalloc_ptr[dev]) {
+    return cudaErrorStreamCaptureUnsupported;
   }
   *out = g_noalloc_ptr[dev];
   return cudaSuccess;
@@ -954,7 +963,7 @@ extern "C" int ixb_tridiag_f64_noalloc(const double* a, const double* b, const d
   } else {
     if ((size_t)n * (size_t)nsys > (size_t)IXB_NOALLOC_MAX_ELEMS) return IXB_EINVAL;
     double* work = nullptr;
-    e = noalloc_scratch(&work);
+    e = noalloc_scratch(st, &work);
     if (e == cudaSuccess) {
       // every work[] element is written before it is read: nothing to clear
       if (solver == IXB_SOLVER_EXACT)

@@ -75,18 +75,36 @@ def _locate_ref(coord, x1s, size):
     return idx
 
 
+def _lib_locate(side, segs, xx, yy):
+    """The library's ixb_bc_locate on the same segments."""
+    out = F.BCSide()
+    nd = len(segs)
+    x1 = (C.c_double * max(nd, 1))(*[s[0] for s in segs])
+    ty = (C.c_int * max(nd, 1))(*[s[1] for s in segs])
+    va = (C.c_double * max(nd, 1))(*[s[2] for s in segs])
+    xx = np.ascontiguousarray(xx, dtype=np.float64)
+    yy = np.ascontiguousarray(yy, dtype=np.float64)
+    F.check(F.lib.ixb_bc_locate(side, nd, x1, ty, va, F.dptr(xx), xx.size, F.dptr(yy), yy.size, C.byref(out)),
+            "ixb_bc_locate")
+    return out
+
+
+@pytest.mark.parametrize("nseg", [0, 1, 5])
 @pytest.mark.parametrize("side", [0, 1, 2, 3])
-def test_bc_locate_follows_reference_rule(side):
+def test_bc_locate_follows_reference_rule(side, nseg):
     c = cases.lid_driven_mixed(31, 19)
     xx, yy = c.xp, c.yp
     coord = yy if side in (0, 2) else xx
-    x1s = [0.2, 0.55, 0.1, 0.9, 5.0]  # unsorted and past the end on purpose
+    x1s = [0.2, 0.55, 0.1, 0.9, 5.0][:nseg]  # unsorted and past the end on purpose
     segs = [(x, F.BC_DIRI if k % 2 else F.BC_NEUM, float(k)) for k, x in enumerate(x1s)]
-    b = cases.bc_side(side, segs, xx, yy)
-    assert b.ndivis == 5 and b.side == side
-    assert list(b.index[:6]) == _locate_ref(coord, x1s, coord.size)
-    assert list(b.type[:5]) == [s[1] for s in segs]
-    assert list(b.value[:5]) == [s[2] for s in segs]
+    b = _lib_locate(side, segs, xx, yy)
+    assert b.ndivis == nseg and b.side == side
+    assert list(b.index[:nseg + 1]) == _locate_ref(coord, x1s, coord.size)
+    assert list(b.type[:nseg]) == [s[1] for s in segs]
+    assert list(b.value[:nseg]) == [s[2] for s in segs]
+    # the case builders' table (built without the library) is the same table, byte for byte
+    p = cases.bc_side(side, segs, xx, yy)
+    assert bytes(p) == bytes(b)
 
 
 def test_read_bc_file(tmp_path):

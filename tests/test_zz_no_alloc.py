@@ -71,3 +71,39 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     st = F.lib.ixb_tridiag_f64_noalloc(p, p, p, p, p, n, nsys, 1, F.SOLVER_HYBRID,
                                        torch.cuda.current_stream().cuda_stream)
     assert st == F.EINVAL
+
+
+def test_noalloc_calls_leave_device_memory_unchanged():
+    # the property the entry point exists for: after a first call on the
+    # device, further calls (both layouts, both solvers) take no device
+    # memory.  torch's cache is emptied and the device's free memory compared
+    # around 20 calls; the comparison is retried so that a change made by
+    # another process on the same GPU cannot fail it.
+    import torch
+    n, nsys = 702, 300
+    arrs = _systems(n, nsys, seed=7)
+    dev = {lay: [torch.tensor(np.ascontiguousarray(x if lay == 0 else x.T), dtype=torch.float64, device="cuda")
+                 for x in arrs] for lay in (0, 1)}
+    out = {lay: torch.empty_like(dev[lay][3]) for lay in (0, 1)}
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def calls(k):
+        for _ in range(k):
+            for lay in (0, 1):
+                for solver in (F.SOLVER_EXACT, F.SOLVER_HYBRID):
+                    st = F.lib.ixb_tridiag_f64_noalloc(*(t.data_ptr() for t in dev[lay]), out[lay].data_ptr(), n,
+                                                       nsys, lay, solver, stream)
+                    assert st == F.OK
+        torch.cuda.synchronize()
+
+    calls(1)  # first calls: module loading and the scratch address lookup
+    torch.cuda.empty_cache()
+    same = []
+    for _ in range(3):
+        free0, _ = torch.cuda.mem_get_info()
+        calls(5)
+        free1, _ = torch.cuda.mem_get_info()
+        same.append(free1 == free0)
+        if same[-1]:
+            break
+    assert any(same), "device memory changed across ixb_tridiag_f64_noalloc calls"
