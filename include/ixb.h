@@ -102,7 +102,9 @@ typedef struct {
   double err_u, err_p, err_t; /* last inner-loop errors (||dv||, ||dp'||, ||dT||) */
   int64_t n_simple; /* outer iterations run in this call */
   int64_t n_momen, n_pres, n_ener; /* inner passes run in this call */
-  int exit_code;    /* 0 none (fixed count), 1 converged, 2 iteration limit */
+  int exit_code;    /* 0 none (fixed count), 1 converged, 2 iteration limit;
+                       ixb_simple_converge: 3 |dNu| below tol_dnu, 4 maxbo below
+                       tol_maxbo, 5 max_iters reached */
   int status;
 } ixb_report;
 
@@ -151,6 +153,31 @@ int ixb_simple_iterations(ixb_handle* h, int n, ixb_report* rep);
 /* The ALGORITMO_SIMPLE loop of one time step, with the reference's exit
  * logic (main.f90:1202-1215). */
 int ixb_simple_loop(ixb_handle* h, ixb_report* rep);
+/* Nusselt monitor of ixb_simple_converge: the wall-averaged Nusselt number
+ * of ixb_nusselt_y (vertical = 0: walls jj = 1 and nj+1, panels
+ * ii = k0..k1 step 2) or ixb_nusselt_x (vertical = 1: walls ii = 1 and
+ * mi+1, panels jj = k0..k1 step 2), evaluated every `every` outer
+ * iterations on the device.  `wall` picks the monitored one (0: index 1,
+ * 1: the last index). */
+typedef struct {
+  int vertical, k0, k1, wall;
+  int every;            /* outer iterations between evaluations (>= 1) */
+  int reserved;
+  int64_t max_iters;    /* stop once this many outer iterations ran (checked every `every`) */
+  double tol_dnu;       /* stop when |Nu - Nu of the previous evaluation| < tol_dnu */
+  double tol_maxbo;     /* stop when maxbo < tol_maxbo (0: never) */
+} ixb_nu_monitor;
+/* Outer SIMPLE iterations (ixb_simple_iterations' passes, no outer exit
+ * test) until the monitored Nusselt number settles: one CUDA graph launch,
+ * the Nusselt numbers and the stopping test run on the device between
+ * blocks of `every` iterations, with no host round trip.  Derived from the
+ * reference's periodic Nusselt evaluation (main.f90:1226-1247,
+ * nusselt_promedio_y of mod_postproceso.f90:100-215), which runs on the
+ * host every 1000 time steps and stops nothing.  nu[2] (may be NULL): both
+ * walls' Nusselt numbers at the last evaluation; dnu (may be NULL): the
+ * monitored wall's last change (infinite after a single evaluation).
+ * rep->exit_code: 3 |dNu| < tol_dnu, 4 maxbo < tol_maxbo, 5 max_iters. */
+int ixb_simple_converge(ixb_handle* h, const ixb_nu_monitor* mon, ixb_report* rep, double* nu, double* dnu);
 /* Time-step roll T_ant,u_ant,v_ant <- T,u,v (main.f90:1251-1270). */
 int ixb_roll(ixb_handle* h);
 /* One time step: ixb_simple_loop then ixb_roll (main.f90:391-1271 body). */

@@ -49,6 +49,12 @@ module ixb
      integer(c_int) :: exit_code, status
   end type ixb_report
 
+  type, bind(C) :: ixb_nu_monitor
+     integer(c_int) :: vertical, k0, k1, wall, every, reserved
+     integer(c_int64_t) :: max_iters
+     real(c_double) :: tol_dnu, tol_maxbo
+  end type ixb_nu_monitor
+
   interface
      integer(c_int) function ixb_create(mi, nj, prec_mode, h) bind(C, name="ixb_create")
        import :: c_int, c_ptr
@@ -106,6 +112,14 @@ module ixb
        type(c_ptr), value :: h
        type(ixb_report), intent(out) :: rep
      end function ixb_simple_loop
+
+     integer(c_int) function ixb_simple_converge(h, mon, rep, nu, dnu) bind(C, name="ixb_simple_converge")
+       import :: c_int, c_ptr, c_double, ixb_report, ixb_nu_monitor
+       type(c_ptr), value :: h
+       type(ixb_nu_monitor), intent(in) :: mon
+       type(ixb_report), intent(out) :: rep
+       real(c_double), intent(out) :: nu(2), dnu
+     end function ixb_simple_converge
 
      integer(c_int) function ixb_step(h, rep) bind(C, name="ixb_step")
        import :: c_int, c_ptr, ixb_report

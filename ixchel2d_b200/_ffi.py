@@ -18,7 +18,7 @@ from ._types import (  # noqa: F401,E402  (re-exported)
     BC_DIRI, BC_NEUM, BC_OTHER, BODY_BOX, BODY_CHIME, BODY_CUADR, BODY_REGION, BODY_TEMP, BODY_TRIAN, BODY_VEL,
     EBC, ECUDA, EINVAL, EIO, ENOMEM, ENONFINITE, ESTATE, ETIMEOUT, MESH_CENT, MESH_TANH, MESH_TUBO, MESH_UNIF,
     NOALLOC_MAX_ELEMS, OK, PREC_FP32_REFINED, PREC_FP64, SOLVER_EXACT, SOLVER_HYBRID, VAR_T, VAR_U, VAR_V,
-    BCSide, Params, Report,
+    BCSide, NuMonitor, Params, Report,
 )
 
 
@@ -50,6 +50,7 @@ SIGNATURES = [
     ("ixb_download_aux", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     ("ixb_simple_iterations", C.c_int, [_vp, C.c_int, C.POINTER(Report)]),
     ("ixb_simple_loop", C.c_int, [_vp, C.POINTER(Report)]),
+    ("ixb_simple_converge", C.c_int, [_vp, C.POINTER(NuMonitor), C.POINTER(Report), _dp, _dp]),
     ("ixb_roll", C.c_int, [_vp]),
     ("ixb_step", C.c_int, [_vp, C.POINTER(Report)]),
     ("ixb_phase", C.c_int, [_vp, C.c_int]),

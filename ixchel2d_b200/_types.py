@@ -43,3 +43,8 @@ class Report(C.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class NuMonitor(C.Structure):
+    _fields_ = [("vertical", C.c_int), ("k0", C.c_int), ("k1", C.c_int), ("wall", C.c_int), ("every", C.c_int),
+                ("reserved", C.c_int), ("max_iters", C.c_int64), ("tol_dnu", C.c_double), ("tol_maxbo", C.c_double)]

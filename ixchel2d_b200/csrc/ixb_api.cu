@@ -341,28 +341,17 @@ bool do_while_loops() {
   return v;
 }
 
-// The SIMPLE loop as one graph: a WHILE node over `unroll` outer passes.
-// unroll > 1 serves fixed counts that are multiples of it (every pass's
-// outer test counts; the last one of the body decides whether it repeats).
-int build_graph(ixb_handle* h, int unroll, cudaGraph_t* graph, cudaGraphExec_t* exec) {
-  if (*exec) { cudaGraphExecDestroy(*exec); *exec = nullptr; }
-  if (*graph) { cudaGraphDestroy(*graph); *graph = nullptr; }
-  // the graph bakes buffer parity 0 into its kernel arguments
-  const int cu = h->cu, cv = h->cv, cT = h->cT, cpc = h->cpc;
-  h->cu = h->cv = h->cT = h->cpc = 0;
-  cudaGraph_t g;
-  CK(cudaGraphCreate(&g, 0));
-  *graph = g;
+// Add the SIMPLE outer loop to graph `g` after `dep`: a WHILE node on
+// `c_outer` (a conditional handle of `g`) whose body runs `unroll` outer
+// passes.  unroll > 1 serves fixed counts that are multiples of it (every
+// pass's outer test counts; the last one of the body decides whether it
+// repeats).  Buffer parity must be 0 on entry (the passes return it to 0).
+int add_outer_loop(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, cudaGraphConditionalHandle c_outer,
+                   int unroll, cudaGraphNode_t* n_outer) {
   // a conditional handle belongs to the graph that holds its node: the
   // outer handle to g, the inner ones to the outer loop's body
-  cudaGraphConditionalHandle c_outer;
-  CK(cudaGraphConditionalHandleCreate(&c_outer, g, 1, cudaGraphCondAssignDefault));
-  cudaGraphNode_t n_begin, n_outer;
-  TRY(capture_into(h, g, nullptr, [&]() {
-    return launch_k(ctl_begin_kernel, 1, 1, 0, h->stream, h->ctl_d, c_outer) == cudaSuccess ? IXB_OK : IXB_ECUDA;
-  }, &n_begin));
   cudaGraph_t outer_body;
-  TRY(add_while(h, g, &n_begin, c_outer, &outer_body, &n_outer));
+  TRY(add_while(h, g, dep, c_outer, &outer_body, n_outer));
   cudaGraphNode_t last = nullptr, wn;
   cudaGraph_t b;
   const double* nrm = h->norms;
@@ -435,24 +424,73 @@ int build_graph(ixb_handle* h, int unroll, cudaGraph_t* graph, cudaGraphExec_t* 
     TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
                      &last));
   }
+  return IXB_OK;
+}
+
+// Start of a block of outer passes inside the Nusselt monitor's loop: the
+// block counts its passes from zero (fixed_count = the monitor's interval).
+__global__ void block_begin_kernel(Ctl* c, cudaGraphConditionalHandle outer) {
+  cudaGraphSetConditional(outer, 1u);
+  c->outer_done = 0;
+  c->inner_done = 0;
+}
+
+// The SIMPLE loop graphs.  GRAPH_PLAIN / GRAPH_UNROLLED: begin kernel, then
+// the outer loop (1 or kOuterUnroll passes per WHILE body).  GRAPH_MON_*:
+// begin kernel, then a WHILE node (the Nusselt monitor's loop) whose body is
+// a block of outer passes (fixed_count of them, the monitor's interval) and
+// the Nusselt kernel, whose monitor test decides whether another block runs.
+int build_graph(ixb_handle* h, int kind, cudaGraph_t* graph, cudaGraphExec_t* exec) {
+  if (*exec) { cudaGraphExecDestroy(*exec); *exec = nullptr; }
+  if (*graph) { cudaGraphDestroy(*graph); *graph = nullptr; }
+  const int unroll = (kind == GRAPH_UNROLLED || kind == GRAPH_MON_UNROLLED) ? kOuterUnroll : 1;
+  const bool monitor = kind == GRAPH_MON_PLAIN || kind == GRAPH_MON_UNROLLED;
+  // the graph bakes buffer parity 0 into its kernel arguments
+  const int cu = h->cu, cv = h->cv, cT = h->cT, cpc = h->cpc;
+  h->cu = h->cv = h->cT = h->cpc = 0;
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  *graph = g;
+  cudaGraphConditionalHandle c_top;
+  CK(cudaGraphConditionalHandleCreate(&c_top, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNode_t n_begin, n_top;
+  TRY(capture_into(h, g, nullptr, [&]() {
+    return launch_k(ctl_begin_kernel, 1, 1, 0, h->stream, h->ctl_d, c_top) == cudaSuccess ? IXB_OK : IXB_ECUDA;
+  }, &n_begin));
+  if (!monitor) {
+    TRY(add_outer_loop(h, g, &n_begin, c_top, unroll, &n_top));
+  } else {
+    cudaGraph_t mbody;
+    TRY(add_while(h, g, &n_begin, c_top, &mbody, &n_top));
+    cudaGraphConditionalHandle c_outer;
+    CK(cudaGraphConditionalHandleCreate(&c_outer, mbody, 1, cudaGraphCondAssignDefault));
+    cudaGraphNode_t n_bb, n_outer, n_nu;
+    TRY(capture_into(h, mbody, nullptr, [&]() {
+      return launch_k(block_begin_kernel, 1, 1, 0, h->stream, h->ctl_d, c_outer) == cudaSuccess ? IXB_OK : IXB_ECUDA;
+    }, &n_bb));
+    TRY(add_outer_loop(h, mbody, &n_bb, c_outer, unroll, &n_outer));
+    const Geo<double> G = make_geo(h);
+    TRY(capture_into(h, mbody, &n_outer, [&]() {
+      return launch_nusselt_f64(G, h->T[h->cT], h->xp_d, h->yp_d, 0, 1, 1, h->nu_d, h->stream, h->ctl_d, c_top) ==
+                     cudaSuccess ? IXB_OK : IXB_ECUDA;
+    }, &n_nu));
+  }
   CK(cudaGraphInstantiate(exec, g, 0));
   h->cu = cu; h->cv = cv; h->cT = cT; h->cpc = cpc;
   return IXB_OK;
 }
 
-// The graph for `unroll` outer passes per body (1 or kOuterUnroll), built
-// or rebuilt when stale.
-int ensure_graph(ixb_handle* h, int unroll, cudaGraphExec_t* exec) {
+// The graph of `kind`, built or rebuilt when stale.
+int ensure_graph(ixb_handle* h, int kind, cudaGraphExec_t* exec) {
   if (h->graph_dirty) {
-    h->graph_stale[0] = h->graph_stale[1] = true;
+    for (bool& st : h->graph_stale) st = true;
     h->graph_dirty = false;
   }
-  const int k = unroll > 1 ? 1 : 0;
-  cudaGraph_t* g = k ? &h->graph_u : &h->graph;
-  cudaGraphExec_t* e = k ? &h->graph_u_exec : &h->graph_exec;
-  if (h->graph_stale[k] || !*e) {
-    TRY(build_graph(h, unroll, g, e));
-    h->graph_stale[k] = false;
+  cudaGraph_t* g = &h->graphs[kind];
+  cudaGraphExec_t* e = &h->graph_execs[kind];
+  if (h->graph_stale[kind] || !*e) {
+    TRY(build_graph(h, kind, g, e));
+    h->graph_stale[kind] = false;
   }
   *exec = *e;
   return IXB_OK;
@@ -468,12 +506,23 @@ int normalize_parity(ixb_handle* h) {
   return IXB_OK;
 }
 
-int run_graph_once(ixb_handle* h, int unroll, int fixed_count, ixb_report* rep) {
+// Launch the graph of `kind` with the loop inputs of the handle; `mon`
+// (monitor graphs only) sets the Nusselt monitor's inputs.
+int run_graph_once(ixb_handle* h, int kind, int fixed_count, ixb_report* rep, const ixb_nu_monitor* mon = nullptr) {
   cudaGraphExec_t exec = nullptr;
-  TRY(ensure_graph(h, unroll, &exec));
+  TRY(ensure_graph(h, kind, &exec));
   TRY(normalize_parity(h));
   Ctl* c = h->ctl_h;
   std::memset(c, 0, sizeof(Ctl));
+  if (mon) {
+    c->mon_vertical = mon->vertical;
+    c->mon_k0 = mon->k0;
+    c->mon_k1 = mon->k1;
+    c->mon_wall = mon->wall;
+    c->mon_max_iters = mon->max_iters;
+    c->mon_tol_dnu = mon->tol_dnu;
+    c->mon_tol_maxbo = mon->tol_maxbo;
+  }
   c->conv_u = h->prm.conv_u; c->conv_p = h->prm.conv_p; c->conv_t = h->prm.conv_t;
   c->conv_resi = h->prm.conv_resi; c->conv_paso = h->prm.conv_paso;
   c->iter_ecuaci_max = h->prm.iter_ecuaci_max; c->iter_simple_max = h->prm.iter_simple_max;
@@ -500,14 +549,14 @@ int run_graph_once(ixb_handle* h, int unroll, int fixed_count, ixb_report* rep) 
 // call, more than the unrolling saves on small grids.)
 int run_graph(ixb_handle* h, int fixed_count, ixb_report* rep) {
   const bool unrolled = fixed_count > 0 && fixed_count % kOuterUnroll == 0;
-  return run_graph_once(h, unrolled ? kOuterUnroll : 1, fixed_count, rep);
+  return run_graph_once(h, unrolled ? GRAPH_UNROLLED : GRAPH_PLAIN, fixed_count, rep);
 }
 
 void free_all(ixb_handle* h) {
-  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-  if (h->graph) cudaGraphDestroy(h->graph);
-  if (h->graph_u_exec) cudaGraphExecDestroy(h->graph_u_exec);
-  if (h->graph_u) cudaGraphDestroy(h->graph_u);
+  for (int k = 0; k < 4; ++k) {
+    if (h->graph_execs[k]) cudaGraphExecDestroy(h->graph_execs[k]);
+    if (h->graphs[k]) cudaGraphDestroy(h->graphs[k]);
+  }
   if (h->egraph_exec) cudaGraphExecDestroy(h->egraph_exec);
   if (h->egraph) cudaGraphDestroy(h->egraph);
   if (h->agraph_exec) cudaGraphExecDestroy(h->agraph_exec);
@@ -922,6 +971,63 @@ int ixb_simple_loop(ixb_handle* h, ixb_report* rep) {
   return st;
 }
 
+static int nusselt(ixb_handle* h, int vertical, int k0, int k1, double* nu0, double* nu1);
+
+// Panels k0..k1 (step 2) of a wall-averaged Nusselt number fit the walls.
+static bool nu_range_ok(const ixb_handle* h, int vertical, int k0, int k1) {
+  const int n_along = vertical ? h->nj + 1 : h->mi + 1;
+  if (k0 < 1 || k1 < k0) return false;
+  return k0 + 2 * ((k1 - k0) / 2) + 2 <= n_along;
+}
+
+int ixb_simple_converge(ixb_handle* h, const ixb_nu_monitor* mon, ixb_report* rep, double* nu, double* dnu) {
+  TRY(ready(h));
+  if (!mon || mon->every < 1 || mon->max_iters < 1 || (mon->vertical != 0 && mon->vertical != 1) ||
+      (mon->wall != 0 && mon->wall != 1) || !(mon->tol_dnu >= 0.0) || !(mon->tol_maxbo >= 0.0) ||
+      !nu_range_ok(h, mon->vertical, mon->k0, mon->k1))
+    return IXB_EINVAL;
+  ixb_report local;
+  ixb_report* r = rep ? rep : &local;
+  rep_clear(r);
+  double nu2[2] = {0.0, 0.0}, d = INFINITY;
+  int st;
+  if (h->use_graph) {
+    const int kind = mon->every % kOuterUnroll == 0 ? GRAPH_MON_UNROLLED : GRAPH_MON_PLAIN;
+    st = run_graph_once(h, kind, mon->every, r, mon);
+    const Ctl* c = h->ctl_h;
+    nu2[0] = c->mon_nu[0];
+    nu2[1] = c->mon_nu[1];
+    d = c->mon_dnu;
+  } else {
+    // host-driven: blocks of `every` passes, the Nusselt number and the
+    // monitor's test on the host, in the order the graph applies them
+    st = IXB_OK;
+    long long evals = 0;
+    double prev = 0.0;
+    while (st == IXB_OK) {
+      ixb_report b;
+      st = ixb_simple_iterations(h, mon->every, &b);
+      r->n_simple += b.n_simple; r->n_momen += b.n_momen; r->n_pres += b.n_pres; r->n_ener += b.n_ener;
+      r->maxbo = b.maxbo; r->residuo = b.residuo; r->err_u = b.err_u; r->err_p = b.err_p; r->err_t = b.err_t;
+      if (st != IXB_OK) break;
+      st = nusselt(h, mon->vertical, mon->k0, mon->k1, &nu2[0], &nu2[1]);
+      if (st != IXB_OK) break;
+      const double v = nu2[mon->wall];
+      d = evals > 0 ? std::fabs(v - prev) : INFINITY;
+      prev = v;
+      ++evals;
+      if (!std::isfinite(v)) { st = IXB_ENONFINITE; break; }
+      if (d < mon->tol_dnu) { r->exit_code = 3; break; }
+      if (r->maxbo < mon->tol_maxbo) { r->exit_code = 4; break; }
+      if (r->n_simple >= mon->max_iters) { r->exit_code = 5; break; }
+    }
+  }
+  if (nu) { nu[0] = nu2[0]; nu[1] = nu2[1]; }
+  if (dnu) *dnu = d;
+  r->status = st;
+  return st;
+}
+
 int ixb_roll(ixb_handle* h) {
   if (!h) return IXB_EINVAL;
   const size_t fb = h->fsz * sizeof(double);
@@ -1099,10 +1205,7 @@ int ixb_autotune(ixb_handle* h, int reps, size_t flush_bytes, int* chosen, doubl
 
 static int nusselt(ixb_handle* h, int vertical, int k0, int k1, double* nu0, double* nu1) {
   if (!h || !h->has_mesh) return IXB_ESTATE;
-  const int n_along = vertical ? h->nj + 1 : h->mi + 1;
-  if (k0 < 1 || k1 < k0) return IXB_EINVAL;
-  for (int k = k0; k <= k1; k += 2)
-    if (k + 2 > n_along) return IXB_EINVAL;
+  if (!nu_range_ok(h, vertical, k0, k1)) return IXB_EINVAL;
   Geo<double> G = make_geo(h);
   CK(launch_nusselt_f64(G, h->T[h->cT], h->xp_d, h->yp_d, vertical, k0, k1, h->nu_d, h->stream));
   double out[2];

@@ -62,4 +62,33 @@ static __device__ void ctl_outer_step(Ctl* c, const double* norms, cudaGraphCond
   cudaGraphSetConditional(outer, again ? 1u : 0u);
 }
 
+// After a block of outer passes of ixb_simple_converge: record the Nusselt
+// numbers of both walls (nu2) and |Nu - Nu at the previous evaluation| of the
+// monitored wall, then stop the monitor loop (exit_code 3) when that change
+// is below mon_tol_dnu, (4) when maxbo is below mon_tol_maxbo, (5) once
+// mon_max_iters outer passes are done, or on an error status of the passes.
+static __device__ void ctl_monitor_step(Ctl* c, const double* nu2, cudaGraphConditionalHandle mon) {
+  c->mon_nu[0] = nu2[0];
+  c->mon_nu[1] = nu2[1];
+  const double nu = nu2[c->mon_wall];
+  const double dnu = c->mon_evals > 0 ? fabs(nu - c->mon_nu_prev) : INFINITY;
+  c->mon_dnu = dnu;
+  c->mon_nu_prev = nu;
+  c->mon_evals++;
+  bool stop = true;
+  if (c->status != 0) {
+  } else if (!finite_d(nu)) {
+    c->status = IXB_ENONFINITE;
+  } else if (dnu < c->mon_tol_dnu) {
+    c->exit_code = 3;
+  } else if (c->maxbo < c->mon_tol_maxbo) {
+    c->exit_code = 4;
+  } else if (c->n_simple >= c->mon_max_iters) {
+    c->exit_code = 5;
+  } else {
+    stop = false;
+  }
+  cudaGraphSetConditional(mon, stop ? 0u : 1u);
+}
+
 }  // namespace ixb

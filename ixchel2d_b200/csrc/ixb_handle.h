@@ -19,12 +19,22 @@ struct Ctl {
   int fixed_count;   // >0: run exactly this many outer passes, no outer test
   // state
   int iter_ecuaci, iter_simple;
-  int outer_done;    // passes done in this launch
+  int outer_done;    // passes done in this launch (in a monitor block: in this block)
   int inner_done;    // passes of the current inner loop (hard cap: iter_ecuaci_max + 2)
   int exit_code, status;
   long long n_simple, n_momen, n_pres, n_ener;
   double err_u, err_p, err_t, maxbo, residuo;
+  // Nusselt monitor (ixb_simple_converge): inputs
+  int mon_vertical, mon_k0, mon_k1, mon_wall;
+  long long mon_max_iters;
+  double mon_tol_dnu, mon_tol_maxbo;
+  // Nusselt monitor: state
+  long long mon_evals;
+  double mon_nu[2], mon_nu_prev, mon_dnu;
 };
+
+// the SIMPLE loop graphs of a handle
+enum GraphKind { GRAPH_PLAIN = 0, GRAPH_UNROLLED = 1, GRAPH_MON_PLAIN = 2, GRAPH_MON_UNROLLED = 3 };
 
 }  // namespace ixb
 
@@ -65,14 +75,14 @@ struct ixb_handle {
   // control for graphs
   ixb::Ctl* ctl_d = nullptr;
   ixb::Ctl* ctl_h = nullptr;  // pinned
-  cudaGraphExec_t graph_exec = nullptr;
-  cudaGraph_t graph = nullptr;
   bool graph_dirty = true;  // set by every change that invalidates the SIMPLE graphs
-  // the same loop with kOuterUnroll outer passes per WHILE body, for fixed
-  // counts (ixb_simple_iterations); stale flags of [0] graph, [1] graph_u
-  cudaGraphExec_t graph_u_exec = nullptr;
-  cudaGraph_t graph_u = nullptr;
-  bool graph_stale[2] = {true, true};
+  // the SIMPLE loop graphs, by kind (ixb::GraphKind): the plain loop, the
+  // same loop with kOuterUnroll outer passes per WHILE body for fixed counts
+  // (ixb_simple_iterations), and both of those inside the Nusselt monitor's
+  // WHILE loop (ixb_simple_converge)
+  cudaGraph_t graphs[4] = {};
+  cudaGraphExec_t graph_execs[4] = {};
+  bool graph_stale[4] = {true, true, true, true};
   // K passes of the energy sweeps (ixb_energy_iterations) and of the energy
   // adjoint's reversed sweeps (ixb_adjoint_energy): WHILE graphs whose
   // counter kernel closes the loop after `loop_left` passes

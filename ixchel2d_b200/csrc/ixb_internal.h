@@ -246,8 +246,12 @@ cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const dou
 // p' = 0 over a whole field, opening the pressure loop (graph only)
 cudaError_t launch_preset_f64(double* pc, size_t n, const CtlRef& gate, cudaStream_t st);
 int residual_grid(int mi, int nj);
+// Nusselt numbers of both walls (out2); with `mon` set, the wall and panel
+// range come from the monitor fields of `mon`, and the monitor's stopping
+// test sets `cond` (graph only)
 cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,
-                               int vertical, int k0, int k1, double* out2, cudaStream_t st);
+                               int vertical, int k0, int k1, double* out2, cudaStream_t st, Ctl* mon = nullptr,
+                               cudaGraphConditionalHandle cond = 0);
 cudaError_t sweep_set_smem_limits();
 cudaError_t launch_tables_f64(const Geo<double>& G, double* met, double* tab, cudaStream_t st);
 

@@ -200,21 +200,62 @@ cudaError_t residual_batch_launch(const CellInst* inst, const int2* items, int n
 
 // ---------------------------------------------------------------------------
 // Nusselt number on a wall (nusselt_promedio_y, source/mod_postproceso.f90:100-215,
-// and its vertical-wall counterpart); one thread, serial like the reference.
-// out2[0] = wall at index 1, out2[1] = wall at the last index.  With
-// `quirk` set (the reference rule) the wall-normal derivative is known only
-// on k0..k1 and reads as 0 beyond, as derivada does in the reference; the
-// vertical-wall extension evaluates it on every node the panels touch.
+// and its vertical-wall counterpart).  out2[0] = wall at index 1, out2[1] =
+// wall at the last index.  With `quirk` set (the reference rule) the
+// wall-normal derivative is known only on k0..k1 and reads as 0 beyond, as
+// derivada does in the reference; the vertical-wall extension evaluates it
+// on every node the panels touch.
+//
+// The panels' terms are evaluated in parallel (one panel per thread, in
+// chunks of kNuThreads), then one thread per wall adds them in panel order
+// with the reference's left-to-right accumulation, so the value equals the
+// serial evaluation bit for bit.  With `mon` set (the Nusselt monitor of
+// ixb_simple_converge, inside the loop graph) the wall and panel range come
+// from the monitor's fields, and thread 0 applies the monitor's stopping
+// test to the result, setting the monitor loop's condition `cond`.
 // ---------------------------------------------------------------------------
-__global__ void nusselt_kernel(const Geo<double> G, const double* __restrict__ T, const double* __restrict__ xp,
-                               const double* __restrict__ yp, int vertical, int quirk, int k0, int k1,
-                               double* __restrict__ out2) {
-  if (threadIdx.x != 0) return;
-  const double* along = vertical ? yp : xp;   // 1-based
+constexpr int kNuThreads = 256;
+
+__global__ void __launch_bounds__(kNuThreads)
+    nusselt_kernel(const Geo<double> G, const double* __restrict__ T, const double* __restrict__ xp,
+                   const double* __restrict__ yp, int vertical, int k0, int k1, double* __restrict__ out2, Ctl* mon,
+                   cudaGraphConditionalHandle cond) {
+  __shared__ double terms[2][3][kNuThreads];
+  if (mon) {
+    vertical = mon->mon_vertical;
+    k0 = mon->mon_k0;
+    k1 = mon->mon_k1;
+  }
+  const int quirk = vertical ? 0 : 1;
+  const double* along = vertical ? yp : xp;  // 1-based
   const double* across = vertical ? xp : yp;
   const int n_across = vertical ? G.mi + 1 : G.nj + 1;
   auto f = [&](int k, int l) { return vertical ? T[G.at(l, k)] : T[G.at(k, l)]; };
-  for (int wall = 0; wall < 2; ++wall) out2[wall] = nusselt_wall(f, along, across, n_across, wall, quirk, k0, k1);
+  const int npan = (k1 - k0) / 2 + 1;
+  const int tid = threadIdx.x;
+  const int my_wall = tid == 0 ? 0 : 1;  // the summing threads: 0 (wall 0) and 32 (wall 1)
+  double acc = 0.0;
+  for (int base = 0; base < npan; base += kNuThreads) {
+    const int pnl = base + tid;
+    if (pnl < npan) {
+      for (int wall = 0; wall < 2; ++wall) {
+        double t[3];
+        nusselt_panel(f, along, across, n_across, wall, quirk, k1, k0 + 2 * pnl, t);
+        terms[wall][0][tid] = t[0];
+        terms[wall][1][tid] = t[1];
+        terms[wall][2][tid] = t[2];
+      }
+    }
+    __syncthreads();
+    if (tid == 0 || tid == 32) {
+      const int cnt = min(kNuThreads, npan - base);
+      for (int q = 0; q < cnt; ++q) acc = acc + terms[my_wall][0][q] + terms[my_wall][1][q] + terms[my_wall][2][q];
+    }
+    __syncthreads();
+  }
+  if (tid == 0 || tid == 32) out2[my_wall] = -acc;
+  __syncthreads();
+  if (mon && tid == 0) ctl_monitor_step(mon, out2, cond);
 }
 
 // ---------------------------------------------------------------------------
@@ -371,8 +412,9 @@ cudaError_t launch_residual_f64(const Geo<double>& G, const double* u, const dou
 }
 
 cudaError_t launch_nusselt_f64(const Geo<double>& G, const double* T, const double* xp, const double* yp,
-                               int vertical, int k0, int k1, double* out2, cudaStream_t st) {
-  nusselt_kernel<<<1, 32, 0, st>>>(G, T, xp, yp, vertical, vertical ? 0 : 1, k0, k1, out2);
+                               int vertical, int k0, int k1, double* out2, cudaStream_t st, Ctl* mon,
+                               cudaGraphConditionalHandle cond) {
+  nusselt_kernel<<<1, kNuThreads, 0, st>>>(G, T, xp, yp, vertical, k0, k1, out2, mon, cond);
   return cudaGetLastError();
 }
 

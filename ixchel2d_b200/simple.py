@@ -113,6 +113,25 @@ class Simple2D:
         F.check(F.lib.ixb_simple_loop(self.h, C.byref(r)), "ixb_simple_loop")
         return r.as_dict()
 
+    def converge(self, k0: int, k1: int, vertical: bool = True, wall: int = 0, every: int = 1000,
+                 tol_dnu: float = 1e-8, tol_maxbo: float = 0.0, max_iters: int = 200000) -> dict:
+        """Outer iterations until the monitored wall's Nusselt number changes by
+        less than tol_dnu between evaluations `every` iterations apart (exit_code
+        3), maxbo < tol_maxbo (4) or max_iters (5), all on the device in one
+        graph launch (ixb_simple_converge).  The report adds 'nu' (both walls at
+        the last evaluation) and 'dnu' (the monitored wall's last change)."""
+        m = F.NuMonitor(vertical=int(vertical), k0=k0, k1=k1, wall=wall, every=every, reserved=0,
+                        max_iters=max_iters, tol_dnu=tol_dnu, tol_maxbo=tol_maxbo)
+        r = F.Report()
+        nu = np.zeros(2)
+        dnu = C.c_double()
+        F.check(F.lib.ixb_simple_converge(self.h, C.byref(m), C.byref(r), F.dptr(nu), C.byref(dnu)),
+                "ixb_simple_converge")
+        out = r.as_dict()
+        out["nu"] = (float(nu[0]), float(nu[1]))
+        out["dnu"] = dnu.value
+        return out
+
     def step(self) -> dict:
         r = F.Report()
         F.check(F.lib.ixb_step(self.h, C.byref(r)), "ixb_step")
