@@ -188,10 +188,13 @@ int correct(ixb_handle* h, const CtlRef& gate = CtlRef{}) {
   return IXB_OK;
 }
 
-int residual(ixb_handle* h, const CtlRef& outer = CtlRef{}) {
+// without_T: the u residual without reading T (only when Ri == 0, where its
+// buoyancy term is zero whatever T holds), so it may run beside the T sweeps
+int residual(ixb_handle* h, const CtlRef& outer = CtlRef{}, bool without_T = false) {
   Geo<double> G = make_geo(h);
-  CK(launch_residual_f64(G, h->u[h->cu], h->v[h->cv], h->T[h->cT], h->p, h->u_ant, h->fcon[0], h->flin[0],
-                         h->resu, slot(h, N_RES), h->prm.solver == IXB_SOLVER_HYBRID, h->stream, outer));
+  CK(launch_residual_f64(G, h->u[h->cu], h->v[h->cv], without_T ? nullptr : h->T[h->cT], h->p, h->u_ant,
+                         h->fcon[0], h->flin[0], h->resu, slot(h, N_RES), h->prm.solver == IXB_SOLVER_HYBRID,
+                         h->stream, outer));
   return IXB_OK;
 }
 
@@ -305,27 +308,54 @@ int add_while(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, cudaGraphCondi
 }
 
 // Capture the launches issued by `fn` on the handle's stream into `g`,
-// appended after `dep` (or as roots); returns the last captured node.
+// appended after the `ndep` nodes `deps` (or as roots); returns the last
+// captured node (the capture's tail: `fn` issues its launches in order on
+// one stream).
 template <class F>
-int capture_into(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, F fn, cudaGraphNode_t* last) {
-  CK(cudaStreamBeginCaptureToGraph(h->stream, g, dep, nullptr, dep ? 1 : 0, cudaStreamCaptureModeThreadLocal));
+int capture_into_deps(ixb_handle* h, cudaGraph_t g, const cudaGraphNode_t* deps, size_t ndep, F fn,
+                      cudaGraphNode_t* last, const cudaGraphEdgeData* edges = nullptr) {
+  CK(cudaStreamBeginCaptureToGraph(h->stream, g, deps, edges, ndep, cudaStreamCaptureModeThreadLocal));
   int st = fn();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const cudaGraphNode_t* tail = nullptr;
+  size_t ntail = 0;
+  cudaError_t ei = st == IXB_OK ? cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, nullptr, &tail, &ntail)
+                                : cudaSuccess;
+  *last = (ei == cudaSuccess && ntail == 1) ? tail[0] : nullptr;
   cudaGraph_t out = nullptr;
   cudaError_t e = cudaStreamEndCapture(h->stream, &out);
   if (st != IXB_OK) return st;
+  CK(ei);
   CK(e);
-  // find the sink node (the only node without dependents)
-  size_t nn = 0;
-  CK(cudaGraphGetNodes(g, nullptr, &nn));
-  std::vector<cudaGraphNode_t> nodes(nn);
-  CK(cudaGraphGetNodes(g, nodes.data(), &nn));
-  *last = nullptr;
-  for (auto n : nodes) {
-    size_t nd = 0;
-    CK(cudaGraphNodeGetDependentNodes(n, nullptr, &nd));
-    if (nd == 0) *last = n;
-  }
+  if (!*last) return IXB_ECUDA;  // nothing captured, or no single tail
   return IXB_OK;
+}
+template <class F>
+int capture_into(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, F fn, cudaGraphNode_t* last) {
+  return capture_into_deps(h, g, dep, dep ? 1 : 0, fn, last);
+}
+
+// End of an outer pass whose u residual ran beside the energy loop: the
+// outer test after both (ixb_ctl.cuh).
+__global__ void outer_test_kernel(Ctl* c, const double* norms, cudaGraphConditionalHandle outer,
+                                  cudaGraphConditionalHandle first_inner) {
+  ctl_outer_step(c, norms, outer, first_inner);
+}
+
+// The u residual runs on a branch of its own beside the energy loop when
+// Ri == 0: residuo_u (mod_ec_momento.f90:1107-1266) then reads u, v, p and
+// u_ant only, none of which the T sweeps write, and its buoyancy term is
+// zero.  It depends on the correction (an ordinary edge) and on the first
+// T-y sweep's launch completion (a programmatic edge: it starts once every
+// CTA of that sweep is resident, so it takes the SMs the y-line sweep leaves
+// idle instead of competing with it for SMs).  IXB_RES_BRANCH=0 keeps it
+// after the energy loop.
+bool residual_branch(const ixb_handle* h) {
+  static const bool on = [] {
+    const char* e = std::getenv("IXB_RES_BRANCH");
+    return !(e && e[0] == '0');
+  }();
+  return on && h->prm.Ri == 0.0;
 }
 
 // Inner loops in do-while form (the default): the first pass sits in the
@@ -420,9 +450,33 @@ int add_outer_loop(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, cudaGraph
       TRY(inner_loop(&last, c_pres, pres_pass));
     }
     TRY(capture_into(h, outer_body, &wn, [&]() { return correct(h, CtlRef{h->ctl_d, nrm, c_ener, 0, 0}); }, &last));
-    TRY(inner_loop(&last, c_ener, ener_pass));
-    TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
-                     &last));
+    if (dw && residual_branch(h)) {
+      // correction -> { energy loop | u residual once the first T-y sweep is resident } -> outer test
+      const cudaGraphNode_t n_corr = last;
+      cudaGraphNode_t n_ty, n_res;
+      const double* t_start = h->T[h->cT];
+      TRY(capture_into(h, outer_body, &last, [&]() { return sweep(h, EQ_TY, nullptr, false); }, &n_ty));
+      TRY(capture_into(h, outer_body, &n_ty, [&]() {
+        return sweep(h, EQ_TX, t_start, true, CtlRef{h->ctl_d, nrm, c_ener, 0, 2});
+      }, &last));
+      TRY(add_while(h, outer_body, &last, c_ener, &b, &wn));
+      TRY(capture_into(h, b, nullptr, ener_pass, &last));
+      const cudaGraphNode_t rdeps[2] = {n_corr, n_ty};
+      cudaGraphEdgeData red[2] = {};
+      red[1].from_port = cudaGraphKernelNodePortLaunchCompletion;
+      red[1].type = cudaGraphDependencyTypeProgrammatic;
+      TRY(capture_into_deps(h, outer_body, rdeps, 2, [&]() { return residual(h, CtlRef{}, true); }, &n_res, red));
+      const cudaGraphNode_t join[2] = {n_res, wn};
+      TRY(capture_into_deps(h, outer_body, join, 2, [&]() {
+        return launch_k(outer_test_kernel, 1, 1, 0, h->stream, h->ctl_d, nrm, c_outer, c_mom) == cudaSuccess
+                   ? IXB_OK : IXB_ECUDA;
+      }, &wn));
+    } else {
+      TRY(inner_loop(&last, c_ener, ener_pass));
+      TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
+                       &wn));
+    }
+    last = wn;
   }
   return IXB_OK;
 }
@@ -1113,8 +1167,11 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms) {
 int ixb_iteration_launches(ixb_handle* h, int* launches) {
   if (!h || !launches) return IXB_EINVAL;
   // p/u/v correction, u residual, and the p' reset kernel unless the graph
-  // runs the inner loops in do-while form (whose first pressure pass reads zeros)
-  int k = (h->use_graph && do_while_loops()) ? 2 : 3;
+  // runs the inner loops in do-while form (whose first pressure pass reads
+  // zeros); with the residual on its own branch, the outer test kernel
+  const bool dw = h->use_graph && do_while_loops();
+  int k = dw ? 2 : 3;
+  if (dw && residual_branch(h)) k += 1;
   for (int eq = 0; eq < EQ_COUNT; ++eq) {
     if (h->shape_tl[eq] == 0) pick_shape(h, eq);
     k += (fused_enabled() && fused_shape(eq, h->shape_tl[eq], h->shape_g[eq])) ? 1 : 2;

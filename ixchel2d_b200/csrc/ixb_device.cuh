@@ -458,7 +458,10 @@ __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v,
   R di = G.met(M_DXP, ii), dd = G.met(M_DXP, ii + 1), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   const R dxu = G.met(M_DXU, ii), dyu = G.met(M_DYU, jj);
   const int c0 = G.at(ii, jj);
-  R temp_int = fexp_i * ldg(T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ldg(T, c0);
+  // T == nullptr: the caller knows Ri == 0, so the buoyancy term is a signed
+  // zero whatever T holds and T is not read
+  const R t_e = T ? ldg(T, G.at(ii + 1, jj)) : R(0), t_c = T ? ldg(T, c0) : R(0);
+  R temp_int = fexp_i * t_e + (R(1) - fexp_i) * t_c;
   R AI = (G.t(T_CU1, ii, jj) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * dyu));
   R AD = (G.t(T_CU1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) + dmax0(-ud * dyu));
   R BS = (G.t(T_CU2, ii, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) + dmax0(vs * dxu));
