@@ -143,6 +143,27 @@ int ixb_upload_state(ixb_handle* h, const double* u, const double* v, const doub
                      const double* u_ant, const double* v_ant, const double* T_ant);
 int ixb_download_state(ixb_handle* h, double* u, double* v, double* p, double* T, double* u_ant,
                        double* v_ant, double* T_ant);
+/* Asynchronous form of ixb_download_state, for writers that run beside the
+ * next iterations (the restart and output files of main.f90:1327-1363 and
+ * mod_postproceso.f90:225-365, which the reference writes from a blocking
+ * `!$acc update self`).  On the handle's stream it snapshots the requested
+ * arrays (a device-side copy in host layout) and returns; the copies to
+ * the host run on a stream of their own, so the next ixb_step can start
+ * at once.  The host arrays must stay valid, and should be pinned
+ * (ixb_host_alloc) for the copies to overlap, until ixb_download_wait
+ * returns.  A second asynchronous download waits on the device for the
+ * first one's copies before reusing the snapshot. */
+int ixb_download_state_async(ixb_handle* h, double* u, double* v, double* p, double* T, double* u_ant,
+                             double* v_ant, double* T_ant);
+/* Block until the last ixb_download_state_async of the handle has landed in
+ * host memory.  It touches only that download's completion event, so a
+ * writer thread may call it while the handle runs other calls, as long as
+ * no new ixb_download_state_async starts meanwhile. */
+int ixb_download_wait(ixb_handle* h);
+/* Page-locked host memory for the asynchronous downloads (cudaMallocHost);
+ * no counterpart in the reference. */
+int ixb_host_alloc(size_t bytes, void** out);
+int ixb_host_free(void* p);
 /* Work arrays after the last iteration: au, av, b_o, Resu, corr_pres. */
 int ixb_download_aux(ixb_handle* h, double* au, double* av, double* b_o, double* resu, double* corr_pres);
 

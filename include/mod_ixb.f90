@@ -113,6 +113,29 @@ module ixb
        type(ixb_report), intent(out) :: rep
      end function ixb_simple_loop
 
+     integer(c_int) function ixb_download_state_async(h, u, v, p, T, u_ant, v_ant, T_ant) &
+          bind(C, name="ixb_download_state_async")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       type(c_ptr), value :: u, v, p, T, u_ant, v_ant, T_ant  ! pinned host arrays (c_loc) or c_null_ptr
+     end function ixb_download_state_async
+
+     integer(c_int) function ixb_download_wait(h) bind(C, name="ixb_download_wait")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function ixb_download_wait
+
+     integer(c_int) function ixb_host_alloc(bytes, p) bind(C, name="ixb_host_alloc")
+       import :: c_int, c_ptr, c_size_t
+       integer(c_size_t), value :: bytes
+       type(c_ptr) :: p
+     end function ixb_host_alloc
+
+     integer(c_int) function ixb_host_free(p) bind(C, name="ixb_host_free")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: p
+     end function ixb_host_free
+
      integer(c_int) function ixb_simple_converge(h, mon, rep, nu, dnu) bind(C, name="ixb_simple_converge")
        import :: c_int, c_ptr, c_double, ixb_report, ixb_nu_monitor
        type(c_ptr), value :: h

@@ -47,6 +47,10 @@ SIGNATURES = [
     ("ixb_set_sources", C.c_int, [_vp, C.c_int, _dp, _dp]),
     ("ixb_upload_state", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     ("ixb_download_state", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    ("ixb_download_state_async", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    ("ixb_download_wait", C.c_int, [_vp]),
+    ("ixb_host_alloc", C.c_int, [C.c_size_t, C.POINTER(_vp)]),
+    ("ixb_host_free", C.c_int, [_vp]),
     ("ixb_download_aux", C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     ("ixb_simple_iterations", C.c_int, [_vp, C.c_int, C.POINTER(Report)]),
     ("ixb_simple_loop", C.c_int, [_vp, C.POINTER(Report)]),

@@ -108,7 +108,7 @@ def build_driver() -> Path:
     if DRIVER.exists() and DRIVER.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return DRIVER
     tmp = DRIVER.with_name(DRIVER.name + ".tmp")
-    cmd = [HOST_CXX, *CXXFLAGS, "-o", str(tmp), *map(str, srcs), "-L", str(PKG), "-lixb",
+    cmd = [HOST_CXX, *CXXFLAGS, "-pthread", "-o", str(tmp), *map(str, srcs), "-L", str(PKG), "-lixb",
            "-Wl,-rpath,$ORIGIN"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

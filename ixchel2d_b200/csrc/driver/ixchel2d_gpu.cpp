@@ -24,7 +24,10 @@
 //   postprocesar is true, out_n<nj>m<mi>_R<Re>{u,v,p}.dat (form24/form25),
 //   out_..{u,v,p}.bin (postproceso_bin, mod_postproceso.f90:310-365) and the
 //   big-endian VTK file n<nj>m<mi>R<Re>/t_<mcdud>.vtk (postproceso_vtk,
-//   :225-300).
+//   :225-300).  The package's state leaves the device through
+//   ixb_download_state_async (a snapshot copied to pinned host buffers on the
+//   library's download stream), and a writer thread formats and writes these
+//   files while the next package runs on the GPU.
 //
 // mi and nj are compile-time parameters of the reference (mod_malla.f90:15);
 // here they are taken from the record counts of the mesh files, or from
@@ -47,6 +50,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/ixb.h"
@@ -492,9 +496,28 @@ int main(int argc, char** argv) {
   // uf, vf: velocities at the p nodes for the VTK file (main.f90:1290-1312);
   // entries the reference never writes stay 0
   std::vector<double> uf(NP, 0.0), vf(NP, 0.0);
-  auto U = [&](int ii, int jj) -> double& { return u[(size_t)(jj - 1) * mi + (ii - 1)]; };
-  auto V = [&](int ii, int jj) -> double& { return v[(size_t)(jj - 1) * (mi + 1) + (ii - 1)]; };
   auto Pn = [&](std::vector<double>& a, int ii, int jj) -> double& { return a[(size_t)(jj - 1) * (mi + 1) + (ii - 1)]; };
+
+  // pinned host buffers of the package writer (u, v, p, T in the reference's shapes)
+  struct Pinned {
+    double* p = nullptr;
+    ~Pinned() { if (p) ixb_host_free(p); }
+  } U_, V_, P_, T_;
+  const size_t nu_ = (size_t)mi * (nj + 1), nv_ = (size_t)(mi + 1) * nj;
+  ck(ixb_host_alloc(nu_ * sizeof(double), (void**)&U_.p), "ixb_host_alloc");
+  ck(ixb_host_alloc(nv_ * sizeof(double), (void**)&V_.p), "ixb_host_alloc");
+  ck(ixb_host_alloc(NP * sizeof(double), (void**)&P_.p), "ixb_host_alloc");
+  ck(ixb_host_alloc(NP * sizeof(double), (void**)&T_.p), "ixb_host_alloc");
+  auto WU = [&](int ii, int jj) -> double { return U_.p[(size_t)(jj - 1) * mi + (ii - 1)]; };
+  auto WV = [&](int ii, int jj) -> double { return V_.p[(size_t)(jj - 1) * (mi + 1) + (ii - 1)]; };
+  auto WP = [&](int ii, int jj) -> double { return P_.p[(size_t)(jj - 1) * (mi + 1) + (ii - 1)]; };
+  auto WT = [&](int ii, int jj) -> double { return T_.p[(size_t)(jj - 1) * (mi + 1) + (ii - 1)]; };
+  std::thread writer;
+  std::string writer_error;
+  auto join_writer = [&]() {
+    if (writer.joinable()) writer.join();
+    if (!writer_error.empty()) die(3, writer_error);
+  };
 
   int itera = 0;
   double nusselt0 = 0.0, nusselt1 = 0.0, maxbo = 0.0, residuo = 0.0;
@@ -540,23 +563,13 @@ int main(int argc, char** argv) {
     const int decima =
         q / 10 > 0 ? (itera_total - millar * 1000 * q - centena * 100 * q - decena * 10 * q - unidad * q) / (q / 10)
                    : 0;
-    ck(ixb_download_state(h, u.data(), v.data(), p.data(), T.data(), nullptr, nullptr, nullptr),
-       "ixb_download_state");
-    for (int jj = 2; jj <= nj; ++jj) {
-      for (int ii = 2; ii <= mi; ++ii) Pn(uf, ii, jj) = (U(ii, jj) + U(ii - 1, jj)) / 2.0;
-      Pn(vf, 1, jj) = V(1, jj);
-      Pn(vf, mi + 1, jj) = V(mi + 1, jj);
-    }
-    for (int ii = 2; ii <= mi; ++ii)
-      for (int jj = 2; jj <= nj; ++jj) Pn(vf, ii, jj) = (V(ii, jj) + V(ii, jj - 1)) / 2.0;
-    for (int jj = 1; jj <= nj + 1; ++jj) {
-      Pn(uf, 1, jj) = U(1, jj);
-      Pn(uf, mi + 1, jj) = U(mi, jj);
-    }
-    for (int ii = 1; ii <= mi + 1; ++ii) {
-      Pn(vf, ii, 1) = V(ii, 1);
-      Pn(vf, ii, nj + 1) = V(ii, nj);
-    }
+    // the package's state goes to the writer: a snapshot on the device, copied
+    // to pinned host buffers on the library's download stream while the next
+    // package runs; the writer thread formats and writes the files once the
+    // copies have landed.  The previous writer is joined first: it reads the
+    // same host buffers.
+    join_writer();
+    ck(ixb_download_state_async(h, U_.p, V_.p, P_.p, T_.p, nullptr, nullptr, nullptr), "ixb_download_state_async");
     if (say) {
       std::printf(" itera_total=%s\n", fi(itera_total).c_str());
       std::printf(" N_Izq=%s, N_Der=%s\n", fmt_d23_15(nusselt0).c_str(), fmt_d23_15(nusselt1).c_str());
@@ -564,23 +577,48 @@ int main(int argc, char** argv) {
       std::printf(" Res_T=%s, Res_v=%s\n  \n", fmt_d23_15(0.0).c_str(), fmt_d23_15(0.0).c_str());
       std::fflush(stdout);
     }
-    if (P.postprocesar) {
+    writer = std::thread([&, itera_total, millar, centena, decena, unidad, decima]() {
+      if (ixb_download_wait(h) != IXB_OK) {
+        writer_error = "ixb_download_wait failed";
+        return;
+      }
+      for (int jj = 2; jj <= nj; ++jj) {
+        for (int ii = 2; ii <= mi; ++ii) Pn(uf, ii, jj) = (WU(ii, jj) + WU(ii - 1, jj)) / 2.0;
+        Pn(vf, 1, jj) = WV(1, jj);
+        Pn(vf, mi + 1, jj) = WV(mi + 1, jj);
+      }
+      for (int ii = 2; ii <= mi; ++ii)
+        for (int jj = 2; jj <= nj; ++jj) Pn(vf, ii, jj) = (WV(ii, jj) + WV(ii, jj - 1)) / 2.0;
+      for (int jj = 1; jj <= nj + 1; ++jj) {
+        Pn(uf, 1, jj) = WU(1, jj);
+        Pn(uf, mi + 1, jj) = WU(mi, jj);
+      }
+      for (int ii = 1; ii <= mi + 1; ++ii) {
+        Pn(vf, ii, 1) = WV(ii, 1);
+        Pn(vf, ii, nj + 1) = WV(ii, nj);
+      }
+      if (!P.postprocesar) return;
       const std::string fu = "out_" + tag + "u.dat", fv = "out_" + tag + "v.dat", fp = "out_" + tag + "p.dat";
-      const int st = ixb_write_state_files(fu.c_str(), fv.c_str(), fp.c_str(), mi, nj, xu.data(), yv.data(), xp.data(),
-                                           yp.data(), u.data(), v.data(), T.data(), p.data(), placa_min, placa_max,
+      const int st = ixb_write_state_files(fu.c_str(), fv.c_str(), fp.c_str(), mi, nj, xu.data(), yv.data(),
+                                           xp.data(), yp.data(), U_.p, V_.p, T_.p, P_.p, placa_min, placa_max,
                                            itera_total, ao);
-      if (st != IXB_OK) die(3, std::string("writing out_*.dat: ") + ixb_strerror(st));
+      if (st != IXB_OK) {
+        writer_error = std::string("writing out_*.dat: ") + ixb_strerror(st);
+        return;
+      }
       // postproceso_bin: unformatted stream records, native byte order
       std::string bu, bv, bp;
       for (int jj = 1; jj <= nj + 1; ++jj)
-        for (int ii = 1; ii <= mi; ++ii) put_doubles(&bu, xu[ii - 1], yp[jj - 1], U(ii, jj));
+        for (int ii = 1; ii <= mi; ++ii) put_doubles(&bu, xu[ii - 1], yp[jj - 1], WU(ii, jj));
       for (int jj = 1; jj <= nj; ++jj)
-        for (int ii = 1; ii <= mi + 1; ++ii) put_doubles(&bv, xp[ii - 1], yv[jj - 1], V(ii, jj));
+        for (int ii = 1; ii <= mi + 1; ++ii) put_doubles(&bv, xp[ii - 1], yv[jj - 1], WV(ii, jj));
       for (int jj = 1; jj <= nj + 1; ++jj)
-        for (int ii = 1; ii <= mi + 1; ++ii) put_doubles(&bp, Pn(T, ii, jj), Pn(p, ii, jj));
+        for (int ii = 1; ii <= mi + 1; ++ii) put_doubles(&bp, WT(ii, jj), WP(ii, jj));
       if (!write_file("out_" + tag + "u.bin", bu) || !write_file("out_" + tag + "v.bin", bv) ||
-          !write_file("out_" + tag + "p.bin", bp))
-        die(3, "cannot write out_*.bin");
+          !write_file("out_" + tag + "p.bin", bp)) {
+        writer_error = "cannot write out_*.bin";
+        return;
+      }
       // postproceso_vtk: legacy VTK structured grid, big-endian binary
       const std::string npts = fi((int64_t)(mi + 1) * (nj + 1));
       std::string vtk;
@@ -595,9 +633,9 @@ int main(int argc, char** argv) {
         }
       vtk += "\nPOINT_DATA " + npts;
       vtk += "SCALARS PRESS float\nLOOKUP_TABLE default\n";
-      for (size_t k = 0; k < NP; ++k) put_be_float(&vtk, p[k]);
+      for (size_t k = 0; k < NP; ++k) put_be_float(&vtk, P_.p[k]);
       vtk += "\nSCALARS TEMPER float\nLOOKUP_TABLE default\n";
-      for (size_t k = 0; k < NP; ++k) put_be_float(&vtk, T[k]);
+      for (size_t k = 0; k < NP; ++k) put_be_float(&vtk, T_.p[k]);
       vtk += "\nVECTORS VELOCITY float\n";
       for (size_t k = 0; k < NP; ++k) {
         put_be_float(&vtk, uf[k]);
@@ -606,9 +644,11 @@ int main(int argc, char** argv) {
       }
       const std::string vname = folder + "/t_" + std::string{digit(millar), digit(centena), digit(decena),
                                                              digit(unidad), digit(decima)} + ".vtk";
-      if (!write_file(vname, vtk)) die(3, "cannot write " + vname);
-    }
+      if (!write_file(vname, vtk)) writer_error = "cannot write " + vname;
+    });
   }
+  join_writer();
+  if (!writer_error.empty()) die(3, writer_error);
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   ck(ixb_destroy(h), "ixb_destroy");
   // run summary (also under --quiet): time steps, SIMPLE iterations, the

@@ -167,7 +167,7 @@ SweepIO<double> sweep_io(ixb_handle* h, int eq, const double* prev, bool with_no
 // zero_input the swept field is read as zeros (the handle's zero field),
 // whatever its current buffer holds.
 int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm, const CtlRef& ctl = CtlRef{},
-          bool zero_input = false) {
+          bool zero_input = false, const ResidIO* rio = nullptr) {
   Geo<double> G = make_geo(h);
   if (h->shape_tl[eq] == 0) pick_shape(h, eq);
   SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), h->shape_tl[eq], h->shape_g[eq]);
@@ -177,8 +177,20 @@ int sweep(ixb_handle* h, int eq, const double* prev, bool with_norm, const CtlRe
     if (eq == EQ_PY || eq == EQ_PX) io.pc = h->zero;
   }
   const StageBuf stage{h->stage, h->stage_stride, h->stage_P};
-  CK(launch_sweep_f64(eq, solver_form(h), s, G, io, stage, h->stream, ctl));
+  CK(launch_sweep_f64(eq, solver_form(h), s, G, io, stage, h->stream, ctl, rio));
   return IXB_OK;
+}
+
+// In the graph's do-while form the u residual and the outer test ride on
+// every T-x sweep of the energy loop when that sweep runs fused: the
+// residual of u-row jj reads T on row jj only, the line the sweep's CTA has
+// just solved, so the separate residual kernel and its launch go away, and
+// the last energy pass's values are the ones the outer test reads.
+bool do_while_loops();
+bool residual_in_tx(ixb_handle* h) {
+  if (!h->use_graph || !do_while_loops()) return false;
+  if (h->shape_tl[EQ_TX] == 0) pick_shape(h, EQ_TX);
+  return fused_enabled() && fused_shape(EQ_TX, h->shape_tl[EQ_TX], h->shape_g[EQ_TX]);
 }
 
 int correct(ixb_handle* h, const CtlRef& gate = CtlRef{}) {
@@ -188,13 +200,10 @@ int correct(ixb_handle* h, const CtlRef& gate = CtlRef{}) {
   return IXB_OK;
 }
 
-// without_T: the u residual without reading T (only when Ri == 0, where its
-// buoyancy term is zero whatever T holds), so it may run beside the T sweeps
-int residual(ixb_handle* h, const CtlRef& outer = CtlRef{}, bool without_T = false) {
+int residual(ixb_handle* h, const CtlRef& outer = CtlRef{}) {
   Geo<double> G = make_geo(h);
-  CK(launch_residual_f64(G, h->u[h->cu], h->v[h->cv], without_T ? nullptr : h->T[h->cT], h->p, h->u_ant,
-                         h->fcon[0], h->flin[0], h->resu, slot(h, N_RES), h->prm.solver == IXB_SOLVER_HYBRID,
-                         h->stream, outer));
+  CK(launch_residual_f64(G, h->u[h->cu], h->v[h->cv], h->T[h->cT], h->p, h->u_ant, h->fcon[0], h->flin[0],
+                         h->resu, slot(h, N_RES), h->prm.solver == IXB_SOLVER_HYBRID, h->stream, outer));
   return IXB_OK;
 }
 
@@ -335,29 +344,6 @@ int capture_into(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, F fn, cudaG
   return capture_into_deps(h, g, dep, dep ? 1 : 0, fn, last);
 }
 
-// End of an outer pass whose u residual ran beside the energy loop: the
-// outer test after both (ixb_ctl.cuh).
-__global__ void outer_test_kernel(Ctl* c, const double* norms, cudaGraphConditionalHandle outer,
-                                  cudaGraphConditionalHandle first_inner) {
-  ctl_outer_step(c, norms, outer, first_inner);
-}
-
-// The u residual runs on a branch of its own beside the energy loop when
-// Ri == 0: residuo_u (mod_ec_momento.f90:1107-1266) then reads u, v, p and
-// u_ant only, none of which the T sweeps write, and its buoyancy term is
-// zero.  It depends on the correction (an ordinary edge) and on the first
-// T-y sweep's launch completion (a programmatic edge: it starts once every
-// CTA of that sweep is resident, so it takes the SMs the y-line sweep leaves
-// idle instead of competing with it for SMs).  IXB_RES_BRANCH=0 keeps it
-// after the energy loop.
-bool residual_branch(const ixb_handle* h) {
-  static const bool on = [] {
-    const char* e = std::getenv("IXB_RES_BRANCH");
-    return !(e && e[0] == '0');
-  }();
-  return on && h->prm.Ri == 0.0;
-}
-
 // Inner loops in do-while form (the default): the first pass sits in the
 // outer body, so the WHILE node launches its body only for further passes.
 // With one pass per loop that took an outer iteration at 701x301 from 147
@@ -411,10 +397,13 @@ int add_outer_loop(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, cudaGraph
       TRY(sweep(h, EQ_PX, pc_start, true, CtlRef{h->ctl_d, nrm, c_pres, 0, 1}));
       return IXB_OK;
     };
+    const bool res_tx = residual_in_tx(h);
+    const ResidIO rio{h->u[h->cu], h->v[h->cv], h->p, h->u_ant, h->fcon[0], h->flin[0], h->resu, slot(h, N_RES),
+                      CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}};
     const auto ener_pass = [&]() -> int {
       const double* t_start = h->T[h->cT];
       TRY(sweep(h, EQ_TY, nullptr, false));
-      TRY(sweep(h, EQ_TX, t_start, true, CtlRef{h->ctl_d, nrm, c_ener, 0, 2}));
+      TRY(sweep(h, EQ_TX, t_start, true, CtlRef{h->ctl_d, nrm, c_ener, 0, 2}, false, res_tx ? &rio : nullptr));
       return IXB_OK;
     };
     const bool dw = do_while_loops();
@@ -450,32 +439,10 @@ int add_outer_loop(ixb_handle* h, cudaGraph_t g, cudaGraphNode_t* dep, cudaGraph
       TRY(inner_loop(&last, c_pres, pres_pass));
     }
     TRY(capture_into(h, outer_body, &wn, [&]() { return correct(h, CtlRef{h->ctl_d, nrm, c_ener, 0, 0}); }, &last));
-    if (dw && residual_branch(h)) {
-      // correction -> { energy loop | u residual once the first T-y sweep is resident } -> outer test
-      const cudaGraphNode_t n_corr = last;
-      cudaGraphNode_t n_ty, n_res;
-      const double* t_start = h->T[h->cT];
-      TRY(capture_into(h, outer_body, &last, [&]() { return sweep(h, EQ_TY, nullptr, false); }, &n_ty));
-      TRY(capture_into(h, outer_body, &n_ty, [&]() {
-        return sweep(h, EQ_TX, t_start, true, CtlRef{h->ctl_d, nrm, c_ener, 0, 2});
-      }, &last));
-      TRY(add_while(h, outer_body, &last, c_ener, &b, &wn));
-      TRY(capture_into(h, b, nullptr, ener_pass, &last));
-      const cudaGraphNode_t rdeps[2] = {n_corr, n_ty};
-      cudaGraphEdgeData red[2] = {};
-      red[1].from_port = cudaGraphKernelNodePortLaunchCompletion;
-      red[1].type = cudaGraphDependencyTypeProgrammatic;
-      TRY(capture_into_deps(h, outer_body, rdeps, 2, [&]() { return residual(h, CtlRef{}, true); }, &n_res, red));
-      const cudaGraphNode_t join[2] = {n_res, wn};
-      TRY(capture_into_deps(h, outer_body, join, 2, [&]() {
-        return launch_k(outer_test_kernel, 1, 1, 0, h->stream, h->ctl_d, nrm, c_outer, c_mom) == cudaSuccess
-                   ? IXB_OK : IXB_ECUDA;
-      }, &wn));
-    } else {
-      TRY(inner_loop(&last, c_ener, ener_pass));
+    TRY(inner_loop(&last, c_ener, ener_pass));
+    if (!res_tx)
       TRY(capture_into(h, outer_body, &wn, [&]() { return residual(h, CtlRef{h->ctl_d, nrm, c_outer, c_mom, 0}); },
                        &wn));
-    }
     last = wn;
   }
   return IXB_OK;
@@ -624,6 +591,11 @@ void free_all(ixb_handle* h) {
   if (h->stage) cudaFree(h->stage);
   if (h->adj_pool) cudaFree(h->adj_pool);
   if (h->xfer) cudaFree(h->xfer);
+  if (h->dl_stream) cudaStreamSynchronize(h->dl_stream);
+  if (h->snap) cudaFree(h->snap);
+  if (h->snap_ev) cudaEventDestroy(h->snap_ev);
+  if (h->dl_ev) cudaEventDestroy(h->dl_ev);
+  if (h->dl_stream) cudaStreamDestroy(h->dl_stream);
   if (h->bc) cudaFree(h->bc);
   if (h->counters) cudaFree(h->counters);
   if (h->ctl_d) cudaFree(h->ctl_d);
@@ -655,8 +627,9 @@ __global__ void xfer_kernel(XferSet s, double* xfer, int LD, int to_padded) {
   }
 }
 
-// host arrays (NULL: skipped) <-> the state fields
-int xfer_state(ixb_handle* h, const std::array<double*, 7>& pad, const std::array<double*, 7>& host, bool upload) {
+// The transfer set of the state arrays whose host pointer is not NULL, in
+// the order u, v, p, T, u_ant, v_ant, T_ant, packed one after the other.
+XferSet make_xfer_set(const ixb_handle* h, const std::array<double*, 7>& pad, const std::array<double*, 7>& host) {
   const int mi = h->mi, nj = h->nj;
   const int rows[7] = {mi, mi + 1, mi + 1, mi + 1, mi, mi + 1, mi + 1};
   const int cols[7] = {nj + 1, nj, nj + 1, nj + 1, nj + 1, nj, nj + 1};
@@ -668,6 +641,13 @@ int xfer_state(ixb_handle* h, const std::array<double*, 7>& pad, const std::arra
     off += (size_t)rows[k] * cols[k];
     ++s.n;
   }
+  return s;
+}
+
+// host arrays (NULL: skipped) <-> the state fields
+int xfer_state(ixb_handle* h, const std::array<double*, 7>& pad, const std::array<double*, 7>& host, bool upload) {
+  const int mi = h->mi, nj = h->nj;
+  const XferSet s = make_xfer_set(h, pad, host);
   if (s.n == 0) return IXB_OK;
   if (!h->xfer) {  // allocated on the first transfer (7 host-shaped arrays)
     CK(cudaStreamSynchronize(h->stream));
@@ -960,6 +940,65 @@ int ixb_download_state(ixb_handle* h, double* u, double* v, double* p, double* T
                     {u, v, p, T, u_ant, v_ant, T_ant}, false);
 }
 
+int ixb_download_state_async(ixb_handle* h, double* u, double* v, double* p, double* T, double* u_ant,
+                             double* v_ant, double* T_ant) {
+  if (!h) return IXB_EINVAL;
+  const std::array<double*, 7> host = {u, v, p, T, u_ant, v_ant, T_ant};
+  const XferSet s = make_xfer_set(h, {h->u[h->cu], h->v[h->cv], h->p, h->T[h->cT], h->u_ant, h->v_ant, h->T_ant},
+                                  host);
+  if (s.n == 0) return IXB_OK;
+  if (!h->snap) {  // first use: the snapshot buffer, the download stream and its events
+    CK(cudaStreamSynchronize(h->stream));
+    if (cudaMalloc(&h->snap, (size_t)7 * (h->mi + 1) * (h->nj + 1) * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      h->snap = nullptr;
+      return IXB_ENOMEM;
+    }
+    CK(cudaStreamCreateWithFlags(&h->dl_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->snap_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->dl_ev, cudaEventDisableTiming));
+  }
+  // the snapshot buffer is reused once the previous download has read it
+  if (h->dl_pending) CK(cudaStreamWaitEvent(h->stream, h->dl_ev, 0));
+  const dim3 grid(148 * 2, s.n);
+  xfer_kernel<<<grid, 256, 0, h->stream>>>(s, h->snap, h->LD, 0);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->snap_ev, h->stream));
+  CK(cudaStreamWaitEvent(h->dl_stream, h->snap_ev, 0));
+  for (int k = 0, q = 0; k < 7; ++k) {
+    if (!host[k]) continue;
+    CK(cudaMemcpyAsync(host[k], h->snap + s.off[q], (size_t)s.rows[q] * s.cols[q] * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->dl_stream));
+    ++q;
+  }
+  CK(cudaEventRecord(h->dl_ev, h->dl_stream));
+  h->dl_pending = true;
+  return IXB_OK;
+}
+
+int ixb_download_wait(ixb_handle* h) {
+  if (!h) return IXB_EINVAL;
+  if (!h->dl_pending) return IXB_OK;
+  CK(cudaEventSynchronize(h->dl_ev));
+  return IXB_OK;
+}
+
+int ixb_host_alloc(size_t bytes, void** out) {
+  if (!out || bytes == 0) return IXB_EINVAL;
+  *out = nullptr;
+  if (cudaMallocHost(out, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return IXB_ENOMEM;
+  }
+  return IXB_OK;
+}
+
+int ixb_host_free(void* p) {
+  if (p && cudaFreeHost(p) != cudaSuccess) return IXB_ECUDA;
+  return IXB_OK;
+}
+
 int ixb_download_aux(ixb_handle* h, double* au, double* av, double* b_o, double* resu, double* corr_pres) {
   if (!h) return IXB_EINVAL;
   const int mi = h->mi, nj = h->nj;
@@ -1167,11 +1206,9 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms) {
 int ixb_iteration_launches(ixb_handle* h, int* launches) {
   if (!h || !launches) return IXB_EINVAL;
   // p/u/v correction, u residual, and the p' reset kernel unless the graph
-  // runs the inner loops in do-while form (whose first pressure pass reads
-  // zeros); with the residual on its own branch, the outer test kernel
-  const bool dw = h->use_graph && do_while_loops();
-  int k = dw ? 2 : 3;
-  if (dw && residual_branch(h)) k += 1;
+  // runs the inner loops in do-while form (whose first pressure pass reads zeros)
+  int k = (h->use_graph && do_while_loops()) ? 2 : 3;
+  if (residual_in_tx(h)) k -= 1;  // the u residual rides on the fused T-x sweep
   for (int eq = 0; eq < EQ_COUNT; ++eq) {
     if (h->shape_tl[eq] == 0) pick_shape(h, eq);
     k += (fused_enabled() && fused_shape(eq, h->shape_tl[eq], h->shape_g[eq])) ? 1 : 2;

@@ -14,7 +14,8 @@ __device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
 
 // End of an inner pass.  which: 0 momentum (||dv|| vs conv_u), 1 pressure
 // (||dp'|| vs conv_p, with maxbo), 2 energy (||dT|| vs conv_t).
-static __device__ void ctl_inner_step(Ctl* c, const double* norms, int which, cudaGraphConditionalHandle inner) {
+// Returns whether the loop runs another pass.
+static __device__ bool ctl_inner_step(Ctl* c, const double* norms, int which, cudaGraphConditionalHandle inner) {
   double err, conv;
   if (which == 0) { err = norms[N_DV]; conv = c->conv_u; c->err_u = err; c->n_momen++; }
   else if (which == 1) { err = norms[N_DP]; conv = c->conv_p; c->err_p = err; c->maxbo = norms[N_BO]; c->n_pres++; }
@@ -32,6 +33,7 @@ static __device__ void ctl_inner_step(Ctl* c, const double* norms, int which, cu
   if (again && (long long)c->inner_done >= (long long)c->iter_ecuaci_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
   if (!again) c->inner_done = 0;  // the next inner loop counts from zero
   cudaGraphSetConditional(inner, again ? 1u : 0u);
+  return again;
 }
 
 // Start of an inner loop: after a non-finite stop, the later inner loops of

@@ -436,7 +436,10 @@ __device__ __forceinline__ Row<R> assemble_py(const Geo<R>& G, const SweepIO<F>&
 // uniform gamma the reference's different south numerator (:1208) has the
 // same value as in ensambla_velu_x, so it shares the u tables.
 // ---------------------------------------------------------------------------
-template <bool FAST, class R>
+// T_WRITTEN: T was written earlier in the calling kernel (a fused T-x sweep
+// evaluating the residual of the rows it solved), so it is read with
+// ordinary coherent loads instead of the read-only path.
+template <bool FAST, class R, bool T_WRITTEN = false>
 __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v, const R* T, const R* p,
                                         const R* u_ant, const R* fcon, const R* flin, int ii, int jj) {
   const R fexu_i = G.met(M_FEXU, ii), fexu_m = G.met(M_FEXU, ii - 1);
@@ -458,9 +461,8 @@ __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v,
   R di = G.met(M_DXP, ii), dd = G.met(M_DXP, ii + 1), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   const R dxu = G.met(M_DXU, ii), dyu = G.met(M_DYU, jj);
   const int c0 = G.at(ii, jj);
-  // T == nullptr: the caller knows Ri == 0, so the buoyancy term is a signed
-  // zero whatever T holds and T is not read
-  const R t_e = T ? ldg(T, G.at(ii + 1, jj)) : R(0), t_c = T ? ldg(T, c0) : R(0);
+  const R t_e = T_WRITTEN ? T[G.at(ii + 1, jj)] : ldg(T, G.at(ii + 1, jj));
+  const R t_c = T_WRITTEN ? T[c0] : ldg(T, c0);
   R temp_int = fexp_i * t_e + (R(1) - fexp_i) * t_c;
   R AI = (G.t(T_CU1, ii, jj) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * dyu));
   R AD = (G.t(T_CU1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) + dmax0(-ud * dyu));

@@ -101,6 +101,12 @@ struct ixb_handle {
   int nsm = 148;
   // adjoint workspace (ixb_adjoint_energy), allocated on first use
   double* xfer = nullptr;  // seven host-shaped (column-major, unpadded) state arrays: the state transfers' staging, allocated on the first transfer
+  // asynchronous downloads (ixb_download_state_async): a snapshot of the
+  // state in host layout, copied to the host on a stream of its own
+  double* snap = nullptr;
+  cudaStream_t dl_stream = nullptr;
+  cudaEvent_t snap_ev = nullptr, dl_ev = nullptr;
+  bool dl_pending = false;
   double* adj_pool = nullptr;
   size_t adj_size = 0;
 };

@@ -149,6 +149,17 @@ cudaError_t assemble_batch_launch(const void* inst, const int2* items, int nitem
                                   const BatchNorm& bn, cudaStream_t st);
 
 // line solve of a sweep (ixb_solve.cu): staged rows in, field out
+// The u residual (residuo_u, mod_ec_momento.f90:1107-1266, main.f90:1169-1199)
+// of the rows a fused T-x sweep has just solved, its norm, and the outer
+// test after the energy loop's last pass (graph only; resu null: off).  The
+// residual of u-row jj reads T on row jj only, which is that sweep's line jj.
+struct ResidIO {
+  const double *u, *v, *p, *u_ant, *fcon, *flin;
+  double* resu;
+  NormSlot ns;
+  CtlRef outer;
+};
+
 struct SolveIO {
   const void* coef;     // a | b | c | d, `stride` elements each
   size_t stride;
@@ -160,6 +171,7 @@ struct SolveIO {
   CtlRef ctl;           // inner-loop test after nrm0 (graph only)
   int LD;
   int m, mp;            // chunk rows per thread, padded pitch
+  ResidIO res;          // fused T-x sweeps only
 };
 // Launch shapes of the line sweeps (lines per CTA, threads per line); every
 // sweep runs in one of them (ixb_set_sweep_shape, the autotuners).  The
@@ -233,9 +245,10 @@ cudaError_t residual_batch_launch(const CellInst* inst, const int2* items, int n
                                   const BatchNorm& bn, int fast, cudaStream_t st);
 
 // kernel launchers (ixb_kernels.cu); return cudaError_t
+// rio (T-x in a fused shape only): the u residual rides on the sweep
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
                              const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st,
-                             const CtlRef& ctl = CtlRef{});
+                             const CtlRef& ctl = CtlRef{}, const ResidIO* rio = nullptr);
 cudaError_t launch_correct_f64(const Geo<double>& G, double* u, double* v, double* p, const double* pc,
                                const double* au, const double* av, int fast, cudaStream_t st,
                                const CtlRef& gate = CtlRef{});

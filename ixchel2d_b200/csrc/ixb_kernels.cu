@@ -347,13 +347,16 @@ cudaError_t sweep_set_smem_limits() {
 // line in `buf`, then the line solve writes the field.
 cudaError_t launch_sweep_f64(int eq, int solver, const SweepShape& s, const Geo<double>& G,
                              const SweepIO<double>& io, const StageBuf& buf, cudaStream_t st,
-                             const CtlRef& ctl) {
+                             const CtlRef& ctl, const ResidIO* rio) {
   cudaError_t e;
-  if (fused_enabled() && fused_shape(eq, s.tl, s.g)) {
+  const bool fused = fused_enabled() && fused_shape(eq, s.tl, s.g);
+  if (rio && (eq != EQ_TX || !fused || !io.nrm0.partials)) return cudaErrorInvalidValue;
+  if (fused) {
     // assembly and solve in one kernel where the launch shape allows it
     SolveIO so{};
     so.in = io.in; so.out = io.out; so.prev = io.prev; so.nrm0 = io.nrm0; so.ctl = ctl;
     so.LD = G.LD; so.m = s.m; so.mp = s.mp;
+    if (rio) so.res = *rio;
     auto fx = [&](auto solver_c) -> cudaError_t {
       constexpr int SV = decltype(solver_c)::value;
       IXB_EQ_SWITCH(return fused_launch<E_, SV>(s, G, io, so, st))

@@ -56,6 +56,38 @@ static __device__ bool finish_norm(const NormSlot& ns, double block_total) {
   return is_last != 0;
 }
 
+// Two norms of one launch with a single arrival counter (a's): every CTA
+// publishes both partials, and the last to arrive sums each in CTA order
+// and stores both results before returning true (one counter round trip
+// instead of two, and both norms final together).
+static __device__ bool finish_norm2(const NormSlot& a, double total_a, const NormSlot& b, double total_b) {
+  __shared__ int is_last;
+  if (threadIdx.x == 0) {
+    a.partials[blockIdx.x] = total_a;
+    b.partials[blockIdx.x] = total_b;
+    __threadfence();
+    const unsigned prev = atomicAdd(a.counter, 1u);
+    is_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (is_last) {
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+      sa += __ldcg(a.partials + i);
+      sb += __ldcg(b.partials + i);
+    }
+    sa = block_sum(sa);
+    sb = block_sum(sb);
+    if (threadIdx.x == 0) {
+      *a.result = sqrt(sa);
+      *b.result = sqrt(sb);
+      *a.counter = 0u;
+    }
+  }
+  return is_last != 0;
+}
+
 // Per-instance norms of a batched launch.  Work item `item` (of instance
 // `inst`, whose items are first .. first+count-1) publishes its partial;
 // the last item of the instance to arrive sums the instance's partials in

@@ -311,6 +311,45 @@ __global__ void __launch_bounds__(TL * G)
   __syncthreads();
   const double acc = solve_lines<S, EqIsX<EQ>::value, ST::DC, SOLVER == IXB_SOLVER_EXACT, TL, G, M>(
       sm, so, n, line_lo, line_hi, nfull, L0);
+  if constexpr (EQ == EQ_TX) {
+    if (so.res.resu) {
+      // u residual of row jj = L0 (TL = 1 for x-sweeps), whose T this CTA has just written
+      __syncthreads();
+      double acc_res = 0.0;
+      if (L0 >= 2 && L0 <= G_.nj) {
+        // cells ii = 2..mi-1 of the row, m per thread (G*m >= mi+1 rows of the line); with a
+        // compile-time m the cells' loads are independent and issued together
+        const ResidIO& r = so.res;
+#pragma unroll
+        for (int k = 0; k < (M > 0 ? M : m); ++k) {
+          const int ii = 2 + (int)threadIdx.x + k * G;
+          const bool valid = ii <= G_.mi - 1;
+          const double v = residual_u<SOLVER != IXB_SOLVER_EXACT, double, true>(
+              G_, r.u, r.v, so.out, r.p, r.u_ant, r.fcon, r.flin, valid ? ii : G_.mi - 1, L0);
+          if (valid) {
+            r.resu[G_.at(ii, L0)] = v;
+            acc_res += v * v;
+          }
+        }
+      }
+      const double s0 = block_sum(acc);
+      const double s1 = block_sum(acc_res);
+      // the energy test, then (after the loop's last pass) the outer test
+      if (finish_norm2(so.nrm0, s0, so.res.ns, s1) && so.ctl.ctl && threadIdx.x == 0) {
+        const bool again = ctl_inner_step(so.ctl.ctl, so.ctl.norms, so.ctl.which, so.ctl.cond);
+        if (!again) ctl_outer_step(so.res.outer.ctl, so.res.outer.norms, so.res.outer.cond, so.res.outer.cond2);
+      }
+      return;
+    }
+  }
+  if (io.nrm1.partials && so.nrm0.partials) {
+    // p'-x: ||b_o|| and ||dp'|| with one arrival counter, then the pressure test
+    const double s0 = block_sum(acc);
+    const double s1 = block_sum(acc_bo);
+    if (finish_norm2(so.nrm0, s0, io.nrm1, s1) && so.ctl.ctl && threadIdx.x == 0)
+      ctl_inner_step(so.ctl.ctl, so.ctl.norms, so.ctl.which, so.ctl.cond);
+    return;
+  }
   if (io.nrm1.partials) finish_norm(io.nrm1, block_sum(acc_bo));
   if (so.nrm0.partials) {
     const bool last = finish_norm(so.nrm0, block_sum(acc));

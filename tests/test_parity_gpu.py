@@ -132,18 +132,19 @@ def test_iteration_launch_count():
     if os.environ.get("IXB_SPLIT") == "1":
         pytest.skip("fused sweeps switched off")
     g = Simple2D.from_case(cases.lid_driven_mixed(45, 29))
-    # the correction, the residual and (Ri == 0: the residual runs beside the
-    # energy loop) the outer test; the graph's do-while pressure loop starts
-    # from the zero field: no p' reset kernel
-    extra = 2 + (0 if os.environ.get("IXB_RES_BRANCH") == "0" else 1)
+    # plus the correction and the residual (the graph's do-while pressure
+    # loop starts from the zero field: no p' reset kernel); the residual
+    # rides on the T-x sweep when that sweep runs fused
     for k in range(8):
         g.set_sweep_shape(k, 1, 128)  # x-sweeps fused, y-sweeps two kernels
-    assert g.iteration_launches() == 4 * 1 + 4 * 2 + extra
+    assert g.iteration_launches() == 4 * 1 + 4 * 2 + 1
     for k in range(8):
         g.set_sweep_shape(k, 4, 64)  # y-sweeps fused, x-sweeps two kernels
-    assert g.iteration_launches() == 4 * 2 + 4 * 1 + extra
+    assert g.iteration_launches() == 4 * 2 + 4 * 1 + 2
     g.set_sweep_shape(1, 1, 256)
-    assert g.iteration_launches() == 3 * 2 + 5 * 1 + extra
+    assert g.iteration_launches() == 3 * 2 + 5 * 1 + 2
+    g.set_sweep_shape(7, 1, 256)  # T-x fused as well
+    assert g.iteration_launches() == 2 * 2 + 6 * 1 + 1
 
 
 _SPLIT_CHILD = """
@@ -163,8 +164,7 @@ for solver, iters in ((F.SOLVER_EXACT, 40), (F.SOLVER_HYBRID, 200)):
         o = O.OracleCase(case, solver=solver)
         for k in range(8):
             g.set_sweep_shape(k, *shape)
-        # 8 sweeps x 2, correction, residual (+ the outer test with the residual on its own branch)
-        assert g.iteration_launches() == 18 + (os.environ.get("IXB_RES_BRANCH") != "0"), g.iteration_launches()
+        assert g.iteration_launches() == 18, g.iteration_launches()
         g.iterations(iters)
         o.iterations(iters)
         gs, os_ = g.download(), o.get_state()
@@ -425,9 +425,9 @@ def test_tridiag_batch(layout, n, nsys, dtype, solver):
     assert F.lib.ixb_tridiag_status() == F.OK  # no bounded copy wait expired
 
 
-def test_u_buoyancy_keeps_the_residual_after_the_energy_loop():
-    # with Ri != 0 the u residual reads T after the energy loop (no branch);
-    # both placements stay bit-identical to the oracle in exact mode
+def test_u_buoyancy_keeps_parity():
+    # the u residual reads T (Ri != 0: a nonzero buoyancy term in the u rows
+    # and the residual); exact mode stays bit-identical to the oracle
     for ri in (0.0, 0.3):
         case = cases.lid_driven_mixed(37, 23, Re=100.0, Ri=1.0)
         case.params["Ri"] = ri
