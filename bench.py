@@ -442,7 +442,8 @@ def adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, warm=500, fd_nodes=8):
     the flow held fixed the objective is affine in the nodes, so central
     differences are exact for any step and the small step only adds the
     forward's rounding divided by h.  A linearity check compares
-    J(theta + d) - J(theta) with the adjoint's g . d."""
+    J(theta + d) - J(theta) with the adjoint's g . d.  The same central
+    differences on two nodes of the CPU oracle's forward (oracle_fd)."""
     from ixchel2d_b200 import Simple2D, cases
     from ixchel2d_b200.adjoint import HotWallNusselt
     case = cases.natural_cavity(n, n, Ra=Ra, T0=0.5)
@@ -472,6 +473,20 @@ def adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, warm=500, fd_nodes=8):
     dj = J.value(theta + d) - nu
     sim.close()
     fd = fds[1e-6]
+
+    # central differences of the CPU oracle (the restatement of the reference's CPU path) on two nodes
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+
+    def J_oracle(th):
+        o = O.OracleCase(case)
+        o.set_state(state)
+        o.set_bc_values(2, 0, J.P @ th)
+        o.energy_passes(K)
+        v = o.nusselt_x(2, n - 2)[0]
+        o.close()
+        return v
+    oracle_fd = oracle_central_differences(J_oracle, g, theta, nodes)
     return {"case": f"natural_cavity_{n}x{n}_Ra{Ra:g}", "flow": f"held fixed after {warm} SIMPLE iterations",
             "nodes": nodes, "K": K, "nu_hot_wall": nu,
             "adjoint_s": t_adj, "forward_s": t_fwd, "fd_all_nodes_s_estimate": 2 * nodes * t_fwd,
@@ -480,7 +495,26 @@ def adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, warm=500, fd_nodes=8):
             "normwise_rel_err_vs_fd": float(np.linalg.norm(g[pick] - fd) / np.linalg.norm(fd)),
             "max_rel_err_vs_fd_h1e-2": float(np.max(np.abs(g[pick] - fds[1e-2]) /
                                                  np.maximum(np.abs(fds[1e-2]), 1e-300))),
-            "linearity_rel_err": float(abs(dj - g @ d) / abs(dj))}
+            "linearity_rel_err": float(abs(dj - g @ d) / abs(dj)),
+            "oracle_fd": oracle_fd}
+
+
+def oracle_central_differences(J_oracle, g, theta, nodes, picks=2):
+    """Central differences of an objective evaluated on the CPU oracle, on
+    `picks` nodes at steps 1e-6 and 1e-2, against the adjoint gradient g."""
+    pick = [nodes // 4, nodes // 2][:picks]
+    out = {"nodes_checked": pick}
+    t0 = time.perf_counter()
+    for h in (1e-6, 1e-2):
+        errs = []
+        for k in pick:
+            e = np.zeros(nodes)
+            e[k] = h
+            fd = (J_oracle(theta + e) - J_oracle(theta - e)) / (2 * h)
+            errs.append(abs(g[k] - fd) / max(abs(fd), 1e-300))
+        out[f"max_rel_err_h{h:g}"] = float(max(errs))
+    out["oracle_s"] = time.perf_counter() - t0
+    return out
 
 
 def coupled_adjoint_bench(n=256, Re=100.0, nodes=128, K=500, C=50, fd_nodes=8):
@@ -492,7 +526,8 @@ def coupled_adjoint_bench(n=256, Re=100.0, nodes=128, K=500, C=50, fd_nodes=8):
     after the K iterations.  The T loop runs up to 5 passes per iteration
     (conv_t = 1e-4, iter_ecuaci_max = 3).  Gradient against central
     differences of the same GPU forward on fd_nodes nodes, h = 1e-6 and
-    h = 1e-2 (the objective is affine in the nodes: exact for any step)."""
+    h = 1e-2 (the objective is affine in the nodes: exact for any step), and
+    of the CPU oracle's forward on two nodes (oracle_fd)."""
     from ixchel2d_b200 import Simple2D, cases
     from ixchel2d_b200.adjoint import HotWallNusseltCoupled
     case = cases.lid_driven_forced(n, n, Re=Re, conv_t=1e-4, iter_ecuaci_max=3)
@@ -518,12 +553,24 @@ def coupled_adjoint_bench(n=256, Re=100.0, nodes=128, K=500, C=50, fd_nodes=8):
         fds[h] = fd
     sim.close()
     rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+
+    def J_oracle(th):
+        o = O.OracleCase(case)
+        o.set_bc_values(2, 0, J.P @ th)
+        o.iterations(K)
+        v = o.nusselt_x(2, n - 2)[0]
+        o.close()
+        return v
+    oracle_fd = oracle_central_differences(J_oracle, g, theta, nodes)
     return {"case": case.name, "flow": "evolving over the K iterations from rest (Ri = Riy = 0)",
             "nodes": nodes, "K": K, "C": C, "nu_hot_wall": nu, "adjoint_s": t_adj, "forward_s": t_fwd,
             "fd_all_nodes_s_estimate": 2 * nodes * t_fwd, "fd_nodes_checked": fd_nodes,
             "max_rel_err_vs_fd": rel(g[pick], fds[1e-6]),
             "normwise_rel_err_vs_fd": float(np.linalg.norm(g[pick] - fds[1e-6]) / np.linalg.norm(fds[1e-6])),
-            "max_rel_err_vs_fd_h1e-2": rel(g[pick], fds[1e-2])}
+            "max_rel_err_vs_fd_h1e-2": rel(g[pick], fds[1e-2]), "oracle_fd": oracle_fd}
 
 
 def make_sim(case, prec, stream, shapes):

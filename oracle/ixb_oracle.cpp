@@ -51,6 +51,11 @@ struct BCSide {
   int tipo[15] = {0};      // 1 = 'diri', 2 = 'neum', 0 = anything else ('desc')
   double valor[15] = {0};
   int indice[16] = {0};    // indice_div(1..ndivis+1)
+  // Extension (no counterpart in the reference, whose sides hold at most 15
+  // piecewise-constant segments): when set, the value written on line l is
+  // line_val[l-1] instead of its segment's valor -- the per-line boundary
+  // values of the GPU library's ixb_set_bc_values.
+  std::vector<double> line_val;
 };
 
 // x**5 with the reference's integer power: DMAX1(0, (1-0.1|P|)**5)
@@ -382,8 +387,9 @@ struct Case {
     for (int ldiv = 1; ldiv <= cf.ndivis; ++ldiv) {
       int t = cf.tipo[ldiv - 1];
       if (t != 1 && t != 2) continue;
-      double val = cf.valor[ldiv - 1];
       for (int jj = cf.indice[ldiv - 1]; jj <= cf.indice[ldiv]; ++jj) {
+        const double val =
+            (jj >= 1 && jj <= (int)cf.line_val.size()) ? cf.line_val[jj - 1] : cf.valor[ldiv - 1];
         switch (cf.lado) {
           case 'a':
             if (t == 1) setrow(1, jj, 0.0, 1.0, 0.0, val); else setrow(1, jj, 0.0, -1.0, 1.0, val);
@@ -750,6 +756,20 @@ int ixo_set_bc(ixo_case* h, int var, int side, int ndivis, const int* tipo, cons
   b.lado = ndivis > 0 ? (char)('a' + side) : 'z';
   for (int k = 0; k < ndivis; ++k) { b.tipo[k] = tipo[k]; b.valor[k] = valor[k]; }
   for (int k = 0; k <= ndivis; ++k) b.indice[k] = indice[k];
+  return 0;
+}
+
+// Per-line boundary values of one side (the extension of BCSide above), for
+// the lines of that side in the variable's shape: sides a and c have nj+1
+// lines for u and T and nj for v; sides b and d have mi for u and mi+1 for v
+// and T.  Call after ixo_set_bc for the same side.
+int ixo_set_bc_values(ixo_case* h, int var, int side, const double* values) {
+  Case& c = *reinterpret_cast<Case*>(h);
+  if (var < 0 || var > 2 || side < 0 || side > 3 || !values) return 1;
+  const int mi = c.mi, nj = c.nj;
+  const int nl = (side == 0 || side == 2) ? (var == 1 ? nj : nj + 1) : (var == 0 ? mi : mi + 1);
+  BCSide* s = var == 0 ? c.bcu : var == 1 ? c.bcv : c.bct;
+  s[side].line_val.assign(values, values + nl);
   return 0;
 }
 

@@ -39,6 +39,7 @@ def _load():
         "ixo_set_mesh": (C.c_int, [_vp, _dp, _dp, _dp, _dp]),
         "ixo_set_params": (C.c_int, [_vp, _dp, _ip]),
         "ixo_set_bc": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _ip, _dp, _ip]),
+        "ixo_set_bc_values": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
         "ixo_set_sources": (C.c_int, [_vp, C.c_int, _dp, _dp]),
         "ixo_set_state": (C.c_int, [_vp] + [_dp] * 7),
         "ixo_get_state": (C.c_int, [_vp] + [_dp] * 7),
@@ -178,6 +179,20 @@ class OracleCase:
         for var, (fc, fl) in case.sources.items():
             self.set_sources(var, fc, fl)
         self.set_state(case.state)
+
+    def set_bc_values(self, var: int, side: int, values):
+        """Per-line boundary values of one side (the extension of ixo_set_bc_values,
+        mirroring the library's ixb_set_bc_values)."""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        if lib.ixo_set_bc_values(self.h, var, side, _p(a)) != 0:
+            raise ValueError("ixo_set_bc_values")
+
+    def energy_passes(self, n: int):
+        """n passes of the two T sweeps (T-y, T-x) at the current u, v: the
+        oracle side of the library's ixb_energy_iterations."""
+        for _ in range(n):
+            self.phase(7)
+            self.phase(8)
 
     def set_params(self, prm: dict):
         d = (C.c_double * len(PARAM_ORDER))(*[float(prm[k]) for k in PARAM_ORDER])

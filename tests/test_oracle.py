@@ -142,3 +142,16 @@ def test_nusselt_y_reference_rule_uses_zero_derivative_past_range():
     ga = y0 - al * x0 * x0 - be * x0
     last = al / 3 * (x2 ** 3 - x0 ** 3) + be / 2 * (x2 ** 2 - x0 ** 2) + ga * (x2 - x0)
     assert abs(nu0 - (inner - last)) < 1e-12
+
+
+def test_per_line_values_equal_to_the_segment_values_change_nothing():
+    # the oracle's per-line extension with the values the segments already hold
+    c = cases.lid_driven_forced(14, 12)
+    a = O.OracleCase(c)
+    b = O.OracleCase(c)
+    b.set_bc_values(2, 0, np.ones(13))  # side a of T: Dirichlet 1 everywhere
+    a.iterations(20)
+    b.iterations(20)
+    sa, sb = a.get_state(), b.get_state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
