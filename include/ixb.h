@@ -268,6 +268,15 @@ int ixb_tridiag_f32(const float* a, const float* b, const float* c, const float*
  * the device reports an error, else IXB_OK.  No counterpart in the
  * reference, whose solver has no waits. */
 int ixb_tridiag_status(void);
+/* Failure-detection hook, no counterpart in the reference: the number of
+ * polls the first copy wait of every CTA of the streamed contiguous solve
+ * (hybrid solver, layout 0) may take before it counts as expired; polls < 0
+ * restores the default (2^22 polls, at most about two seconds).  With 0 the
+ * first wait expires at once: each CTA records the timeout, waits at the
+ * default bound for its copies already in flight, and returns without
+ * writing, so ixb_tridiag_status reports IXB_ETIMEOUT and the device stays
+ * usable.  Process-wide; for tests only. */
+int ixb_tridiag_set_first_wait_limit(int polls);
 
 /* Allocation-free form of ixb_tridiag_f64 (no counterpart in the reference),
  * for callers that cannot let a library allocate device memory during their

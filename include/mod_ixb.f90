@@ -365,6 +365,11 @@ module ixb
        import :: c_int
      end function ixb_tridiag_status
 
+     integer(c_int) function ixb_tridiag_set_first_wait_limit(polls) bind(C, name="ixb_tridiag_set_first_wait_limit")
+       import :: c_int
+       integer(c_int), value :: polls
+     end function ixb_tridiag_set_first_wait_limit
+
      ! ---- energy equation with the flow held fixed, and its adjoint ----
      integer(c_int) function ixb_energy_iterations(h, n) bind(C, name="ixb_energy_iterations")
        import :: c_int, c_ptr

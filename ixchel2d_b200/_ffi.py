@@ -87,6 +87,7 @@ SIGNATURES = [
     ("ixb_read_state_files", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_int] + [_vp] * 8 +
      [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     ("ixb_tridiag_status", C.c_int, []),
+    ("ixb_tridiag_set_first_wait_limit", C.c_int, [C.c_int]),
     ("ixb_iteration_launches", C.c_int, [_vp, C.POINTER(C.c_int)]),
     ("ixb_body_sources", C.c_int, [C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double] + [_vp] * 6),
     ("ixb_bc_locate", C.c_int, [C.c_int, C.c_int, _dp, C.POINTER(C.c_int), _dp, _dp, C.c_int, _dp, C.c_int,

@@ -144,6 +144,10 @@ namespace {
 constexpr int kStreamT = 256;       // threads per CTA (one system at a time)
 constexpr int kSpinLimit = 1 << 22;  // bounded mbarrier polls (a hang guard)
 __device__ int g_tri_timeout = 0;
+// Poll limit of the streamed kernel's first wait of every CTA (its other
+// waits, and the drain after a timeout, keep kSpinLimit); lowered only by
+// ixb_tridiag_set_first_wait_limit, for failure-detection tests.
+__device__ int g_tri_first_wait_polls = kSpinLimit;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -183,9 +187,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-  for (int i = 0; i < kSpinLimit; ++i)
+// At most `limit` polls, and no longer than about two seconds (%globaltimer).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int limit = kSpinLimit) {
+  unsigned long long t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (int i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 255) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      if (t - t0 > 2000000000ull) return false;
+    }
+  }
   return false;
 }
 
@@ -225,10 +238,11 @@ __global__ void __launch_bounds__(kStreamT, 1) tri_stream_kernel(const R* __rest
     bulk_load(buf + 3 * NP, d + off, bytes, bar);
   };
   if (tid == 0 && blockIdx.x < nsys) issue(blockIdx.x);
+  const int first_limit = *(volatile int*)&g_tri_first_wait_polls;
   unsigned parity = 0;
   bool failed = false;
   for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
-    const bool ok = mbar_wait_bounded(bar, parity);
+    const bool ok = mbar_wait_bounded(bar, parity, s == (int)blockIdx.x ? first_limit : kSpinLimit);
     if (__syncthreads_or(!ok)) { failed = true; break; }
     parity ^= 1;
     // own rows into registers (row 0 has no a, row n-1 no c)
@@ -882,6 +896,11 @@ cudaError_t tridiag_take_timeout(int* flag) {
   return cudaSuccess;
 }
 
+cudaError_t tridiag_set_first_wait_polls(int polls) {
+  const int v = polls < 0 ? kSpinLimit : polls;
+  return cudaMemcpyToSymbol(g_tri_first_wait_polls, &v, sizeof(int));
+}
+
 cudaError_t tridiag_f64(const double* a, const double* b, const double* c, const double* d, double* x, int n,
                         int nsys, int layout, int solver, cudaStream_t st) {
   if (solver == IXB_SOLVER_EXACT) return tridiag_impl<double, IXB_SOLVER_EXACT>(a, b, c, d, x, n, nsys, layout, st);
@@ -975,4 +994,10 @@ extern "C" int ixb_tridiag_f64_noalloc(const double* a, const double* b, const d
   }
   if (e == cudaErrorInvalidValue) return IXB_EINVAL;
   return e == cudaSuccess ? IXB_OK : IXB_ECUDA;
+}
+
+// Failure-detection hook (no counterpart in the reference): the poll limit of
+// the first copy wait of every CTA of the streamed contiguous solve.
+extern "C" int ixb_tridiag_set_first_wait_limit(int polls) {
+  return ixb::tridiag_set_first_wait_polls(polls) == cudaSuccess ? IXB_OK : IXB_ECUDA;
 }
