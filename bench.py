@@ -350,7 +350,7 @@ def adi_microbench(stream, n=4096, nsys=4096, reps=5):
     return out
 
 
-def batched_bench(stream, n_inst=256, iters=30, n_conv=16, conv_cap=20000):
+def batched_bench(stream, n_inst=256, iters=30, n_conv=16, conv_cap=20000, full_cap=3000):
     """Batched cavities (ixb_batch_*): natural-convection cavities, square
     side uniform in {64..512} and Ra log-uniform in [1e3, 1e6] (Pr 0.71,
     seed 1234).  Throughput: `iters` outer iterations of all n_inst
@@ -359,7 +359,10 @@ def batched_bench(stream, n_inst=256, iters=30, n_conv=16, conv_cap=20000):
     16 instances.  Convergence: n_conv smaller cavities (side 64..128, Ra
     1e3..1e5) each iterated to maxbo < 1e-8 (cap conv_cap iterations),
     batched refined vs the single-instance binary64 path one after the
-    other; instances per second of each."""
+    other; instances per second of each.  The full configuration (all
+    n_inst instances from rest, batched refined) to maxbo < 1e-8 under a cap
+    of full_cap iterations: how many converge and in what time (the largest
+    cavities need on the order of 1e5 iterations, beyond a bench budget)."""
     import torch
     from ixchel2d_b200 import Batch, Simple2D, cases
     from ixchel2d_b200 import _ffi as F
@@ -395,6 +398,21 @@ def batched_bench(stream, n_inst=256, iters=30, n_conv=16, conv_cap=20000):
         sm.close()
     out["batched_refined_over_looped_fp64"] = (out["batched_refined"]["mcell_iter_s"] /
                                                out["looped_single_fp64"]["mcell_iter_s"])
+    # the full configuration to convergence under a cap: every instance from rest, each leaving
+    # the batch when its maxbo < 1e-8 (the reference's outer test with conv_paso = 1e-8)
+    bt = Batch.from_cases(cs, prec=F.PREC_FP32_REFINED, conv_paso=1e-8, conv_resi=1e30)
+    bt.autotune(reps=2)
+    bt.restart()
+    left = [n_inst]
+    dt_f = timed(lambda: left.__setitem__(0, bt.iterate(full_cap)))
+    reps_f = [bt.report(i) for i in range(n_inst)]
+    bt.close()
+    conv_f = [i for i, r in enumerate(reps_f) if r["exit_code"] == 1]
+    out["converge_full_capped"] = {
+        "instances": n_inst, "criterion": "maxbo < 1e-8", "cap_iters": full_cap, "form": "batched refined",
+        "converged": len(conv_f), "seconds": dt_f, "instances_per_s": len(conv_f) / dt_f,
+        "largest_side_converged": int(max((sides[i] for i in conv_f), default=0)),
+        "median_iters_converged": float(np.median([reps_f[i]["n_simple"] for i in conv_f])) if conv_f else None}
     # convergence of smaller cavities
     sides = rng.integers(64, 129, n_conv)
     ras = 10.0 ** rng.uniform(3.0, 5.0, n_conv)
