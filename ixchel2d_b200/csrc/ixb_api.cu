@@ -142,7 +142,7 @@ SweepIO<double> sweep_io(ixb_handle* h, int eq, const double* prev, bool with_no
   io.in = buf[*cur];
   io.out = buf[*cur ^ 1];
   io.prev = prev;
-  io.fcon = io.flin = h->zero;
+  io.fcon = io.flin = nullptr;  // an equation without sources reads none
   if (var >= 0) {
     if (h->fcon[var]) io.fcon = h->fcon[var];
     if (h->flin[var]) io.flin = h->flin[var];

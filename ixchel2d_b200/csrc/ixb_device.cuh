@@ -49,8 +49,9 @@ enum Metric {
 //   T_CV2(ii,jj)  v: gammas*deltaxv/ds; BN conductance = T_CV2(ii,jj+1)
 //   T_CT1(ii,jj)  T: gammai*deltayp/di; AD conductance = T_CT1(ii+1,jj)
 //   T_CT2(ii,jj)  T: gamman*deltaxp/dn; BS conductance = T_CT2(ii,jj-1)
-//   T_RGU, T_RGV  1/T_GU, 1/T_GV (fast form: Peclet numbers by multiplication)
-enum Table { T_GU = 0, T_CU1, T_CU2, T_GV, T_CV1, T_CV2, T_CT1, T_CT2, T_RGU, T_RGV, T_COUNT };
+//   (the fast form divides the Peclet numbers of u and v by multiplying with
+//   the scalar 1/gamma_momen: the face diffusivities of a uniform gamma)
+enum Table { T_GU = 0, T_CU1, T_CU2, T_GV, T_CV1, T_CV2, T_CT1, T_CT2, T_COUNT };
 
 // sweeps: the eight line-solve phases of main.f90
 enum Eq { EQ_UY = 0, EQ_UX, EQ_VY, EQ_VX, EQ_PY, EQ_PX, EQ_TY, EQ_TX, EQ_COUNT };
@@ -100,7 +101,7 @@ struct SweepIO {
   const R *u, *v, *T, *p, *pc;        // current fields
   const R *u_ant, *v_ant, *T_ant;
   const R *au, *av;
-  const R *fcon, *flin;               // sources of this equation (a zero field when none)
+  const R *fcon, *flin;               // sources of this equation (null when none)
   const R* in;                        // swept field, current values
   R* out;                             // swept field, new values
   const R* prev;                      // field at the start of the inner pass (null: zero)
@@ -182,8 +183,10 @@ __device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<F>& io, c
   const R g = G.gm;
   R gamman, gammas, rgn = R(0), rgs = R(0);
   if constexpr (FAST) {
-    rgn = G.t(T_RGU, ii, jj);
-    rgs = G.t(T_RGU, ii, jj - 1);
+    // the face diffusivity is the harmonic mean of a uniform gamma_momen
+    // (ixb_params holds one value), i.e. gamma_momen up to rounding: its
+    // reciprocal is the scalar 1/gamma_momen, no table load
+    rgn = rgs = G.inv_gm;
     gamman = gammas = R(0);
   } else {
     gamman = G.t(T_GU, ii, jj);
@@ -206,8 +209,8 @@ __device__ __forceinline__ Row<R> assemble_ux(const Geo<R>& G, const SweepIO<F>&
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
-  const R flin = ld<R>(io.flin, c0);
-  const R fcon = ld<R>(io.fcon, c0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);  // no sources: no loads (the values would be +0)
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
@@ -227,8 +230,8 @@ __device__ __forceinline__ Row<R> assemble_uy(const Geo<R>& G, const SweepIO<F>&
   R AI, AD, BS, BN, dx, dy, tint;
   u_parts<FAST>(G, io, u, ii, jj, AI, AD, BS, BN, dx, dy, tint);
   const int c0 = G.at(ii, jj);
-  const R flin = ld<R>(io.flin, c0);
-  const R fcon = ld<R>(io.fcon, c0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);  // no sources: no loads (the values would be +0)
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
@@ -256,8 +259,7 @@ __device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<F>& io, c
   const R g = G.gm;  // gamman = gammas = gamma_momen (:854-858)
   R gammad, gammai, rgd = R(0), rgi = R(0);
   if constexpr (FAST) {
-    rgd = G.t(T_RGV, ii, jj);
-    rgi = G.t(T_RGV, ii - 1, jj);
+    rgd = rgi = G.inv_gm;  // uniform gamma_momen, as in u_parts
     gammad = gammai = R(0);
   } else {
     gammad = G.t(T_GV, ii, jj);
@@ -280,8 +282,8 @@ __device__ __forceinline__ Row<R> assemble_vx(const Geo<R>& G, const SweepIO<F>&
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = ld<R>(io.flin, c0);
-  const R fcon = ld<R>(io.fcon, c0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);  // no sources: no loads (the values would be +0)
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
@@ -301,8 +303,8 @@ __device__ __forceinline__ Row<R> assemble_vy(const Geo<R>& G, const SweepIO<F>&
   const int c0 = G.at(ii, jj);
   const R dxv = G.met(M_DXV, ii), dyv = G.met(M_DYV, jj);
   const R dxdy = dxv * dyv;
-  const R flin = ld<R>(io.flin, c0);
-  const R fcon = ld<R>(io.fcon, c0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);  // no sources: no loads (the values would be +0)
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
@@ -348,8 +350,8 @@ __device__ __forceinline__ Row<R> assemble_tx(const Geo<R>& G, const SweepIO<F>&
   t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = ld<R>(io.flin, c0);
-  const R fcon = ld<R>(io.fcon, c0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);  // no sources: no loads (the values would be +0)
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = AI;
   r.c = AD;
@@ -366,8 +368,8 @@ __device__ __forceinline__ Row<R> assemble_ty(const Geo<R>& G, const SweepIO<F>&
   t_parts<FAST>(G, io, ii, jj, AI, AD, BS, BN);
   const int c0 = G.at(ii, jj);
   const R dxdy = G.met(M_DXP, ii) * G.met(M_DYP, jj);
-  const R flin = ld<R>(io.flin, c0);
-  const R fcon = ld<R>(io.fcon, c0);
+  const R flin = io.flin ? ld<R>(io.flin, c0) : R(0);  // no sources: no loads (the values would be +0)
+  const R fcon = io.fcon ? ld<R>(io.fcon, c0) : R(0);
   Row<R> r;
   r.a = BS;
   r.c = BN;
@@ -451,8 +453,10 @@ __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v,
   const R g = G.gm;
   R gamman, gammas, rgn = R(0), rgs = R(0);
   if constexpr (FAST) {
-    rgn = G.t(T_RGU, ii, jj);
-    rgs = G.t(T_RGU, ii, jj - 1);
+    // the face diffusivity is the harmonic mean of a uniform gamma_momen
+    // (ixb_params holds one value), i.e. gamma_momen up to rounding: its
+    // reciprocal is the scalar 1/gamma_momen, no table load
+    rgn = rgs = G.inv_gm;
     gamman = gammas = R(0);
   } else {
     gamman = G.t(T_GU, ii, jj);

@@ -49,7 +49,6 @@ __global__ void table2d_kernel(Geo<R> G, R* tab) {
     const R hy = hmean(g, g, G.met(M_FEYP, jj));
     const R gamman = combo(hy, G.met(M_FEXP, ii));
     T(T_GU) = gamman;
-    T(T_RGU) = R(1) / gamman;
     T(T_CU2) = gamman * G.met(M_DXU, ii) / G.met(M_DYV, jj);
   }
   if (ii >= 2 && ii <= G.mi && jj >= 2 && jj <= G.nj) T(T_CU1) = g * G.met(M_DYU, jj) / G.met(M_DXP, ii);
@@ -57,7 +56,6 @@ __global__ void table2d_kernel(Geo<R> G, R* tab) {
   if (ii <= G.mi && jj <= G.nj) {
     const R hx = hmean(g, g, G.met(M_FEXP, ii));
     T(T_GV) = combo(hx, G.met(M_FEYP, jj));
-    T(T_RGV) = R(1) / T(T_GV);
   }
   if (ii >= 2 && ii <= G.mi + 1 && jj <= G.nj) {
     const R hx = hmean(g, g, G.met(M_FEXP, ii - 1));
