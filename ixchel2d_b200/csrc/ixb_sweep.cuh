@@ -279,7 +279,14 @@ __device__ __forceinline__ void fused_assemble(typename SweepTypes<SOLVER, EQ>::
     const int idx = threadIdx.x + it * NT;
     int l, r;
     if (X) { l = TL == 1 ? 0 : idx / npad; r = idx - l * npad; }
-    else { l = idx % TL; r = idx / TL; }
+    else if (M > 0) {
+      // y-lines with a compile-time chunk: each thread assembles the M
+      // consecutive rows of its own chunk, so neighbouring rows' stencil
+      // loads (row jj+1 of one cell is row jj of the next) repeat within
+      // the thread and the compiler may keep them in registers
+      l = threadIdx.x % TL;
+      r = (threadIdx.x / TL) * M + it;
+    } else { l = idx % TL; r = idx / TL; }
     const int L = L0 + l;
     const bool valid = L >= line_lo && L <= line_hi && r < n;
     // padding rows and unsolved lines: identity rows, nothing to assemble
@@ -410,6 +417,8 @@ cudaError_t fused_launch(const SweepShape& s, const Geo<double>& G, const SweepI
 #define IXB_FUSED_(TL_, G_)                                                                     \
   if (s.tl == TL_ && s.g == G_) {                                                               \
     if (!EXACT && s.m == 3) return fused_go<fused_sweep_kernel<EQ, SOLVER, TL_, G_, 3>>(s, G, io, so, st); \
+    if constexpr (!EqIsX<EQ>::value && !EXACT)                                                  \
+      if (s.m == 5) return fused_go<fused_sweep_kernel<EQ, SOLVER, TL_, G_, 5>>(s, G, io, so, st); \
     return fused_go<fused_sweep_kernel<EQ, SOLVER, TL_, G_, 0>>(s, G, io, so, st);                \
   }
   if constexpr (EqIsX<EQ>::value) {
