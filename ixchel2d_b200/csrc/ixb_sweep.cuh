@@ -301,6 +301,31 @@ __device__ __forceinline__ void fused_assemble(typename SweepTypes<SOLVER, EQ>::
   }
 }
 
+// u residual (residuo_u) of row jj = L0 of a fused T-x sweep (one line per
+// CTA): cells ii = 2..mi-1, m per thread (G*m >= mi+1 rows of the line);
+// with a compile-time m the cells' loads are independent and issued
+// together.  T: the temperature the residual's buoyancy term reads (written
+// earlier in this kernel when T_WRITTEN).  Returns this thread's sum of
+// squares.
+template <bool FAST, bool T_WRITTEN, int G, int M>
+__device__ __forceinline__ double tx_residual_row(const Geo<double>& G_, const ResidIO& r, const double* T, int m,
+                                                  int L0) {
+  double acc = 0.0;
+  if (L0 < 2 || L0 > G_.nj) return acc;
+#pragma unroll
+  for (int k = 0; k < (M > 0 ? M : m); ++k) {
+    const int ii = 2 + (int)threadIdx.x + k * G;
+    const bool valid = ii <= G_.mi - 1;
+    const double v = residual_u<FAST, double, T_WRITTEN>(G_, r.u, r.v, T, r.p, r.u_ant, r.fcon, r.flin,
+                                                         valid ? ii : G_.mi - 1, L0);
+    if (valid) {
+      r.resu[G_.at(ii, L0)] = v;
+      acc += v * v;
+    }
+  }
+  return acc;
+}
+
 template <int EQ, int SOLVER, int TL, int G, int M>
 __global__ void __launch_bounds__(TL * G)
     fused_sweep_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n,
@@ -320,25 +345,10 @@ __global__ void __launch_bounds__(TL * G)
       sm, so, n, line_lo, line_hi, nfull, L0);
   if constexpr (EQ == EQ_TX) {
     if (so.res.resu) {
-      // u residual of row jj = L0 (TL = 1 for x-sweeps), whose T this CTA has just written
+      // u residual of row jj = L0, whose T this CTA has just written (evaluating it before the
+      // solve when Ri == 0, on the T the sweep reads, measured the same)
       __syncthreads();
-      double acc_res = 0.0;
-      if (L0 >= 2 && L0 <= G_.nj) {
-        // cells ii = 2..mi-1 of the row, m per thread (G*m >= mi+1 rows of the line); with a
-        // compile-time m the cells' loads are independent and issued together
-        const ResidIO& r = so.res;
-#pragma unroll
-        for (int k = 0; k < (M > 0 ? M : m); ++k) {
-          const int ii = 2 + (int)threadIdx.x + k * G;
-          const bool valid = ii <= G_.mi - 1;
-          const double v = residual_u<SOLVER != IXB_SOLVER_EXACT, double, true>(
-              G_, r.u, r.v, so.out, r.p, r.u_ant, r.fcon, r.flin, valid ? ii : G_.mi - 1, L0);
-          if (valid) {
-            r.resu[G_.at(ii, L0)] = v;
-            acc_res += v * v;
-          }
-        }
-      }
+      const double acc_res = tx_residual_row<SOLVER != IXB_SOLVER_EXACT, true, G, M>(G_, so.res, so.out, m, L0);
       const double s0 = block_sum(acc);
       const double s1 = block_sum(acc_res);
       // the energy test, then (after the loop's last pass) the outer test
