@@ -573,6 +573,69 @@ def coupled_adjoint_bench(n=256, Re=100.0, nodes=128, K=500, C=50, fd_nodes=8):
             "max_rel_err_vs_fd_h1e-2": rel(g[pick], fds[1e-2]), "oracle_fd": oracle_fd}
 
 
+def full_adjoint_bench(n=256, Ra=1e5, nodes=128, K=500, C=50, fd_nodes=6):
+    """Adjoint of the full coupled SIMPLE iteration (ixb_adjoint_simple): the
+    natural-convection cavity n x n at Ra (buoyancy couples the flow to the
+    wall temperature), from rest and T = 0.5; hot-wall profile of `nodes`
+    piecewise-linear nodes, value 1 + U(-0.05, 0.05) (seed 1234); objective
+    the hot-wall Nusselt number after K outer iterations (one pass of each
+    equation), checkpoints every C.  The objective is nonlinear in the
+    nodes: central differences of the GPU forward on fd_nodes nodes at
+    h = 1e-6 (the configured step) and h = 1e-4, and of the CPU oracle on two
+    nodes (oracle_fd)."""
+    from ixchel2d_b200 import Simple2D, cases
+    from ixchel2d_b200.adjoint import profile_matrix
+    case = cases.natural_cavity(n, n, Ra=Ra, T0=0.5)
+    P = profile_matrix(case.yp, nodes)
+    rng = np.random.default_rng(1234)
+    theta = 1.0 + rng.uniform(-0.05, 0.05, nodes)
+    sim = Simple2D.from_case(case)
+
+    def run(th, gradient):
+        sim.upload(case.state)
+        sim.set_bc_values(2, 0, P @ th)
+        return sim.adjoint_simple(K, C, 2, n - 2, gradient=gradient)
+    run(theta, True)  # warm
+    t0 = time.perf_counter()
+    g_lines, nu = run(theta, True)
+    t_adj = time.perf_counter() - t0
+    g = P.T @ g_lines
+    t0 = time.perf_counter()
+    run(theta, False)
+    t_fwd = time.perf_counter() - t0
+    pick = np.linspace(nodes // 16, nodes - 1 - nodes // 16, fd_nodes).astype(int)  # away from the corners
+    errs, norm_errs = {}, {}
+    for h in (1e-6, 1e-4):
+        fd = np.zeros(len(pick))
+        for q, k in enumerate(pick):
+            e = np.zeros(nodes)
+            e[k] = h
+            fd[q] = (run(theta + e, False)[1] - run(theta - e, False)[1]) / (2 * h)
+        errs[h] = float(np.max(np.abs(g[pick] - fd) / np.maximum(np.abs(fd), 1e-300)))
+        norm_errs[h] = float(np.linalg.norm(g[pick] - fd) / np.linalg.norm(fd))
+    sim.close()
+
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+
+    def J_oracle(th):
+        o = O.OracleCase(case)
+        o.set_bc_values(2, 0, P @ th)
+        o.iterations(K)
+        v = o.nusselt_x(2, n - 2)[0]
+        o.close()
+        return v
+    oracle_fd = oracle_central_differences(J_oracle, g, theta, nodes)
+    return {"case": f"natural_cavity_{n}x{n}_Ra{Ra:g}",
+            "flow": "buoyant, evolving over the K iterations from rest (momentum, pressure correction and "
+                    "energy all reversed)",
+            "nodes": nodes, "K": K, "C": C, "nu_hot_wall": nu, "adjoint_s": t_adj, "forward_s": t_fwd,
+            "fd_all_nodes_s_estimate": 2 * nodes * t_fwd, "fd_nodes_checked": int(len(pick)),
+            "max_rel_err_vs_fd_h1e-6": errs[1e-6], "normwise_rel_err_vs_fd_h1e-6": norm_errs[1e-6],
+            "max_rel_err_vs_fd_h1e-4": errs[1e-4], "normwise_rel_err_vs_fd_h1e-4": norm_errs[1e-4],
+            "oracle_fd": oracle_fd}
+
+
 def make_sim(case, prec, stream, shapes):
     from ixchel2d_b200 import Simple2D
     sim = Simple2D.from_case(case, prec=prec)
@@ -724,6 +787,7 @@ def run_ours(args):
     # ---- energy adjoint (flow held fixed) ----
     adjoint = adjoint_bench()
     adjoint_coupled = coupled_adjoint_bench()
+    adjoint_full = full_adjoint_bench()
 
     cells = case.cells
     dom = int(np.argmax(phase_ms_warm))  # the phase with the largest share of the timed step
@@ -770,6 +834,7 @@ def run_ours(args):
             "batched_cavities": batched,
             "energy_adjoint": adjoint,
             "energy_adjoint_coupled": adjoint_coupled,
+            "simple_adjoint_buoyant": adjoint_full,
             "sweep_shapes": {n: {SWEEPS[int(k)]: list(v[:2]) for k, v in sh.items()} for n, sh in shapes.items()},
             "iteration_alg_bytes": iter_bytes,
             "cpu_baseline": None if cpu_val is None else {

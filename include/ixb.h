@@ -317,6 +317,22 @@ int ixb_tridiag_f64_noalloc(const double* a, const double* b, const double* c, c
  * within their bounded wait.  ixb_set_bc_values sets the per-line values of one side of a
  * boundary table (a per-node profile, beyond the reference's 15 segments),
  * keeping each line's type. */
+/* ---- discrete adjoint of the full coupled SIMPLE iteration ----
+ * No counterpart in the reference.  K outer iterations from the current state,
+ * each one pass of every equation (u-y, u-x, v-y, v-x, p'-y from p' = 0,
+ * p'-x, the velocity/pressure update, T-y, T-x: main.f90:404-1136 with
+ * iter_ecuaci_max = 0), then nu0 = the hot-wall Nusselt number of
+ * ixb_nusselt_x(h, j0, j1).  With grad (nj+1 entries, may be NULL for the
+ * forward only): d nu0 / d value of the side-a T boundary row of every
+ * x-line jj (grad[jj-1]; lines 1 and nj+1 are not solved and get 0),
+ * through the momentum, pressure-correction and energy sweeps and their
+ * coupling (buoyancy, convection): the adjoint for flows that depend on T.
+ * The forward state is saved every C iterations; each segment is recomputed
+ * storing the state after every phase (16 fields per iteration, so device
+ * memory grows with C) and reversed with transposed line solves.  Leaves
+ * the state of the K-iteration forward run.  Binary64 handles only
+ * (IXB_EINVAL otherwise). */
+int ixb_adjoint_simple(ixb_handle* h, int K, int C, int j0, int j1, double* grad, double* nu0);
 int ixb_energy_iterations(ixb_handle* h, int n);
 int ixb_adjoint_energy(ixb_handle* h, int K, int j0, int j1, double* grad);
 int ixb_set_bc_values(ixb_handle* h, int var, int side, const double* values);

@@ -371,6 +371,13 @@ module ixb
      end function ixb_tridiag_set_first_wait_limit
 
      ! ---- energy equation with the flow held fixed, and its adjoint ----
+     integer(c_int) function ixb_adjoint_simple(h, K, C, j0, j1, grad, nu0) bind(C, name="ixb_adjoint_simple")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: K, C, j0, j1
+       type(c_ptr), value :: grad, nu0   ! real(c_double) arrays via c_loc (grad: nj+1 entries), or c_null_ptr
+     end function ixb_adjoint_simple
+
      integer(c_int) function ixb_energy_iterations(h, n) bind(C, name="ixb_energy_iterations")
        import :: c_int, c_ptr
        type(c_ptr), value :: h

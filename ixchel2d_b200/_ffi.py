@@ -75,6 +75,7 @@ SIGNATURES = [
     ("ixb_batch_restart", C.c_int, [_vp]),
     ("ixb_batch_iterate", C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
     ("ixb_batch_report", C.c_int, [_vp, C.c_int, C.POINTER(Report)]),
+    ("ixb_adjoint_simple", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),
     ("ixb_energy_iterations", C.c_int, [_vp, C.c_int]),
     ("ixb_adjoint_energy", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp]),
     ("ixb_adjoint_energy_coupled", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),

@@ -199,6 +199,17 @@ class Simple2D:
                 "ixb_adjoint_energy_coupled")
         return g, nu.value
 
+    def adjoint_simple(self, K: int, ckpt: int, j0: int, j1: int, gradient: bool = True):
+        """Hot-wall Nusselt number nu0 after K outer iterations (one pass of each
+        equation) and, with `gradient`, its gradient with respect to the side-a
+        T boundary value of every x-line (nj+1 entries) through the full coupled
+        iteration (ixb_adjoint_simple).  Returns (grad or None, nu0)."""
+        g = np.zeros(self.nj + 1) if gradient else None
+        nu = C.c_double()
+        F.check(F.lib.ixb_adjoint_simple(self.h, K, ckpt, j0, j1, None if g is None else g.ctypes.data,
+                                         C.addressof(nu)), "ixb_adjoint_simple")
+        return g, nu.value
+
     def set_bc_values(self, var: int, side: int, values):
         v = np.ascontiguousarray(values, dtype=np.float64)
         F.check(F.lib.ixb_set_bc_values(self.h, var, side, F.dptr(v)), "ixb_set_bc_values")
