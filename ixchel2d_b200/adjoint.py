@@ -1,8 +1,10 @@
 """Gradient of the hot-wall Nusselt number with respect to a piecewise-linear
 hot-wall temperature profile: with the flow held fixed (HotWallNusselt, over
-ixb_energy_iterations and ixb_adjoint_energy), or through K outer SIMPLE
+ixb_energy_iterations and ixb_adjoint_energy), through K outer SIMPLE
 iterations of a flow that does not depend on T (HotWallNusseltCoupled, over
-ixb_simple_iterations and ixb_adjoint_energy_coupled).  as_torch() wraps
+ixb_simple_iterations and ixb_adjoint_energy_coupled), or through K outer
+iterations of any flow, buoyant included (HotWallNusseltSimple, over
+ixb_adjoint_simple).  as_torch() wraps
 either in a thin torch.autograd.Function, used to check the adjoint against
 finite differences."""
 from __future__ import annotations
@@ -88,4 +90,23 @@ class HotWallNusseltCoupled(HotWallNusselt):
         self.sim.set_bc_values(F.VAR_T, 0, self.P @ np.asarray(theta, dtype=np.float64))
         self.sim.upload(self.state)
         g, _ = self.sim.adjoint_energy_coupled(self.K, self.ckpt, self.j0, self.j1)
+        return self.P.T @ g
+
+
+class HotWallNusseltSimple(HotWallNusseltCoupled):
+    """J(theta) = nu0 of ixb_nusselt_x(j0, j1) after K outer SIMPLE
+    iterations from `state` (one pass of each equation), with the side-a T
+    boundary values set to P theta, for any flow: the gradient comes from
+    ixb_adjoint_simple, the adjoint of the full coupled iteration (momentum,
+    pressure correction and energy), so buoyant flows are covered."""
+
+    def value(self, theta: np.ndarray) -> float:
+        self.sim.set_bc_values(F.VAR_T, 0, self.P @ np.asarray(theta, dtype=np.float64))
+        self.sim.upload(self.state)
+        return self.sim.adjoint_simple(self.K, self.ckpt, self.j0, self.j1, gradient=False)[1]
+
+    def gradient(self, theta: np.ndarray) -> np.ndarray:
+        self.sim.set_bc_values(F.VAR_T, 0, self.P @ np.asarray(theta, dtype=np.float64))
+        self.sim.upload(self.state)
+        g, _ = self.sim.adjoint_simple(self.K, self.ckpt, self.j0, self.j1)
         return self.P.T @ g

@@ -122,3 +122,24 @@ def test_buoyant_adjoint_matches_oracle_central_differences():
         e[L - 1] = h
         fd = (J(vals + e) - J(vals - e)) / (2 * h)
         assert abs(g[L - 1] - fd) <= TOL * abs(fd), (L, g[L - 1], fd)
+
+
+def test_autograd_function_of_the_full_adjoint():
+    import torch
+    from ixchel2d_b200.adjoint import HotWallNusseltSimple
+    case = _case()
+    sim = Simple2D.from_case(case)
+    nodes, K = 6, 10
+    J = HotWallNusseltSimple(sim, case.state, case.yp, nodes, K, 2, NJ - 2, ckpt=4)
+    theta = torch.tensor(1.0 + 0.02 * np.arange(nodes), dtype=torch.float64, requires_grad=True)
+    y = J.as_torch()(theta)
+    y.backward()
+    g = theta.grad.numpy()
+    th = theta.detach().numpy()
+    assert abs(y.item() - J.value(th)) <= 1e-13 * abs(y.item())
+    h = 1e-5
+    e = np.zeros(nodes)
+    e[2] = h
+    fd = (J.value(th + e) - J.value(th - e)) / (2 * h)
+    assert abs(g[2] - fd) <= TOL * abs(fd)
+    sim.close()
