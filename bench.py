@@ -924,6 +924,18 @@ def run_profile_adjoint():
     sim.close()
 
 
+def run_profile_simple_adjoint():
+    """Profiling driver: the full coupled adjoint on the 256 x 256 natural-
+    convection cavity (Ra 1e5) from rest, K = 2 outer iterations in one
+    checkpoint segment (each reverse kernel launched once per sweep and
+    iteration)."""
+    from ixchel2d_b200 import Simple2D, cases
+    case = cases.natural_cavity(256, 256, Ra=1e5, T0=0.5)
+    sim = Simple2D.from_case(case)
+    sim.adjoint_simple(2, 2, 2, 254)
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -938,6 +950,8 @@ def main():
     ap.add_argument("--profile-adi", action="store_true", help="run the line-solve profiling driver")
     ap.add_argument("--profile-batch", action="store_true", help="run the batched-cavities profiling driver")
     ap.add_argument("--profile-adjoint", action="store_true", help="run the energy-adjoint profiling driver")
+    ap.add_argument("--profile-simple-adjoint", action="store_true",
+                    help="run the profiling driver of the full coupled adjoint")
     args = ap.parse_args()
     if args.profile_phases:
         run_profile_phases(args.prec, args.shapes)
@@ -947,6 +961,9 @@ def main():
         return
     if args.profile_batch:
         run_profile_batch()
+        return
+    if args.profile_simple_adjoint:
+        run_profile_simple_adjoint()
         return
     if args.profile_adjoint:
         run_profile_adjoint()
