@@ -621,7 +621,19 @@ __device__ void thomas_pcr_warp(R* sa, R* sb, R* sc, R* sd, int m, int mp) {
 // in shared memory `red` (12 G elements, two buffers of a | c | d); thread
 // k supplies rows 2k, 2k+1 and receives their solutions x0, xl.  Called by
 // all threads of the CTA (it holds barriers); `active` false: barriers only.
-template <class R, int G>
+// Barrier of the G threads that solve one line when a CTA holds TL lines of
+// whole warps (a named barrier per line, so lines do not wait for each
+// other), else of the whole CTA.
+template <int G, int TL>
+__device__ __forceinline__ void line_sync() {
+  if constexpr (TL > 1 && TL <= 8 && G % 32 == 0) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / G), "r"(G) : "memory");
+  } else {
+    __syncthreads();
+  }
+}
+
+template <class R, int G, int TL = 1>
 __device__ __forceinline__ void reduced_pcr(R* red, int k, bool active, R eA, R eC, R eD, R oA, R oC, R oD, R& x0,
                                             R& xl) {
   R* cur = red;
@@ -630,7 +642,7 @@ __device__ __forceinline__ void reduced_pcr(R* red, int k, bool active, R eA, R 
     cur[2 * k] = eA; cur[2 * G + 2 * k] = eC; cur[4 * G + 2 * k] = eD;
     cur[2 * k + 1] = oA; cur[2 * G + 2 * k + 1] = oC; cur[4 * G + 2 * k + 1] = oD;
   }
-  __syncthreads();
+  line_sync<G, TL>();
 #pragma unroll 1
   for (int s = 1; s < 2 * G; s <<= 1) {
     if (active) {
@@ -649,7 +661,7 @@ __device__ __forceinline__ void reduced_pcr(R* red, int k, bool active, R eA, R 
         Dn[i] = fmaT(-ci, dhi, fmaT(-ai, dlo, di)) * r;
       }
     }
-    __syncthreads();
+    line_sync<G, TL>();
     R* t = cur; cur = nxt; nxt = t;
   }
   x0 = cur[4 * G + 2 * k];
@@ -669,7 +681,7 @@ __device__ __forceinline__ void reduced_pcr(R* red, int k, bool active, R eA, R 
 // Reciprocals use fast_rcp (two Newton steps).  The solution replaces the
 // right-hand side.  Called by all TL*G threads;
 // threads of lines with `active` false only take part in the barriers.
-template <class R, int G>
+template <class R, int G, int TL = 1>
 __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active, int rs) {
   const int k = threadIdx.x % G;
   R* a = line + k * mp;
@@ -710,7 +722,7 @@ __device__ __forceinline__ void chunk_solve(R* line, int m, int mp, bool active,
   }
   R x0, xl;
   if (rs == RS_PCR) {
-    reduced_pcr<R, G>(red, k, active, eA, eC, eD, oA, oC, oD, x0, xl);
+    reduced_pcr<R, G, TL>(red, k, active, eA, eC, eD, oA, oC, oD, x0, xl);
   } else {
     // reduced system in the warp solver's [32][M2P] chunk layout
     constexpr int ARR2 = 32 * M2P;

@@ -32,7 +32,7 @@ __device__ __forceinline__ double solve_lines(S* sm, const SolveIO& io, const in
     if constexpr (EXACT) {
       if (active && threadIdx.x % G == 0) thomas_exact(line, line + arr, line + 2 * arr, line + 3 * arr, n, m, mp);
     } else {
-      chunk_solve<S, G>(line, m, mp, active, RS_PCR);
+      chunk_solve<S, G, TL>(line, m, mp, active, RS_PCR);
     }
   }
   __syncthreads();
