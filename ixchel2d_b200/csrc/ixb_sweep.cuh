@@ -408,11 +408,18 @@ __global__ void __launch_bounds__(TL * G)
 template <auto K>
 cudaError_t fused_go(const SweepShape& s, const Geo<double>& G, const SweepIO<double>& io, const SolveIO& so,
                      cudaStream_t st) {
-  static size_t limit = 48 * 1024 - 1024;  // default limit, less the kernel's static shared memory
-  if (s.smem > limit) {
-    const cudaError_t e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+  // the limit is a per-device attribute of the kernel: raised once per device
+  // (0: the default, 48 KB less the kernel's static shared memory)
+  constexpr int kMaxDev = 64;
+  static size_t limit[kMaxDev] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  if (s.smem > (limit[dev] ? limit[dev] : 48 * 1024 - 1024)) {
+    e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     if (e != cudaSuccess) return e;
-    limit = s.smem;
+    limit[dev] = s.smem;
   }
   return launch_k(K, s.grid, s.tl * s.g, s.smem, st, G, io, so, s.n, s.line_lo, s.line_hi, s.nfull);
 }
