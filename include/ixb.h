@@ -217,8 +217,8 @@ int ixb_phase(ixb_handle* h, int which);
 int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
 /* Launch shape of one sweep (0..7 = u-y, u-x, v-y, v-x, p'-y, p'-x, T-y,
  * T-x): lines per CTA and threads per line, one of (1,128) (1,256) (1,512)
- * (2,64) (2,128) (4,32) (4,64) (4,128) (8,32) (8,64) (8,128) (16,16)
- * (16,32); each thread eliminates a chunk of
+ * (2,64) (2,128) (4,32) (4,64) (4,128) (5,64) (5,128) (6,64) (6,128)
+ * (8,32) (8,64) (8,128) (16,16) (16,32); each thread eliminates a chunk of
  * max(3, ceil(n/threads_per_line)) rows.  lines_per_cta = 0 restores the
  * default (the fewest waves of resident CTAs, then the shortest chunks).
  * No reference counterpart: the reference runs one sequential tridiagonal
@@ -226,7 +226,7 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
 int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads_per_line);
 /* Kernels one outer iteration launches with the current launch shapes (one
  * inner pass per loop): one per sweep whose shape runs assembly and line
- * solve as one kernel (x-sweeps with one line per CTA; y-sweeps with 4, 8 or
+ * solve as one kernel (x-sweeps with one line per CTA; y-sweeps with 4 to
  * 16 lines per CTA), two per other sweep, plus the p/u/v correction and the
  * u residual, and the p' reset when the loop is host-driven
  * (IXB_NO_GRAPH=1) or IXB_DOWHILE=0.  IXB_SPLIT=1 in the environment keeps

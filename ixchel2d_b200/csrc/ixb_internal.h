@@ -176,17 +176,22 @@ struct SolveIO {
 // Launch shapes of the line sweeps (lines per CTA, threads per line); every
 // sweep runs in one of them (ixb_set_sweep_shape, the autotuners).  The
 // line-solve kernels are instantiated for each (IXB_SWEEP_SHAPES, ixb_solve.cu).
-constexpr int kNumShapes = 13;
-constexpr int kShapeList[kNumShapes][2] = {{1, 128}, {1, 256}, {1, 512}, {2, 64},  {2, 128}, {4, 32},  {4, 64},
-                                          {4, 128}, {8, 32},  {8, 64},  {8, 128}, {16, 16}, {16, 32}};
+// 5 and 6 lines per CTA put a 701-line y-sweep on 141 or 117 CTAs (one per
+// SM) where 8 lines leave 60 of the 148 SMs idle.
+constexpr int kNumShapes = 17;
+constexpr int kShapeList[kNumShapes][2] = {{1, 128}, {1, 256}, {1, 512}, {2, 64},  {2, 128}, {4, 32},
+                                          {4, 64},  {4, 128}, {5, 64},  {5, 128}, {6, 64},  {6, 128},
+                                          {8, 32},  {8, 64},  {8, 128}, {16, 16}, {16, 32}};
 
 // Launch shapes (lines per CTA, threads per line) of the fused sweeps:
-// x-sweeps one line per CTA; y-sweeps 4, 8 or 16 adjacent lines per CTA, so
+// x-sweeps one line per CTA; y-sweeps 4 to 16 adjacent lines per CTA, so
 // that a warp's field reads span adjacent lines (with 2 lines a warp reads
 // 16 separate 16-byte pieces and the fused y-sweep measured twice as slow
 // as its two kernels).
 #define IXB_FUSED_X_SHAPES(X_) X_(1, 128) X_(1, 256) X_(1, 512)
-#define IXB_FUSED_Y_SHAPES(X_) X_(4, 32) X_(4, 64) X_(4, 128) X_(8, 32) X_(8, 64) X_(8, 128) X_(16, 16) X_(16, 32)
+#define IXB_FUSED_Y_SHAPES(X_) \
+  X_(4, 32) X_(4, 64) X_(4, 128) X_(5, 64) X_(5, 128) X_(6, 64) X_(6, 128) X_(8, 32) X_(8, 64) X_(8, 128) \
+  X_(16, 16) X_(16, 32)
 inline bool fused_shape(int eq, int tl, int g) {
   bool hit = false;
 #define IXB_HIT_(TL_, G_) hit = hit || (tl == TL_ && g == G_);

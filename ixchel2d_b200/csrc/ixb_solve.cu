@@ -99,8 +99,8 @@ __global__ void __launch_bounds__(TL * G) solve_batch_kernel(const SolveInst* __
 
 // Launch shapes (lines per CTA x threads per line), kShapeList; 128 to 1024 threads.
 #define IXB_SWEEP_SHAPES(X_) \
-  X_(1, 128) X_(1, 256) X_(1, 512) X_(2, 64) X_(2, 128) X_(4, 32) X_(4, 64) X_(4, 128) X_(8, 32) X_(8, 64) \
-  X_(8, 128) X_(16, 16) X_(16, 32)
+  X_(1, 128) X_(1, 256) X_(1, 512) X_(2, 64) X_(2, 128) X_(4, 32) X_(4, 64) X_(4, 128) X_(5, 64) X_(5, 128) \
+  X_(6, 64) X_(6, 128) X_(8, 32) X_(8, 64) X_(8, 128) X_(16, 16) X_(16, 32)
 
 template <class S, bool X, bool DC, bool EXACT>
 struct SolveSet {

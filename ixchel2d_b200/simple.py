@@ -160,8 +160,8 @@ class Simple2D:
         F.check(F.lib.ixb_nusselt_y(self.h, i0, i1, C.byref(a), C.byref(b)), "ixb_nusselt_y")
         return a.value, b.value
 
-    SHAPES = ((1, 128), (1, 256), (1, 512), (2, 64), (2, 128), (4, 32), (4, 64), (4, 128), (8, 32), (8, 64),
-              (8, 128), (16, 16), (16, 32))
+    SHAPES = ((1, 128), (1, 256), (1, 512), (2, 64), (2, 128), (4, 32), (4, 64), (4, 128), (5, 64), (5, 128),
+              (6, 64), (6, 128), (8, 32), (8, 64), (8, 128), (16, 16), (16, 32))
 
     def set_sweep_shape(self, sweep: int, lines_per_cta: int = 0, threads_per_line: int = 0):
         F.check(F.lib.ixb_set_sweep_shape(self.h, sweep, lines_per_cta, threads_per_line), "ixb_set_sweep_shape")
