@@ -289,7 +289,10 @@ __device__ __forceinline__ void fused_assemble(typename SweepTypes<SOLVER, EQ>::
     } else { l = idx % TL; r = idx / TL; }
     const int L = L0 + l;
     const bool valid = L >= line_lo && L <= line_hi && r < n;
-    // padding rows and unsolved lines: identity rows, nothing to assemble
+    // padding rows and unsolved lines become identity rows.  The row is
+    // evaluated for them too (at clamped, in-bounds indices) and then
+    // replaced, so that no branch separates the unrolled rows and their
+    // stencil loads can be issued together.
     const Row<double> row = valid ? staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, true, acc_bo)
                                   : Row<double>{0.0, 1.0, 0.0, 0.0};
     const int ch = r / m;
@@ -312,7 +315,7 @@ __device__ __forceinline__ double tx_residual_row(const Geo<double>& G_, const R
                                                   int L0) {
   double acc = 0.0;
   if (L0 < 2 || L0 > G_.nj) return acc;
-#pragma unroll
+#pragma unroll (M > 0 ? M : 3)
   for (int k = 0; k < (M > 0 ? M : m); ++k) {
     const int ii = 2 + (int)threadIdx.x + k * G;
     const bool valid = ii <= G_.mi - 1;
