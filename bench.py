@@ -303,10 +303,13 @@ def adi_microbench(stream, n=4096, nsys=4096, reps=5):
     """Batched line-solve microbenchmark: nsys independent tridiagonal systems
     of n unknowns, a,c ~ U(-1,0), b = |a|+|c|+U(0.1,1), rhs ~ U(-1,1) (Philox,
     seed 1234), contiguous (x-sweep) and interleaved (y-sweep) layouts, binary64
-    and binary32, through ixb_tridiag_f64/_f32 (hybrid solver).  Algorithmic
-    bytes: a, b, c, d read and x written once (40 B per unknown binary64, 20 B
-    binary32).  Error: max |x - x_ref| / max |x_ref| against the sequential
-    binary64 Thomas (IXB_SOLVER_EXACT) on the same inputs."""
+    and binary32, through ixb_tridiag_f64/_f32: the hybrid solver (Thomas-PCR
+    over many threads per system) and, beside it, Thomas per thread
+    (IXB_SOLVER_EXACT: one thread walks each system, from shared memory in
+    the contiguous layout, straight from global memory with coalesced rows in
+    the interleaved one).  Algorithmic bytes: a, b, c, d read and x written
+    once (40 B per unknown binary64, 20 B binary32).  Error: max |x - x_ref| /
+    max |x_ref| against the sequential binary64 Thomas on the same inputs."""
     import torch
     from ixchel2d_b200 import _ffi as F
     gen = torch.Generator(device="cuda").manual_seed(1234)
@@ -327,23 +330,24 @@ def adi_microbench(stream, n=4096, nsys=4096, reps=5):
         for dt, fn, eb in ((torch.float64, F.lib.ixb_tridiag_f64, 8), (torch.float32, F.lib.ixb_tridiag_f32, 4)):
             Ai, Bi, Ci, Di = (t.to(dt) for t in (A, B, C, D))
             X = torch.empty_like(Di)
-            args = (Ai.data_ptr(), Bi.data_ptr(), Ci.data_ptr(), Di.data_ptr(), X.data_ptr(), n, nsys, layout,
-                    F.SOLVER_HYBRID, sh)
-            torch.cuda.synchronize()
-            with torch.cuda.stream(stream):
-                for _ in range(2):
-                    F.check(fn(*args), "ixb_tridiag")
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                for _ in range(reps):  # inputs (5 x n x nsys) exceed L2: no flush needed
-                    F.check(fn(*args), "ixb_tridiag")
-                e1.record(stream)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-            gbs = 5 * eb * n * nsys / (ms / 1e3) / 1e9
-            err = float((X.double() - ref).abs().max() / ref.abs().max())
-            out[f"{lname}_{'f64' if eb == 8 else 'f32'}"] = {"ms": ms, "gbs": gbs, "frac": gbs / peak,
-                                                             "max_err_vs_f64_thomas": err}
+            for solver, sname in ((F.SOLVER_HYBRID, ""), (F.SOLVER_EXACT, "_thomas_per_thread")):
+                args = (Ai.data_ptr(), Bi.data_ptr(), Ci.data_ptr(), Di.data_ptr(), X.data_ptr(), n, nsys, layout,
+                        solver, sh)
+                torch.cuda.synchronize()
+                with torch.cuda.stream(stream):
+                    for _ in range(2):
+                        F.check(fn(*args), "ixb_tridiag")
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for _ in range(reps):  # inputs (5 x n x nsys) exceed L2: no flush needed
+                        F.check(fn(*args), "ixb_tridiag")
+                    e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                gbs = 5 * eb * n * nsys / (ms / 1e3) / 1e9
+                err = float((X.double() - ref).abs().max() / ref.abs().max())
+                out[f"{lname}_{'f64' if eb == 8 else 'f32'}{sname}"] = {"ms": ms, "gbs": gbs, "frac": gbs / peak,
+                                                                        "max_err_vs_f64_thomas": err}
             del Ai, Bi, Ci, Di, X
         del A, B, C, D, ref
     torch.cuda.empty_cache()

@@ -330,7 +330,7 @@ __device__ __forceinline__ double tx_residual_row(const Geo<double>& G_, const R
 }
 
 template <int EQ, int SOLVER, int TL, int G, int M>
-__global__ void __launch_bounds__(TL * G)
+__global__ void __launch_bounds__(TL * G, TL > 1 ? 1 : (G >= 512 ? 2 : 3))
     fused_sweep_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n,
                        const int line_lo, const int line_hi, const int nfull) {
   IXB_PDL_ENTRY();
