@@ -29,10 +29,14 @@ namespace ixb {
 // metric arrays inside one device buffer, each `mstride` long, 1-based.
 // M_HXU/M_HYV are the energy equation's face diffusivities
 // hmean(ge,ge,fexu(k)) / hmean(ge,ge,feyv(k)), M_RHXU/M_RHYV their
-// reciprocals (fast form), filled by the table kernel.
+// reciprocals (fast form), filled by the table kernel.  The fast form also
+// forms the diffusive conductances gamma*delta/d of the 2-D tables below
+// from 1-D factors (a uniform gamma makes them separable): M_GRDXP =
+// gamma_momen/dxp, M_GRDYV = gamma_momen/dyv, M_GRDXU = gamma_momen/dxu,
+// M_GRDYP = gamma_momen/dyp, M_HRDXU = M_HXU/dxu, M_HRDYV = M_HYV/dyv.
 enum Metric {
   M_DXP = 0, M_DYP, M_DXU, M_DYU, M_DXV, M_DYV, M_FEXP, M_FEYP, M_FEXU, M_FEYV,
-  M_HXU, M_HYV, M_RHXU, M_RHYV, M_COUNT
+  M_HXU, M_HYV, M_RHXU, M_RHYV, M_GRDXP, M_GRDYV, M_GRDXU, M_GRDYP, M_HRDXU, M_HRDYV, M_COUNT
 };
 
 // Mesh-constant 2-D tables (field layout).  With the uniform diffusion
@@ -95,6 +99,21 @@ struct Geo {
   __device__ __forceinline__ int at(int ii, int jj) const { return (jj - 1) * LD + (ii - 1); }
   __device__ __forceinline__ R t(int which, int ii, int jj) const { return __ldg(tab + which * tstride + at(ii, jj)); }
 };
+
+// Diffusive conductances of the assembly.  Exact form: the 2-D table entry
+// (the reference's operands in its order).  Fast form: the product of the
+// cell's 1-D mesh factor, which the caller holds already (`f`), and a 1-D
+// reciprocal factor, an L1-resident load in place of a 2-D table read; it
+// differs from the table by rounding (the face diffusivities of a uniform
+// gamma are gamma itself up to rounding, as in the Peclet numbers).
+//   u: T_CU1(ii,jj) = dyu(jj) * GRDXP(ii);   T_CU2(ii,jj) = dxu(ii) * GRDYV(jj)
+//   v: T_CV1(ii,jj) = dyv(jj) * GRDXU(ii-1); T_CV2(ii,jj) = dxv(ii) * GRDYP(jj)
+//   T: T_CT1(ii,jj) = dyp(jj) * HRDXU(ii-1); T_CT2(ii,jj) = dxp(ii) * HRDYV(jj)
+template <bool FAST, class R>
+__device__ __forceinline__ R cond_t(const Geo<R>& G, int table, int ii, int jj, R f, int metric, int k) {
+  if constexpr (FAST) return f * G.met(metric, k);
+  else return G.t(table, ii, jj);
+}
 
 template <class R>
 struct SweepIO {
@@ -196,10 +215,13 @@ __device__ __forceinline__ void u_parts(const Geo<R>& G, const SweepIO<F>& io, c
   deltax = G.met(M_DXU, ii);
   deltay = G.met(M_DYU, jj);
   temp_int = fexp_i * ld<R>(io.T, G.at(ii + 1, jj)) + (R(1) - fexp_i) * ld<R>(io.T, G.at(ii, jj));
-  AI = -(G.t(T_CU1, ii, jj) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * deltay));
-  AD = -(G.t(T_CU1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) + dmax0(-ud * deltay));
-  BS = -(G.t(T_CU2, ii, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) + dmax0(vs * deltax));
-  BN = -(G.t(T_CU2, ii, jj) * plaw(qdiv<FAST>(vn * dn, gamman, rgn)) + dmax0(-vn * deltax));
+  AI = -(cond_t<FAST>(G, T_CU1, ii, jj, deltay, M_GRDXP, ii) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * deltay));
+  AD = -(cond_t<FAST>(G, T_CU1, ii + 1, jj, deltay, M_GRDXP, ii + 1) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) +
+         dmax0(-ud * deltay));
+  BS = -(cond_t<FAST>(G, T_CU2, ii, jj - 1, deltax, M_GRDYV, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) +
+         dmax0(vs * deltax));
+  BN = -(cond_t<FAST>(G, T_CU2, ii, jj, deltax, M_GRDYV, jj) * plaw(qdiv<FAST>(vn * dn, gamman, rgn)) +
+         dmax0(-vn * deltax));
 }
 
 // X form (ensambla_velu_x): a=AI c=AD b=AC d=Rx, aux = au = AC*rel
@@ -268,10 +290,13 @@ __device__ __forceinline__ void v_parts(const Geo<R>& G, const SweepIO<F>& io, c
   R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYP, jj), dn = G.met(M_DYP, jj + 1);
   const R dyv = G.met(M_DYV, jj), dxv = G.met(M_DXV, ii);
   temp_int = feyp_j * ld<R>(io.T, G.at(ii, jj + 1)) + (R(1) - feyp_j) * ld<R>(io.T, G.at(ii, jj));
-  AI = -(G.t(T_CV1, ii, jj) * plaw(qdiv<FAST>(ui * di, gammai, rgi)) + dmax0(ui * dyv));
-  AD = -(G.t(T_CV1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, gammad, rgd)) + dmax0(-ud * dyv));
-  BS = -(G.t(T_CV2, ii, jj) * plaw(qdiv<FAST>(vs * ds, g, G.inv_gm)) + dmax0(vs * dxv));
-  BN = -(G.t(T_CV2, ii, jj + 1) * plaw(qdiv<FAST>(vn * dn, g, G.inv_gm)) + dmax0(-vn * dxv));
+  AI = -(cond_t<FAST>(G, T_CV1, ii, jj, dyv, M_GRDXU, ii - 1) * plaw(qdiv<FAST>(ui * di, gammai, rgi)) +
+         dmax0(ui * dyv));
+  AD = -(cond_t<FAST>(G, T_CV1, ii + 1, jj, dyv, M_GRDXU, ii) * plaw(qdiv<FAST>(ud * dd, gammad, rgd)) +
+         dmax0(-ud * dyv));
+  BS = -(cond_t<FAST>(G, T_CV2, ii, jj, dxv, M_GRDYP, jj) * plaw(qdiv<FAST>(vs * ds, g, G.inv_gm)) + dmax0(vs * dxv));
+  BN = -(cond_t<FAST>(G, T_CV2, ii, jj + 1, dxv, M_GRDYP, jj + 1) * plaw(qdiv<FAST>(vn * dn, g, G.inv_gm)) +
+         dmax0(-vn * dxv));
 }
 
 template <bool FAST, class R, class F>
@@ -327,10 +352,12 @@ __device__ __forceinline__ void t_parts(const Geo<R>& G, const SweepIO<F>& io, i
   const R di = G.met(M_DXU, ii - 1), dd = G.met(M_DXU, ii), ds = G.met(M_DYV, jj - 1), dn = G.met(M_DYV, jj);
   const R dyp = G.met(M_DYP, jj), dxp = G.met(M_DXP, ii);
   if constexpr (FAST) {
-    AI = -(G.t(T_CT1, ii, jj) * plaw(ui * di * G.met(M_RHXU, ii - 1)) + dmax0(ui * dyp));
-    AD = -(G.t(T_CT1, ii + 1, jj) * plaw(ud * dd * G.met(M_RHXU, ii)) + dmax0(-ud * dyp));
-    BS = -(G.t(T_CT2, ii, jj - 1) * plaw(vs * ds * G.met(M_RHYV, jj - 1)) + dmax0(vs * dxp));
-    BN = -(G.t(T_CT2, ii, jj) * plaw(vn * dn * G.met(M_RHYV, jj)) + dmax0(-vn * dxp));
+    AI = -(cond_t<true>(G, T_CT1, ii, jj, dyp, M_HRDXU, ii - 1) * plaw(ui * di * G.met(M_RHXU, ii - 1)) +
+           dmax0(ui * dyp));
+    AD = -(cond_t<true>(G, T_CT1, ii + 1, jj, dyp, M_HRDXU, ii) * plaw(ud * dd * G.met(M_RHXU, ii)) + dmax0(-ud * dyp));
+    BS = -(cond_t<true>(G, T_CT2, ii, jj - 1, dxp, M_HRDYV, jj - 1) * plaw(vs * ds * G.met(M_RHYV, jj - 1)) +
+           dmax0(vs * dxp));
+    BN = -(cond_t<true>(G, T_CT2, ii, jj, dxp, M_HRDYV, jj) * plaw(vn * dn * G.met(M_RHYV, jj)) + dmax0(-vn * dxp));
   } else {
     const R gammad = G.met(M_HXU, ii);
     const R gammai = G.met(M_HXU, ii - 1);
@@ -468,10 +495,13 @@ __device__ __forceinline__ R residual_u(const Geo<R>& G, const R* u, const R* v,
   const R t_e = T_WRITTEN ? T[G.at(ii + 1, jj)] : ldg(T, G.at(ii + 1, jj));
   const R t_c = T_WRITTEN ? T[c0] : ldg(T, c0);
   R temp_int = fexp_i * t_e + (R(1) - fexp_i) * t_c;
-  R AI = (G.t(T_CU1, ii, jj) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * dyu));
-  R AD = (G.t(T_CU1, ii + 1, jj) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) + dmax0(-ud * dyu));
-  R BS = (G.t(T_CU2, ii, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) + dmax0(vs * dxu));
-  R BN = (G.t(T_CU2, ii, jj) * plaw(qdiv<FAST>(vn * dn, gamman, rgn)) + dmax0(-vn * dxu));
+  R AI = (cond_t<FAST>(G, T_CU1, ii, jj, dyu, M_GRDXP, ii) * plaw(qdiv<FAST>(ui * di, g, G.inv_gm)) + dmax0(ui * dyu));
+  R AD = (cond_t<FAST>(G, T_CU1, ii + 1, jj, dyu, M_GRDXP, ii + 1) * plaw(qdiv<FAST>(ud * dd, g, G.inv_gm)) +
+          dmax0(-ud * dyu));
+  R BS = (cond_t<FAST>(G, T_CU2, ii, jj - 1, dxu, M_GRDYV, jj - 1) * plaw(qdiv<FAST>(vs * ds, gammas, rgs)) +
+          dmax0(vs * dxu));
+  R BN = (cond_t<FAST>(G, T_CU2, ii, jj, dxu, M_GRDYV, jj) * plaw(qdiv<FAST>(vn * dn, gamman, rgn)) +
+          dmax0(-vn * dxu));
   const R fl = flin ? ldg(flin, c0) : R(0);
   const R fc = fcon ? ldg(fcon, c0) : R(0);
   R AC = AI + AD + BS + BN - dxu * dyu * fl + qdiv<FAST>(dxu * dyu, G.dt, G.inv_dt);

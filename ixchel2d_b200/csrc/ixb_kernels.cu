@@ -23,15 +23,26 @@ template <class R>
 __global__ void table1d_kernel(Geo<R> G, R* met) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const R ge = G.ge;
+  // 1-D factor num / d of the fast form's conductances (0 where d is not set)
+  auto ratio = [](R num, R d) { return d != R(0) ? num / d : R(0); };
+  const R g = G.gm;
   if (k >= 1 && k <= G.mi) {
     const R h = hmean(ge, ge, G.met(M_FEXU, k));
     met[M_HXU * G.mstride + k] = h;
     met[M_RHXU * G.mstride + k] = R(1) / h;
+    met[M_HRDXU * G.mstride + k] = ratio(h, G.met(M_DXU, k));
   }
   if (k >= 1 && k <= G.nj) {
     const R h = hmean(ge, ge, G.met(M_FEYV, k));
     met[M_HYV * G.mstride + k] = h;
     met[M_RHYV * G.mstride + k] = R(1) / h;
+    met[M_HRDYV * G.mstride + k] = ratio(h, G.met(M_DYV, k));
+  }
+  if (k >= 1 && k < G.mstride) {
+    met[M_GRDXP * G.mstride + k] = ratio(g, G.met(M_DXP, k));
+    met[M_GRDYV * G.mstride + k] = ratio(g, G.met(M_DYV, k));
+    met[M_GRDXU * G.mstride + k] = ratio(g, G.met(M_DXU, k));
+    met[M_GRDYP * G.mstride + k] = ratio(g, G.met(M_DYP, k));
   }
 }
 
