@@ -122,7 +122,8 @@ __device__ __forceinline__ Row<double> staged_row(
   }
   if constexpr (ST::MIX) {
     // unit diagonal before the binary32 staging; the solution is unchanged
-    const double sc = 1.0 / row.b;
+    // (a Newton-refined reciprocal: the scaled row is rounded to binary32)
+    const double sc = fast_rcp(row.b);
     row.a *= sc;
     row.c *= sc;
     row.d *= sc;
