@@ -914,6 +914,39 @@ def run_profile_batch():
     bt.close()
 
 
+def run_batch_converge(cap):
+    """Batched configuration at full size, run to convergence: the 256
+    natural-convection cavities of batched_bench (side uniform in 64..512, Ra
+    log-uniform in [1e3, 1e6], Pr 0.71, seed 1234) in the refined form, each
+    iterated until maxbo < 1e-8 or `cap` outer iterations, in one batched
+    loop.  Prints one JSON line: instances converged, device wall seconds,
+    converged instances per second, and the iterations each instance took."""
+    import torch
+    from ixchel2d_b200 import Batch, cases
+    from ixchel2d_b200 import _ffi as F
+    rng = np.random.default_rng(1234)
+    n_inst = 256
+    sides = rng.integers(64, 513, n_inst)
+    ras = 10.0 ** rng.uniform(3.0, 6.0, n_inst)
+    cs = [cases.natural_cavity(int(a), int(a), Ra=float(r), T0=0.5) for a, r in zip(sides, ras)]
+    bt = Batch.from_cases(cs, prec=F.PREC_FP32_REFINED, conv_paso=1e-8, conv_resi=1e30)
+    bt.autotune(reps=2)
+    bt.restart()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bt.iterate(cap)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    reps = [bt.report(i) for i in range(n_inst)]
+    bt.close()
+    conv = [i for i, r in enumerate(reps) if r["exit_code"] == 1]
+    print(json.dumps({"batched_converge": {
+        "instances": n_inst, "criterion": "maxbo < 1e-8", "cap_iters": cap, "form": "refined",
+        "converged": len(conv), "seconds": dt, "converged_per_s": len(conv) / dt,
+        "iters": [int(r["n_simple"]) for r in reps], "sides": [int(a) for a in sides],
+        "ra": [float(r) for r in ras]}}))
+
+
 def run_profile_adjoint():
     """Profiling driver: the energy adjoint on the 256 x 256 cavity (Ra 1e5)
     after 50 SIMPLE iterations, 128 hot-wall nodes, K = 2 passes (one launch
@@ -954,6 +987,8 @@ def main():
     ap.add_argument("--profile-adi", action="store_true", help="run the line-solve profiling driver")
     ap.add_argument("--profile-batch", action="store_true", help="run the batched-cavities profiling driver")
     ap.add_argument("--profile-adjoint", action="store_true", help="run the energy-adjoint profiling driver")
+    ap.add_argument("--batch-converge", type=int, default=0, metavar="CAP",
+                    help="run the 256 batched cavities to maxbo < 1e-8 (at most CAP outer iterations) and exit")
     ap.add_argument("--profile-simple-adjoint", action="store_true",
                     help="run the profiling driver of the full coupled adjoint")
     args = ap.parse_args()
@@ -962,6 +997,9 @@ def main():
         return
     if args.profile_adi:
         run_profile_adi()
+        return
+    if args.batch_converge:
+        run_batch_converge(args.batch_converge)
         return
     if args.profile_batch:
         run_profile_batch()

@@ -87,8 +87,11 @@ int ensure_tables(ixb_handle* h) {
 // Default launch shape of a sweep, from per-shape timings of every sweep on
 // 64x64, 256x256 and 701x301 grids in both precision forms: x-lines one per
 // CTA with 256 threads for lines of more than 384 rows, else 128; y-lines in
-// the fused form with 4 adjacent lines per CTA (8 once there are 4 lines per
-// SM) and 128 threads per line for lines of 160 rows or more, else 64.
+// the fused form with the fewest of 4, 5, 6 or 8 adjacent lines per CTA that
+// keeps one CTA per SM (8 beyond that), and 128 threads per line for lines
+// of 160 rows or more, else 64 (at 701x301: 5 x 128, one CTA on each of 141
+// SMs, where 8 x 128 leaves 60 SMs idle; the u-y sweep measured 17.5 against
+// 19.3 us, the other y-sweeps within 1 %).
 // Those shapes were within about 5 % of the best (at worst 15 %, binary64
 // y-sweeps at 701x301), where the rule below was 20-50 % behind.  When the
 // shape cannot be resident: the fewest waves of CTAs, then the shortest
@@ -98,7 +101,12 @@ void pick_shape(ixb_handle* h, int eq) {
     const bool x = (eq & 1) != 0;
     SweepShape probe = sweep_shape(eq, h->mi, h->nj, real_bytes(h), 1, 128);
     const int lines = probe.nfull, n = probe.n;
-    const int tl = x ? 1 : (lines >= 4 * h->nsm ? 8 : 4);
+    int tl = 1;
+    if (!x) {
+      tl = 8;
+      for (const int t : {4, 5, 6})
+        if ((lines + t - 1) / t <= h->nsm) { tl = t; break; }
+    }
     const int g = x ? (n > 384 ? 256 : 128) : (n >= 160 ? 128 : 64);
     const SweepShape s = sweep_shape(eq, h->mi, h->nj, real_bytes(h), tl, g);
     if (sweep_occupancy(eq, solver_form(h), s) > 0) {
