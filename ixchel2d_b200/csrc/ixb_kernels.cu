@@ -107,9 +107,17 @@ __device__ __forceinline__ void correct_cell(const Geo<R>& G, R* __restrict__ u,
   const int ii = 2 + idx % ni;
   const int jj = 2 + idx / ni;
   const size_t c0 = G.at(ii, jj);
-  p[c0] = p[c0] + G.p_update * pc[c0];
-  if (ii <= G.mi - 1) u[c0] = u[c0] + qdiv<FAST>(G.met(M_DYU, jj) * (pc[c0] - pc[G.at(ii + 1, jj)]), au[c0]);
-  if (jj <= G.nj - 1) v[c0] = v[c0] + qdiv<FAST>(G.met(M_DXV, ii) * (pc[c0] - pc[G.at(ii, jj + 1)]), av[c0]);
+  // Every load first, then the stores: u at ii = mi and v at jj = nj are
+  // boundary values the update leaves alone, but their entries (and those of
+  // au, av and p' one cell further) exist, so the three updates' loads go out
+  // together instead of one branch after another; the unused results are
+  // dropped.
+  const R p0 = p[c0], pc0 = pc[c0], pce = pc[G.at(ii + 1, jj)], pcn = pc[G.at(ii, jj + 1)];
+  const R u0 = u[c0], au0 = au[c0], v0 = v[c0], av0 = av[c0];
+  const R dyu = G.met(M_DYU, jj), dxv = G.met(M_DXV, ii);
+  p[c0] = p0 + G.p_update * pc0;
+  if (ii <= G.mi - 1) u[c0] = u0 + qdiv<FAST>(dyu * (pc0 - pce), au0);
+  if (jj <= G.nj - 1) v[c0] = v0 + qdiv<FAST>(dxv * (pc0 - pcn), av0);
 }
 
 template <class R, bool FAST>
