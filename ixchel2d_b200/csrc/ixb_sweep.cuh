@@ -290,10 +290,8 @@ __device__ __forceinline__ void fused_assemble(typename SweepTypes<SOLVER, EQ>::
     } else { l = idx % TL; r = idx / TL; }
     const int L = L0 + l;
     const bool valid = L >= line_lo && L <= line_hi && r < n;
-    // padding rows and unsolved lines become identity rows.  The row is
-    // evaluated for them too (at clamped, in-bounds indices) and then
-    // replaced, so that no branch separates the unrolled rows and their
-    // stencil loads can be issued together.
+    // padding rows and unsolved lines: identity rows, nothing to assemble
+    // (assembling them too, branch-free, and replacing them measured slower)
     const Row<double> row = valid ? staged_row<EQ, SOLVER>(G_, io, L, r, n, line_lo, line_hi, true, acc_bo)
                                   : Row<double>{0.0, 1.0, 0.0, 0.0};
     const int ch = r / m;
@@ -330,6 +328,11 @@ __device__ __forceinline__ double tx_residual_row(const Geo<double>& G_, const R
   return acc;
 }
 
+// The second launch bound is the resident-CTA count a sweep at 701x301 needs
+// for one wave (y-lines: one CTA per SM; x-lines: three, two with 512
+// threads).  Without it ptxas held these kernels to 48-64 registers and the
+// assembly issued a row's stencil loads in several rounds; with it they take
+// up to 104 (y) and 85 (x) registers.
 template <int EQ, int SOLVER, int TL, int G, int M>
 __global__ void __launch_bounds__(TL * G, TL > 1 ? 1 : (G >= 512 ? 2 : 3))
     fused_sweep_kernel(const Geo<double> G_, const SweepIO<double> io, const SolveIO so, const int n,
