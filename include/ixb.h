@@ -220,7 +220,9 @@ int ixb_time_phases(ixb_handle* h, int reps, size_t flush_bytes, double* ms);
  * (2,64) (2,128) (4,32) (4,64) (4,128) (5,64) (5,128) (6,64) (6,128)
  * (8,32) (8,64) (8,128) (16,16) (16,32); each thread eliminates a chunk of
  * max(3, ceil(n/threads_per_line)) rows.  lines_per_cta = 0 restores the
- * default (the fewest waves of resident CTAs, then the shortest chunks).
+ * default: x-lines one per CTA, 256 threads above 384 rows, else 128;
+ * y-lines the fewest of 4, 5, 6 or 8 adjacent lines per CTA that keeps one
+ * CTA per SM (8 beyond that), 128 threads per line from 160 rows, else 64.
  * No reference counterpart: the reference runs one sequential tridiagonal
  * per OpenACC gang. */
 int ixb_set_sweep_shape(ixb_handle* h, int sweep, int lines_per_cta, int threads_per_line);
