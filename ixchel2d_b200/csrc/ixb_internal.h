@@ -20,6 +20,8 @@ namespace ixb {
 // iteration against 109.9 us without it (refined; binary64 138 against
 // 120 us).
 bool pdl_enabled();
+// fused sweeps set a shared-memory carveout of one wave of CTAs unless IXB_CARVEOUT=0
+bool carveout_enabled();
 // fused sweeps (one kernel per sweep) unless IXB_SPLIT=1
 bool fused_enabled();
 template <class... KArgs, class... Args>

@@ -333,6 +333,16 @@ bool fused_enabled() {
   return on;
 }
 
+// Fused sweeps ask for a shared-memory carveout sized to one wave of their
+// CTAs unless IXB_CARVEOUT=0.
+bool carveout_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("IXB_CARVEOUT");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 bool pdl_enabled() {
   static const bool on = [] {
     const char* e = getenv("IXB_PDL");

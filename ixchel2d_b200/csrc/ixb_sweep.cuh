@@ -428,6 +428,22 @@ cudaError_t fused_go(const SweepShape& s, const Geo<double>& G, const SweepIO<do
     if (e != cudaSuccess) return e;
     limit[dev] = s.smem;
   }
+  if (carveout_enabled()) {
+    // shared-memory carveout: just what the CTAs of one wave need per SM (one
+    // y-line CTA, three x-line CTAs, two of 512 threads), the rest of the SM's
+    // unified memory left to L1 for the stencil loads
+    static int pct_set[kMaxDev] = {};
+    int per_sm = 0;
+    if ((e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+      return e;
+    const size_t ctas = s.tl > 1 ? 1 : (s.g >= 512 ? 2 : 3);
+    const size_t need = ctas * (s.smem + 1024);
+    const int pct = per_sm > 0 ? (int)std::min<size_t>(100, (need * 100 + per_sm - 1) / per_sm) : 100;
+    if (pct != pct_set[dev]) {
+      if ((e = cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout, pct)) != cudaSuccess) return e;
+      pct_set[dev] = pct;
+    }
+  }
   return launch_k(K, s.grid, s.tl * s.g, s.smem, st, G, io, so, s.n, s.line_lo, s.line_hi, s.nfull);
 }
 
