@@ -14,24 +14,33 @@ __device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
 
 // End of an inner pass.  which: 0 momentum (||dv|| vs conv_u), 1 pressure
 // (||dp'|| vs conv_p, with maxbo), 2 energy (||dT|| vs conv_t).
-// Returns whether the loop runs another pass.
+// Returns whether the loop runs another pass.  Every field is loaded before
+// any is stored (one round trip to memory instead of a chain of them: a
+// store to the control block would otherwise order the loads after it).
 static __device__ bool ctl_inner_step(Ctl* c, const double* norms, int which, cudaGraphConditionalHandle inner) {
-  double err, conv;
-  if (which == 0) { err = norms[N_DV]; conv = c->conv_u; c->err_u = err; c->n_momen++; }
-  else if (which == 1) { err = norms[N_DP]; conv = c->conv_p; c->err_p = err; c->maxbo = norms[N_BO]; c->n_pres++; }
-  else { err = norms[N_DT]; conv = c->conv_t; c->err_t = err; c->n_ener++; }
+  const double n_dv = norms[N_DV], n_dp = norms[N_DP], n_bo = norms[N_BO], n_dt = norms[N_DT];
+  const double conv_u = c->conv_u, conv_p = c->conv_p, conv_t = c->conv_t;
+  const int iter = c->iter_ecuaci, iter_max = c->iter_ecuaci_max, done = c->inner_done + 1;
+  const long long n_momen = c->n_momen, n_pres = c->n_pres, n_ener = c->n_ener;
+  const double err = which == 0 ? n_dv : (which == 1 ? n_dp : n_dt);
+  const double conv = which == 0 ? conv_u : (which == 1 ? conv_p : conv_t);
   bool again;
-  c->inner_done++;
-  if (!finite_d(err) || (which == 1 && !finite_d(norms[N_BO]))) {
-    c->status = IXB_ENONFINITE;  // the outer control ends the loop
+  int status = 0, iter_new = iter;
+  if (!finite_d(err) || (which == 1 && !finite_d(n_bo))) {
+    status = IXB_ENONFINITE;  // the outer control ends the loop
     again = false;
-  } else if (err < conv) { c->iter_ecuaci = 0; again = false; }
-  else if (c->iter_ecuaci > c->iter_ecuaci_max) { c->iter_ecuaci = 0; again = false; }
-  else { c->iter_ecuaci++; again = true; }
+  } else if (err < conv) { iter_new = 0; again = false; }
+  else if (iter > iter_max) { iter_new = 0; again = false; }
+  else { iter_new = iter + 1; again = true; }
   // the reference's counter logic bounds a loop by iter_ecuaci_max + 2
   // passes; enforce it independently so no WHILE node can run away
-  if (again && (long long)c->inner_done >= (long long)c->iter_ecuaci_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
-  if (!again) c->inner_done = 0;  // the next inner loop counts from zero
+  if (again && (long long)done >= (long long)iter_max + 2) { status = IXB_ETIMEOUT; again = false; }
+  if (which == 0) { c->err_u = err; c->n_momen = n_momen + 1; }
+  else if (which == 1) { c->err_p = err; c->maxbo = n_bo; c->n_pres = n_pres + 1; }
+  else { c->err_t = err; c->n_ener = n_ener + 1; }
+  if (status != 0) c->status = status;
+  c->iter_ecuaci = iter_new;
+  c->inner_done = again ? done : 0;  // the next inner loop counts from zero
   cudaGraphSetConditional(inner, again ? 1u : 0u);
   return again;
 }
@@ -43,24 +52,29 @@ static __device__ void ctl_gate_step(Ctl* c, cudaGraphConditionalHandle inner) {
 }
 
 // End of an outer pass; also opens the momentum loop of the next pass.
+// Loads first, then stores, as in ctl_inner_step.
 static __device__ void ctl_outer_step(Ctl* c, const double* norms, cudaGraphConditionalHandle outer,
                                       cudaGraphConditionalHandle first_inner) {
+  const int status = c->status, fixed = c->fixed_count, done = c->outer_done + 1;
+  const int iter = c->iter_simple, iter_max = c->iter_simple_max;
+  const long long n_simple = c->n_simple;
+  const double res = norms[N_RES], maxbo = c->maxbo, conv_paso = c->conv_paso, conv_resi = c->conv_resi;
   c->inner_done = 0;
   cudaGraphSetConditional(first_inner, 1u);
-  if (c->status != 0) { cudaGraphSetConditional(outer, 0); return; }
-  c->residuo = norms[N_RES];
-  c->n_simple++;
-  c->outer_done++;
-  if (!finite_d(c->residuo)) { c->status = IXB_ENONFINITE; cudaGraphSetConditional(outer, 0); return; }
-  if (c->fixed_count > 0) {
-    cudaGraphSetConditional(outer, c->outer_done < c->fixed_count ? 1u : 0u);
+  if (status != 0) { cudaGraphSetConditional(outer, 0); return; }
+  c->residuo = res;
+  c->n_simple = n_simple + 1;
+  c->outer_done = done;
+  if (!finite_d(res)) { c->status = IXB_ENONFINITE; cudaGraphSetConditional(outer, 0); return; }
+  if (fixed > 0) {
+    cudaGraphSetConditional(outer, done < fixed ? 1u : 0u);
     return;
   }
   bool again;
-  if (c->maxbo < c->conv_paso && c->residuo < c->conv_resi) { c->iter_simple = 0; c->exit_code = 1; again = false; }
-  else if (c->iter_simple > c->iter_simple_max) { c->iter_simple = 0; c->exit_code = 2; again = false; }
-  else { c->iter_simple++; again = true; }
-  if (again && (long long)c->outer_done >= (long long)c->iter_simple_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
+  if (maxbo < conv_paso && res < conv_resi) { c->iter_simple = 0; c->exit_code = 1; again = false; }
+  else if (iter > iter_max) { c->iter_simple = 0; c->exit_code = 2; again = false; }
+  else { c->iter_simple = iter + 1; again = true; }
+  if (again && (long long)done >= (long long)iter_max + 2) { c->status = IXB_ETIMEOUT; again = false; }
   cudaGraphSetConditional(outer, again ? 1u : 0u);
 }
 
